@@ -1,0 +1,138 @@
+"""ctypes front end of the CPU oracle (test infrastructure).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import this module. It is the
+checker of the CUDA path and the timed CPU baseline, never part of the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3}
+BC = {"transmissive": 0, "periodic": 1}
+FLUX = {"hllc": 0, "force": 1}
+N_PARAMS5 = 189
+PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")
+
+_LIBS: dict[str, C.CDLL] = {}
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+
+def _lib(fast: bool = False) -> C.CDLL:
+    name = "liboracle_fast.so" if fast else "liboracle.so"
+    if name not in _LIBS:
+        path = HERE / name
+        if not path.exists():
+            from oracle import build_oracle  # noqa: PLC0415
+            build_oracle.build()
+        lib = C.CDLL(str(path))
+        lib.or_euler2d_run.restype = C.c_int
+        lib.or_euler2d_run.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _fp,
+                                       C.c_int, C.c_int, _dp, C.c_int, C.POINTER(C.c_double)]
+        lib.or_euler2d_stage.restype = C.c_int
+        lib.or_euler2d_stage.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _fp]
+        lib.or_euler2d_max_speed.restype = C.c_double
+        lib.or_euler2d_max_speed.argtypes = [_dp, C.c_int, C.c_int, C.c_double]
+        lib.or_hllc_flux_flat.argtypes = [_dp, _dp, C.c_int, C.c_double, _dp]
+        lib.or_force_flux_flat.argtypes = [_dp, _dp, C.c_int, C.c_double, C.c_double, _dp]
+        lib.or_closure_weights_batch.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _fp, _dp]
+        lib.or_reconstruct_batch.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _fp, _dp]
+        lib.or_mlp_ratios_batch.argtypes = [_dp, C.c_int, C.c_int, _dp, _fp, _dp]
+        lib.or_num_threads.restype = C.c_int
+        _LIBS[name] = lib
+    return _LIBS[name]
+
+
+def pack_params(params: dict, dtype=np.float64) -> np.ndarray:
+    """Flatten w1..b4 (leading dim 1 allowed) into the packed [in][out] row-major layout."""
+    return np.ascontiguousarray(np.concatenate([np.asarray(params[k]).reshape(-1) for k in PARAM_NAMES]),
+                                dtype=dtype)
+
+
+def _params(params):
+    if params is None:
+        return np.zeros(N_PARAMS5), np.zeros(N_PARAMS5, dtype=np.float32)
+    return pack_params(params, np.float64), pack_params(params, np.float32)
+
+
+def closure_weights(q: np.ndarray, head: int, method: str, params=None) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 5)
+    out = np.zeros((q.shape[0], 3))
+    p64, p32 = _params(params)
+    _lib().or_closure_weights_batch(q, q.shape[0], head, METHOD[method], p64, p32, out)
+    return out
+
+
+def reconstruct(q: np.ndarray, head: int, method: str, params=None) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 5)
+    out = np.zeros(q.shape[0])
+    p64, p32 = _params(params)
+    _lib().or_reconstruct_batch(q, q.shape[0], head, METHOD[method], p64, p32, out)
+    return out
+
+
+def mlp_ratios(features: np.ndarray, method: str, params) -> np.ndarray:
+    x = np.ascontiguousarray(features, dtype=np.float64).reshape(-1, 5)
+    out = np.zeros((x.shape[0], 3))
+    p64, p32 = _params(params)
+    _lib().or_mlp_ratios_batch(x, x.shape[0], METHOD[method], p64, p32, out)
+    return out
+
+
+def hllc(ul, ur, direction: int, gamma: float = 1.4) -> np.ndarray:
+    out = np.zeros(4)
+    _lib().or_hllc_flux_flat(np.ascontiguousarray(ul, dtype=np.float64), np.ascontiguousarray(ur, dtype=np.float64),
+                             direction, gamma, out)
+    return out
+
+
+def force(ul, ur, direction: int, c: float, gamma: float = 1.4) -> np.ndarray:
+    out = np.zeros(4)
+    _lib().or_force_flux_flat(np.ascontiguousarray(ul, dtype=np.float64), np.ascontiguousarray(ur, dtype=np.float64),
+                              direction, c, gamma, out)
+    return out
+
+
+def max_speed(u: np.ndarray, nx: int, ny: int, gamma: float = 1.4) -> float:
+    return float(_lib().or_euler2d_max_speed(np.ascontiguousarray(u, dtype=np.float64), nx, ny, gamma))
+
+
+def euler2d_stage(u_stage, u0, u_out, nx, ny, dx, dy, dt, rk, method, bc="transmissive", flux="hllc",
+                  params=None, gamma=1.4) -> np.ndarray:
+    """One SSPRK3 stage; returns a copy of u_out with its interior overwritten."""
+    out = np.array(u_out, dtype=np.float64, copy=True)
+    p64, p32 = _params(params)
+    rc = _lib().or_euler2d_stage(np.ascontiguousarray(u_stage, dtype=np.float64),
+                                 np.ascontiguousarray(u0, dtype=np.float64), out, nx, ny, dx, dy, gamma, dt, rk,
+                                 METHOD[method], BC[bc], FLUX[flux], p64, p32)
+    if rc != 0:
+        raise MemoryError("oracle stage allocation failed")
+    return out
+
+
+def euler2d_run(initial, nx, ny, dx, dy, cfl, t_end, method, bc="transmissive", flux="hllc", params=None,
+                gamma=1.4, check_health=False, fixed_steps=0, max_steps=100000, fast=False):
+    """Time loop of the reference adapters. Returns (final padded array, dts, steps, t)."""
+    init = np.ascontiguousarray(initial, dtype=np.float64)
+    out = np.zeros_like(init)
+    dts = np.zeros(max_steps)
+    t = C.c_double(0.0)
+    p64, p32 = _params(params)
+    steps = _lib(fast).or_euler2d_run(init, out, nx, ny, dx, dy, gamma, cfl, t_end, METHOD[method], BC[bc],
+                                      FLUX[flux], p64, p32, int(check_health), fixed_steps, dts, max_steps,
+                                      C.byref(t))
+    if steps < 0:
+        raise MemoryError("oracle run allocation failed")
+    return out, list(dts[:min(steps, max_steps)]), steps, t.value
+
+
+def num_threads(fast: bool = True) -> int:
+    return int(_lib(fast).or_num_threads())

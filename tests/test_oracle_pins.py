@@ -1,0 +1,139 @@
+"""Pin the CPU oracle to the reference.
+
+The fixtures in tests/golden/ were produced by tests/golden/make_golden.py, which executes the
+reference's own Warp kernels (through a pure-Python warp stand-in) and its torch models. These tests
+need no GPU.
+"""
+from __future__ import annotations
+
+import hashlib
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+G = Path(__file__).resolve().parent / "golden"
+P64 = dict(np.load(G / "models" / "weno5_sr_fp64_step012250.npz"))
+P32 = dict(np.load(G / "models" / "weno5_sr_fp32_step016500.npz"))
+
+# SHA-256 values published in the reference's models/MODEL_CARD.md
+MODEL_SHA = {
+    "weno5_sr_fp64_step012250.npz": "368759415a7dcf5567af76db06fd49c0b89260150f0fab7d9ada7f067ab3f74e",
+    "weno5_sr_fp32_step016500.npz": "c88441a950b91713353685edc0aa4debcb848fdddb1ba1b9442dd893a40600bc",
+    "weno7_sr_fp64_step016750.npz": "0a55fd07a87e73b28e1c471991322dc256ddebccdbfdf2d5ba3722ae8dde3d93",
+}
+
+
+@pytest.mark.parametrize("name", sorted(MODEL_SHA))
+def test_checkpoint_fixture_hashes(name):
+    digest = hashlib.sha256((G / "models" / name).read_bytes()).hexdigest()
+    assert digest == MODEL_SHA[name]
+
+
+def _effective_scale(features_torch_scale: np.ndarray) -> np.ndarray:
+    """Torch-side features carry clip((log10 r + 16)/16); the deployed MLP sees clip((log10 r + 4)/4)."""
+    f = np.array(features_torch_scale, dtype=np.float64)
+    log10r = 16.0 * f[:, 4] - 16.0
+    f[:, 4] = np.clip((log10r + 4.0) / 4.0, 0.0, 1.0)
+    return f
+
+
+def _reflection_average(x, method, params):
+    direct = O.mlp_ratios(x, method, params)
+    reflected = O.mlp_ratios(x[:, [2, 1, 0, 3, 4]], method, params)
+    return 0.5 * (direct + reflected[:, ::-1])
+
+
+def test_mlp_golden_vectors_fp64():
+    g = np.load(G / "mlp_golden.npz")
+    out = _reflection_average(_effective_scale(g["features5_torch_scale"]), "sr_f64", P64)
+    np.testing.assert_allclose(out, g["out5_f64"], rtol=0, atol=5e-15)  # verify_release.py:224-227
+
+
+def test_mlp_golden_vectors_fp32():
+    g = np.load(G / "mlp_golden.npz")
+    out = _reflection_average(_effective_scale(g["features5_torch_scale"]), "sr_f32", P32)
+    np.testing.assert_allclose(out, g["out5_f32"], rtol=0, atol=2e-7)
+
+
+@pytest.mark.parametrize("head", [0, 1, 2, 3])
+def test_closure_weights_fp64_match_reference(head):
+    c = np.load(G / "closure2d.npz")
+    w = O.closure_weights(c["q"], head, "sr_f64", P64)
+    np.testing.assert_allclose(w, c[f"w_sr_f64_h{head}"], rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("head", [0, 1, 2, 3])
+def test_closure_weights_fp32_match_reference(head):
+    c = np.load(G / "closure2d.npz")
+    w = O.closure_weights(c["q"], head, "sr_f32", P32)
+    np.testing.assert_allclose(w, c[f"w_sr_f32_h{head}"], rtol=0, atol=5e-7)
+
+
+def test_plateau_stencils_return_linear_weights():
+    c = np.load(G / "closure2d.npz")
+    q = c["q"][3::8]  # exact plateaus
+    w = O.closure_weights(q, 0, "sr_f64", P64)
+    np.testing.assert_array_equal(w, np.tile([0.1, 0.6, 0.3], (q.shape[0], 1)))
+
+
+@pytest.mark.parametrize("key,head", [("v_js_lr1", 0), ("v_js_lr2", 1), ("v_js_g1", 2), ("v_js_g2", 3)])
+def test_js_reconstruction_bitwise(key, head):
+    c = np.load(G / "closure2d.npz")
+    np.testing.assert_array_equal(O.reconstruct(c["q"], head, "js"), c[key])
+
+
+@pytest.mark.parametrize("key,head", [("lr1", 0), ("lr2", 1), ("g1", 2), ("g2", 3)])
+def test_sr_reconstruction(key, head):
+    c = np.load(G / "closure2d.npz")
+    scale = np.maximum(np.abs(c["q"]).max(axis=1), 1.0)
+    v64 = O.reconstruct(c["q"], head, "sr_f64", P64)
+    np.testing.assert_allclose(v64 / scale, c[f"v_sr_f64_{key}"] / scale, rtol=0, atol=1e-14)
+    v32 = O.reconstruct(c["q"], head, "sr_f32", P32)
+    np.testing.assert_allclose(v32 / scale, c[f"v_sr_f32_{key}"] / scale, rtol=0, atol=1e-6)
+
+
+@pytest.mark.parametrize("direction", [1, 2])
+def test_hllc_and_force_bitwise(direction):
+    h = np.load(G / "hllc2d.npz")
+    f = np.array([O.hllc(a, b, direction) for a, b in zip(h["left"], h["right"])])
+    np.testing.assert_array_equal(f, h[f"hllc_d{direction}"])
+    f = np.array([O.force(a, b, direction, 0.3) for a, b in zip(h["left"], h["right"])])
+    np.testing.assert_array_equal(f, h[f"force_d{direction}"])
+
+
+CASES = ["rough_trans", "quadrant_trans", "smooth_periodic"]
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("method,tol", [("js", 0.0), ("sr_f64", 1e-13), ("sr_f32", 1e-7)])
+def test_euler2d_run_matches_reference(case, method, tol):
+    e = np.load(G / f"euler2d_{case}.npz")
+    nx, ny = int(e["nx"]), int(e["ny"])
+    params = {"js": None, "sr_f64": P64, "sr_f32": P32}[method]
+    fin, dts, steps, t = O.euler2d_run(e["initial"], nx, ny, 1.0 / nx, 1.0 / ny, 0.4, float(e["t_end"]), method,
+                                       str(e["bc"]), params=params, check_health=(method == "sr_f64"))
+    assert steps == int(e[f"{method}_steps"])
+    assert abs(t - float(e[f"{method}_t"])) < 1e-14
+    ref = e[f"{method}_final"]
+    interior = (slice(3, 3 + ny), slice(3, 3 + nx))
+    err = np.abs(fin[interior] - ref[interior]).max() / np.abs(ref[interior]).max()
+    assert err <= tol, err
+    if method == "js":
+        np.testing.assert_array_equal(fin, ref)  # ghost cells included
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_euler2d_first_stage(case):
+    e = np.load(G / f"euler2d_{case}.npz")
+    nx, ny = int(e["nx"]), int(e["ny"])
+    init = e["initial"]
+    for method, params, tol in (("js", None, 0.0), ("sr_f64", P64, 1e-14), ("sr_f32", P32, 1e-7)):
+        dt = float(e[f"{method}_dts"][0])
+        out = O.euler2d_stage(init, init, np.zeros_like(init), nx, ny, 1.0 / nx, 1.0 / ny, dt, 1, method,
+                              str(e["bc"]), params=params)
+        ref = e[f"{method}_stage1"]
+        err = np.abs(out - ref).max() / np.abs(ref).max()
+        assert err <= tol, (method, err)
