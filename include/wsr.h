@@ -1,0 +1,105 @@
+/*
+ * C ABI of the B200 WENO5-SR / WENO5-JS finite-volume path (libwsr.so).
+ *
+ * Plain pointers, sizes and an explicit CUDA stream (passed as void*; NULL = legacy default
+ * stream). All array pointers are DEVICE pointers owned by the caller unless stated otherwise.
+ * Every function returns an int status (WSR_OK = 0); wsr_last_error() gives the message.
+ *
+ * State layout: the reference's padded row-major array u[(ny+6)][(nx+6)][4] of FP64 conserved
+ * variables (rho, rho u, rho v, E), ghost width 3 (warp_weno5_helpers.py:66-87). Ghost cells are
+ * read through the boundary mapping and never written, exactly like the reference's stage buffers.
+ *
+ * Reference interfaces replaced (paths inside the reference project, code/snapshot/):
+ *   wsr_closure_upload     load_mlp_params -> {w1..b4} device arrays
+ *                          (run_weno5_circle_mlp_compare.py:49-81 FP64;
+ *                           teacherfree_lab_weno5_mlp_f32/warp_mlp_f32/run_weno5_circle_mlp_compare_mlp_f32.py:52-84 FP32)
+ *   wsr_euler2d_stage      launch_stage(u_stage, u0, u_out, stage, params, dt, rk, ...)
+ *                          (for_paper_results/solvers/weno5_hllc.py:294-358 JS;
+ *                           teacherfree_lab_weno5_v20_distance_balanced/weno5_hllc_refsym.py:298-435 SR FP64;
+ *                           for_paper_results/solvers/weno5_hllc_mixed.py:121-168 SR FP32)
+ *   wsr_euler2d_max_speed  compute_dt_from_warp_array's max-speed kernel (warp_weno5_helpers.py:189-207, 876-897)
+ *   wsr_euler2d_run        run_to_time(initial, params, t_end, device, mlp_params, boundary, ...)
+ *                          (weno5_hllc.py:386-410; weno5_hllc_refsym.py:462-544; weno5_hllc_mixed.py:185-212)
+ */
+#ifndef WSR_H
+#define WSR_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define WSR_OK 0
+#define WSR_ERR_ARG 1         /* invalid argument (sizes, enum values, null pointers, short workspace) */
+#define WSR_ERR_CUDA 2        /* a CUDA runtime call or kernel launch failed */
+#define WSR_ERR_NO_CLOSURE 3  /* an SR method was requested before wsr_closure_upload */
+
+/* methods: reconstruction weights and closure precision */
+#define WSR_METHOD_JS 0       /* WENO5-JS, eps 1e-6, p 2 */
+#define WSR_METHOD_SR_F64 1   /* WENO5-SR, FP64 MLP (REFSYM) */
+#define WSR_METHOD_SR_F32 2   /* WENO5-SR, FP32 MLP, FP64 elsewhere (MIXED) */
+#define WSR_METHOD_SR_BF16 3  /* WENO5-SR, BF16 inputs/parameters/activations, FP32 accumulation */
+
+/* boundaries */
+#define WSR_BC_TRANSMISSIVE 0
+#define WSR_BC_PERIODIC 1
+
+/* interface fluxes */
+#define WSR_FLUX_HLLC 0
+#define WSR_FLUX_FORCE 1
+
+/* options bitmask */
+#define WSR_OPT_ENO_CUTOFF 1  /* the reference's eno_cutoff flag (4e-7), off in all paper runs */
+#define WSR_OPT_JS_FALLBACK 2 /* per-stencil WENO5-JS weights when the closure is non-finite, and per
+                                 face when an SR face state has rho <= 0 or p <= 0 */
+
+typedef struct wsr_ctx wsr_ctx;
+
+/* Create a context bound to CUDA device `device`. */
+int wsr_ctx_create(int device, wsr_ctx **out);
+void wsr_ctx_destroy(wsr_ctx *ctx);
+/* Message of the last failed call on this context (static storage inside the context). */
+const char *wsr_last_error(const wsr_ctx *ctx);
+
+/* Closure parameters: `packed` is a HOST array of n = 189 values in the order
+ * w1[5][10] b1[10] w2[10][6] b2[6] w3[6][6] b3[6] w4[6][3] b4[3] ([in][out] row-major, the .npz
+ * arrays without their leading dimension). The FP64, FP32 and BF16 methods use the values rounded
+ * to their precision. `kind` must be 5 (WENO5). */
+int wsr_closure_upload(wsr_ctx *ctx, int kind, const double *packed, int n);
+
+/* Bytes of device workspace the 2D functions need for an nx x ny interior. */
+size_t wsr_euler2d_workspace_bytes(int nx, int ny);
+
+/* One SSPRK3 stage (rk = 1, 2, 3): writes the interior of u_out from u_stage and u0
+ * (rk 1: rhs; rk 2: 3/4 u0 + 1/4 rhs; rk 3: 1/3 u0 + 2/3 rhs). dt is a host value. */
+int wsr_euler2d_stage(wsr_ctx *ctx, const double *u_stage, const double *u0, double *u_out, int nx, int ny,
+                      double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux,
+                      int opts, void *workspace, size_t workspace_bytes, void *stream);
+
+/* max over the interior of max(|u|+c, |v|+c), rho and p floored at 1e-15. Synchronises `stream`
+ * and writes the host value. */
+int wsr_euler2d_max_speed(wsr_ctx *ctx, const double *u, int nx, int ny, double gamma, double *out_host,
+                          void *workspace, size_t workspace_bytes, void *stream);
+
+/* Time loop of run_to_time with dt, t and the stop test kept on the device.
+ * u[4] are four padded state buffers: u[0] holds the initial state on entry, u[1], u[2] are stage
+ * buffers, u[3] the swap partner of u[0]. Step s advances from u[0] to u[3] when s is even and from
+ * u[3] to u[0] when it is odd; *final_slot (0 or 3) says which holds the result.
+ * The loop starts at time t_start (0 for a fresh run; a resumed run passes the time reached).
+ * t_end: stop when t >= t_end - 1e-14 (the last dt is clipped). fixed_steps > 0 instead runs exactly
+ * that many full CFL steps. check_health != 0 stops after step 1 (and every check_interval steps when
+ * check_interval > 0) if the state holds a NaN or p <= 0. dts_host (capacity max_steps) receives each
+ * step's dt; the loop also stops at max_steps. */
+int wsr_euler2d_run(wsr_ctx *ctx, double *const u[4], int nx, int ny, double dx, double dy, double gamma,
+                    double cfl, double t_start, double t_end, int method, int bc, int flux, int opts, int check_health,
+                    int check_interval, int fixed_steps, int max_steps, double *dts_host, int *steps_out,
+                    double *t_out, int *final_slot, int *fallbacks_out, void *workspace, size_t workspace_bytes,
+                    void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WSR_H */

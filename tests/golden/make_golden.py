@@ -31,8 +31,8 @@ sys.path.insert(0, str(HERE))
 import warp_shim  # noqa: E402
 
 PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")
-MODEL64 = HERE / "models" / "weno5_sr_fp64_step012250.npz"
-MODEL32 = HERE / "models" / "weno5_sr_fp32_step016500.npz"
+MODEL64 = HERE.parents[1] / "weno_sr_publishing_b200" / "models" / "weno5_sr_fp64_step012250.npz"
+MODEL32 = HERE.parents[1] / "weno_sr_publishing_b200" / "models" / "weno5_sr_fp32_step016500.npz"
 
 
 def _load(path: Path, dtype) -> dict:
@@ -221,7 +221,7 @@ def gen_mlp_golden(reference: Path) -> dict:
     m5f = mixed.load_checkpoint(MODEL32, "cpu").eval()
     sys.path.remove(str(fast_dir))
     w7 = importlib.import_module("teacherfree_lab_weno7_rk4_distance_balanced_fast.weno7_core")
-    m7 = w7.load_checkpoint(HERE / "models" / "weno7_sr_fp64_step016750.npz", "cpu").eval()
+    m7 = w7.load_checkpoint(HERE.parents[1] / "weno_sr_publishing_b200" / "models" / "weno7_sr_fp64_step016750.npz", "cpu").eval()
     with torch.no_grad():
         f5 = torch.tensor(features5)
         f7 = torch.tensor(features7)

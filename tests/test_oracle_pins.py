@@ -15,8 +15,9 @@ import pytest
 from oracle import oracle as O
 
 G = Path(__file__).resolve().parent / "golden"
-P64 = dict(np.load(G / "models" / "weno5_sr_fp64_step012250.npz"))
-P32 = dict(np.load(G / "models" / "weno5_sr_fp32_step016500.npz"))
+MODELS = Path(__file__).resolve().parents[1] / "weno_sr_publishing_b200" / "models"
+P64 = dict(np.load(MODELS / "weno5_sr_fp64_step012250.npz"))
+P32 = dict(np.load(MODELS / "weno5_sr_fp32_step016500.npz"))
 
 # SHA-256 values published in the reference's models/MODEL_CARD.md
 MODEL_SHA = {
@@ -28,7 +29,7 @@ MODEL_SHA = {
 
 @pytest.mark.parametrize("name", sorted(MODEL_SHA))
 def test_checkpoint_fixture_hashes(name):
-    digest = hashlib.sha256((G / "models" / name).read_bytes()).hexdigest()
+    digest = hashlib.sha256((MODELS / name).read_bytes()).hexdigest()
     assert digest == MODEL_SHA[name]
 
 

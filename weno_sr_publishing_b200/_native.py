@@ -1,0 +1,123 @@
+"""ctypes binding of libwsr.so (the C ABI declared in include/wsr.h).
+
+The CUDA library is the only compute path: importing this module fails loudly when libwsr.so is
+missing, and every call raises on a non-zero status. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libwsr.so"
+
+WSR_OK, WSR_ERR_ARG, WSR_ERR_CUDA, WSR_ERR_NO_CLOSURE = 0, 1, 2, 3
+METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3}
+BC = {"transmissive": 0, "periodic": 1}
+FLUX = {"hllc": 0, "force": 1}
+OPT_ENO_CUTOFF, OPT_JS_FALLBACK = 1, 2
+N_PARAMS5 = 189
+PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")
+
+_lib = None
+_lock = threading.Lock()
+
+
+class NativeLibraryMissing(ImportError):
+    pass
+
+
+def lib() -> C.CDLL:
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise NativeLibraryMissing(
+                    f"{LIB_PATH} is not built; run `python -m weno_sr_publishing_b200.build` (needs nvcc)")
+            L = C.CDLL(str(LIB_PATH))
+            vp, i, d, sz = C.c_void_p, C.c_int, C.c_double, C.c_size_t
+            L.wsr_ctx_create.argtypes = [i, C.POINTER(vp)]
+            L.wsr_ctx_destroy.argtypes = [vp]
+            L.wsr_ctx_destroy.restype = None
+            L.wsr_last_error.argtypes = [vp]
+            L.wsr_last_error.restype = C.c_char_p
+            L.wsr_closure_upload.argtypes = [vp, i, C.POINTER(d), i]
+            L.wsr_euler2d_workspace_bytes.argtypes = [i, i]
+            L.wsr_euler2d_workspace_bytes.restype = sz
+            L.wsr_euler2d_stage.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, vp, sz, vp]
+            L.wsr_euler2d_max_speed.argtypes = [vp, vp, i, i, d, C.POINTER(d), vp, sz, vp]
+            L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
+                                          C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
+                                          vp, sz, vp]
+            _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
+            "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run"]
+
+
+def pack_params(params) -> np.ndarray:
+    """w1..b4 (numpy, torch, leading dim 1 allowed) -> 189 FP64 values in the packed layout."""
+    arrs = []
+    for k in PARAM_NAMES:
+        v = params[k]
+        if hasattr(v, "detach"):
+            v = v.detach().cpu().numpy()
+        arrs.append(np.asarray(v, dtype=np.float64).reshape(-1))
+    out = np.ascontiguousarray(np.concatenate(arrs))
+    if out.size != N_PARAMS5:
+        raise ValueError(f"expected {N_PARAMS5} WENO5 parameters, got {out.size}")
+    return out
+
+
+class Context:
+    """One libwsr context per CUDA device (holds the uploaded closure parameters)."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        rc = lib().wsr_ctx_create(device, C.byref(h))
+        if rc != WSR_OK:
+            raise RuntimeError(f"wsr_ctx_create failed with status {rc}")
+        self.handle = h
+        self._closure_key = None
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and _lib is not None:
+            _lib.wsr_ctx_destroy(h)
+            self.handle = None
+
+    def check(self, rc: int) -> None:
+        if rc == WSR_OK:
+            return
+        msg = lib().wsr_last_error(self.handle).decode(errors="replace")
+        if rc == WSR_ERR_ARG:
+            raise ValueError(msg)
+        raise RuntimeError(f"libwsr status {rc}: {msg}")
+
+    def upload_closure(self, packed: np.ndarray) -> None:
+        packed = np.ascontiguousarray(packed, dtype=np.float64)
+        key = packed.tobytes()
+        if key == self._closure_key:
+            return
+        self.check(lib().wsr_closure_upload(self.handle, 5, packed.ctypes.data_as(C.POINTER(C.c_double)),
+                                            int(packed.size)))
+        self._closure_key = key
+
+
+_contexts: dict[int, Context] = {}
+
+
+def context(device: int = 0) -> Context:
+    with _lock:
+        if device not in _contexts:
+            _contexts[device] = None  # placeholder to keep the lock scope simple
+    if _contexts[device] is None:
+        _contexts[device] = Context(device)
+    return _contexts[device]

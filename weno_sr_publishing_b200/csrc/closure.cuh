@@ -1,0 +1,340 @@
+// WENO5 weights: Jiang-Shu and the reflection-averaged MLP smoothness-ratio closure (WENO5-SR).
+//
+// Reference (code/snapshot/):
+//   warp_weno5_helpers.py (wh) 240-242 safe_rcp, 438-446 stencil_2d, 512-570 weno5_lr_value,
+//       798-873 stencil_gauss / weno5_gauss_lr_value (JS, eps 1e-6, p 2);
+//   teacherfree_lab_weno5_v20_distance_balanced/weno5_rk3_diff_v20_deploy.py (DEPLOY)
+//       76-120 sensors and features, 123-131 plateau test, 134-151 linear weights,
+//       154-205 MLP 5->10->6->6->3 with swish, 6 tanh(raw/6) and softmax, 208-279 mlp_weights;
+//   teacherfree_lab_weno5_v20_distance_balanced_mlp_f32_fast/warp_mlp_f32/weno5_rk3_diff_mlp_f32.py
+//       (F32CORE) 94-283: FP32 inputs/parameters/activations, ratios cast back to FP64.
+//
+// Differences in structure (not in results beyond rounding):
+//   * the reflected stencil's features are formed as the permutation (d2, d1, d0, gamma, scale) of
+//     the direct ones instead of being recomputed from the reversed stencil;
+//   * ratios are computed once per stencil and shared by every head that uses the stencil (the two
+//     Gauss points of a transverse reconstruction);
+//   * the two MLP passes (direct and reflected) are evaluated together for instruction-level
+//     parallelism.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace wsr {
+
+enum Method { M_JS = 0, M_SR64 = 1, M_SR32 = 2, M_SRBF16 = 3 };
+
+// Packed parameters, layout w1[5][10] b1[10] w2[10][6] b2[6] w3[6][6] b3[6] w4[6][3] b4[3].
+constexpr int kW1 = 0, kB1 = 50, kW2 = 60, kB2 = 120, kW3 = 126, kB3 = 162, kW4 = 168, kB4 = 186;
+constexpr int kParams5 = 189;
+
+struct Mlp5d {
+  double p[kParams5];
+};
+struct Mlp5f {
+  float p[kParams5];
+};
+struct NoParams {};
+
+template <int M>
+struct ClosureParams {
+  using type = NoParams;
+};
+template <>
+struct ClosureParams<M_SR64> {
+  using type = Mlp5d;
+};
+template <>
+struct ClosureParams<M_SR32> {
+  using type = Mlp5f;
+};
+template <>
+struct ClosureParams<M_SRBF16> {
+  using type = Mlp5f;  // pre-rounded to bfloat16 on upload
+};
+
+// Heads: 0 face lr=1 (x_{i+1/2}^-), 1 face lr=2 (x_{i-1/2}^+), 2 Gauss loca=1, 3 Gauss loca=2.
+struct Lin3 {
+  double d0, d1, d2;
+};
+
+__device__ __forceinline__ Lin3 linear_weights(int head) {
+  // (210 +- sqrt 3)/1080 evaluated in FP64 exactly as the reference does at run time.
+  const double r3 = 1.7320508075688772;  // sqrt(3.0) correctly rounded
+  if (head == 0) return {0.1, 0.6, 0.3};
+  if (head == 1) return {0.3, 0.6, 0.1};
+  if (head == 2) return {(210.0 + r3) / 1080.0, 11.0 / 18.0, (210.0 - r3) / 1080.0};
+  return {(210.0 - r3) / 1080.0, 11.0 / 18.0, (210.0 + r3) / 1080.0};
+}
+
+// Candidate values of the three sub-stencils for a head (wh stencil_2d / stencil_gauss literals).
+__device__ __forceinline__ void candidates(const double q[5], int head, double s[3]) {
+  if (head == 0) {
+    s[0] = (1.0 / 3.0) * q[0] - (7.0 / 6.0) * q[1] + (11.0 / 6.0) * q[2];
+    s[1] = (-1.0 / 6.0) * q[1] + (5.0 / 6.0) * q[2] + (1.0 / 3.0) * q[3];
+    s[2] = (1.0 / 3.0) * q[2] + (5.0 / 6.0) * q[3] - (1.0 / 6.0) * q[4];
+  } else if (head == 1) {
+    s[0] = (-1.0 / 6.0) * q[0] + (5.0 / 6.0) * q[1] + (1.0 / 3.0) * q[2];
+    s[1] = (1.0 / 3.0) * q[1] + (5.0 / 6.0) * q[2] - (1.0 / 6.0) * q[3];
+    s[2] = (11.0 / 6.0) * q[2] - (7.0 / 6.0) * q[3] + (1.0 / 3.0) * q[4];
+  } else if (head == 2) {
+    s[0] = -0.144337567297407 * q[0] + 0.577350269189626 * q[1] + 0.566987298107780 * q[2];
+    s[1] = 0.144337567297406 * q[1] + q[2] - 0.144337567297407 * q[3];
+    s[2] = 1.433012701892220 * q[2] - 0.577350269189626 * q[3] + 0.144337567297406 * q[4];
+  } else {
+    s[0] = 0.144337567297406 * q[0] - 0.577350269189626 * q[1] + 1.433012701892220 * q[2];
+    s[1] = -0.144337567297407 * q[1] + q[2] + 0.144337567297406 * q[3];
+    s[2] = 0.566987298107781 * q[2] + 0.577350269189625 * q[3] - 0.144337567297406 * q[4];
+  }
+}
+
+// Per-stencil state shared by all heads: JS reciprocal betas, or SR averaged ratios.
+struct StencilW {
+  double a0, a1, a2;  // JS: 1/(1e-6+beta_k); SR: 1/(3 r_k + 1e-12)
+  bool linear;        // SR plateau: use the linear weights
+};
+
+__device__ __forceinline__ StencilW js_stencil(const double q[5]) {
+  double t2 = q[2] - 2.0 * q[3] + q[4], u2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
+  double t1 = q[1] - 2.0 * q[2] + q[3], u1 = q[1] - q[3];
+  double t0 = q[0] - 2.0 * q[1] + q[2], u0 = q[0] - 4.0 * q[1] + 3.0 * q[2];
+  double b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * u2 * u2;
+  double b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * u1 * u1;
+  double b0 = (13.0 / 12.0) * t0 * t0 + 0.25 * u0 * u0;
+  StencilW s;
+  s.a0 = 1.0 / (1.0e-6 + b0);
+  s.a1 = 1.0 / (1.0e-6 + b1);
+  s.a2 = 1.0 / (1.0e-6 + b2);
+  s.linear = false;
+  return s;
+}
+
+// JS: w_k = d_k rcp_k^2 / sum   (wh:557-568)
+__device__ __forceinline__ void js_head_weights(const StencilW& s, const Lin3& d, double w[3]) {
+  double a0 = d.d0 * s.a0 * s.a0, a1 = d.d1 * s.a1 * s.a1, a2 = d.d2 * s.a2 * s.a2;
+  double sum = a0 + a1 + a2;
+  w[0] = a0 / sum;
+  w[1] = a1 / sum;
+  w[2] = a2 / sum;
+}
+
+// SR: alpha_k = d_k / (3 r_k + 1e-12)^2; w = alpha / max(sum, 1e-300); optional ENO cutoff
+// (DEPLOY:240-277).
+__device__ __forceinline__ void sr_head_weights(const StencilW& s, const Lin3& d, bool eno_cutoff, double w[3]) {
+  if (s.linear) {
+    w[0] = d.d0;
+    w[1] = d.d1;
+    w[2] = d.d2;
+    return;
+  }
+  double a0 = d.d0 * (s.a0 * s.a0), a1 = d.d1 * (s.a1 * s.a1), a2 = d.d2 * (s.a2 * s.a2);
+  double inv = 1.0 / fmax(a0 + a1 + a2, 1.0e-300);
+  w[0] = a0 * inv;
+  w[1] = a1 * inv;
+  w[2] = a2 * inv;
+  if (eno_cutoff) {
+    const double cut = 4.0e-7;
+    double p0 = w[0] <= cut ? 0.0 : 1.0, p1 = w[1] <= cut ? 0.0 : 1.0, p2 = w[2] <= cut ? 0.0 : 1.0;
+    double ci = 1.0 / fmax(p0 * w[0] + p1 * w[1] + p2 * w[2], 1.0e-300);
+    w[0] = p0 * w[0] * ci;
+    w[1] = p1 * w[1] * ci;
+    w[2] = p2 * w[2] * ci;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Features
+// ---------------------------------------------------------------------------------------------
+struct Sensors {
+  double d0, d1, d2, gamma, dmax, qscale;
+};
+
+__device__ __forceinline__ Sensors raw_sensors(const double q[5]) {
+  double d20 = q[0] - 2.0 * q[1] + q[2], d21 = q[1] - 2.0 * q[2] + q[3], d22 = q[2] - 2.0 * q[3] + q[4];
+  Sensors s;
+  s.d0 = (13.0 / 12.0) * fabs(d20) + 0.25 * fabs(q[0] - 4.0 * q[1] + 3.0 * q[2]);
+  s.d1 = (13.0 / 12.0) * fabs(d21) + 0.25 * fabs(q[1] - q[3]);
+  s.d2 = (13.0 / 12.0) * fabs(d22) + 0.25 * fabs(3.0 * q[2] - 4.0 * q[3] + q[4]);
+  const double eps = 1.0e-15;
+  double g0 = fabs(d20) / (fabs(q[1] - q[0]) + fabs(q[2] - q[1]) + eps);
+  double g1 = fabs(d21) / (fabs(q[2] - q[1]) + fabs(q[3] - q[2]) + eps);
+  double g2 = fabs(d22) / (fabs(q[3] - q[2]) + fabs(q[4] - q[3]) + eps);
+  s.gamma = fmin(1.0, fmax(fmax(g0, g1), g2));
+  s.dmax = fmax(fmax(s.d0, s.d1), s.d2);
+  double qs = fmax(fmax(fmax(fabs(q[0]), fabs(q[1])), fmax(fabs(q[2]), fabs(q[3]))), fabs(q[4]));
+  s.qscale = fmax(qs, 1.0);
+  return s;
+}
+
+// Direct features (d0, d1, d2)/dmax, gamma, clip((log10(dmax/qscale) + 4)/4, 0, 1).
+__device__ __forceinline__ void features64(const Sensors& s, double f[5]) {
+  double inv = 1.0 / fmax(s.dmax, 1.0e-15);
+  double rel = fmax(s.dmax / s.qscale, 1.0e-30);
+  double l10 = log(rel) / 2.302585092994046;  // log(10.0) correctly rounded
+  double sc = fmin(1.0, fmax(0.0, (l10 + 4.0) / 4.0));
+  f[0] = s.d0 * inv;
+  f[1] = s.d1 * inv;
+  f[2] = s.d2 * inv;
+  f[3] = s.gamma;
+  f[4] = sc;
+}
+
+// ---------------------------------------------------------------------------------------------
+// MLP 5->10->6->6->3, two inputs at once (direct and reflected). Parameters are read from kernel
+// parameter space (constant bank), every lane the same address, so they are broadcast operands.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T swish(T z);
+template <>
+__device__ __forceinline__ double swish<double>(double z) {
+  return z / (1.0 + exp(-z));
+}
+template <>
+__device__ __forceinline__ float swish<float>(float z) {
+  return z / (1.0f + expf(-z));
+}
+
+__device__ __forceinline__ double tanh_t(double x) { return tanh(x); }
+__device__ __forceinline__ float tanh_t(float x) { return tanhf(x); }
+__device__ __forceinline__ double exp_t(double x) { return exp(x); }
+__device__ __forceinline__ float exp_t(float x) { return expf(x); }
+
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+template <typename T, bool BF16>
+__device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5], const T xb[5], T ra[3], T rb[3]) {
+  T ha[10], hb[10];
+#pragma unroll
+  for (int o = 0; o < 10; ++o) {
+    T za = P[kB1 + o], zb = P[kB1 + o];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      za = za + xa[k] * P[kW1 + k * 10 + o];
+      zb = zb + xb[k] * P[kW1 + k * 10 + o];
+    }
+    ha[o] = swish<T>(za);
+    hb[o] = swish<T>(zb);
+    if (BF16) {
+      ha[o] = bf16r(ha[o]);
+      hb[o] = bf16r(hb[o]);
+    }
+  }
+  T ga[6], gb[6];
+#pragma unroll
+  for (int o = 0; o < 6; ++o) {
+    T za = P[kB2 + o], zb = P[kB2 + o];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+      za = za + ha[k] * P[kW2 + k * 6 + o];
+      zb = zb + hb[k] * P[kW2 + k * 6 + o];
+    }
+    ga[o] = swish<T>(za);
+    gb[o] = swish<T>(zb);
+    if (BF16) {
+      ga[o] = bf16r(ga[o]);
+      gb[o] = bf16r(gb[o]);
+    }
+  }
+  T ka[6], kb[6];
+#pragma unroll
+  for (int o = 0; o < 6; ++o) {
+    T za = P[kB3 + o], zb = P[kB3 + o];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      za = za + ga[k] * P[kW3 + k * 6 + o];
+      zb = zb + gb[k] * P[kW3 + k * 6 + o];
+    }
+    ka[o] = swish<T>(za);
+    kb[o] = swish<T>(zb);
+    if (BF16) {
+      ka[o] = bf16r(ka[o]);
+      kb[o] = bf16r(kb[o]);
+    }
+  }
+  T ba[3], bb[3];
+#pragma unroll
+  for (int o = 0; o < 3; ++o) {
+    T za = P[kB4 + o], zb = P[kB4 + o];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      za = za + ka[k] * P[kW4 + k * 3 + o];
+      zb = zb + kb[k] * P[kW4 + k * 3 + o];
+    }
+    ba[o] = T(6) * tanh_t(za / T(6));
+    bb[o] = T(6) * tanh_t(zb / T(6));
+  }
+  T ma = ba[0] > ba[1] ? ba[0] : ba[1];
+  ma = ma > ba[2] ? ma : ba[2];
+  T mb = bb[0] > bb[1] ? bb[0] : bb[1];
+  mb = mb > bb[2] ? mb : bb[2];
+  T ea0 = exp_t(ba[0] - ma), ea1 = exp_t(ba[1] - ma), ea2 = exp_t(ba[2] - ma);
+  T eb0 = exp_t(bb[0] - mb), eb1 = exp_t(bb[1] - mb), eb2 = exp_t(bb[2] - mb);
+  T ia = T(1) / (ea0 + ea1 + ea2), ib = T(1) / (eb0 + eb1 + eb2);
+  ra[0] = ea0 * ia;
+  ra[1] = ea1 * ia;
+  ra[2] = ea2 * ia;
+  rb[0] = eb0 * ib;
+  rb[1] = eb1 * ib;
+  rb[2] = eb2 * ib;
+}
+
+// Closure for one stencil: averaged ratios -> reciprocal scaled betas, or the plateau flag.
+// Returns false when the ratios are not finite (the caller may fall back to JS weights).
+template <int M>
+__device__ __forceinline__ bool sr_stencil(const double q[5], const typename ClosureParams<M>::type& P,
+                                           StencilW& out) {
+  Sensors s = raw_sensors(q);
+  out.linear = s.dmax <= 1.0e-13 * s.qscale;
+  if (out.linear) {
+    out.a0 = out.a1 = out.a2 = 0.0;
+    return true;
+  }
+  double f[5];
+  features64(s, f);
+  double r0, r1, r2;  // 0.5 (M(x) + P3 M(P5 x))
+  if (M == M_SR64) {
+    double xa[5] = {f[0], f[1], f[2], f[3], f[4]};
+    double xb[5] = {f[2], f[1], f[0], f[3], f[4]};
+    double ra[3], rb[3];
+    mlp_pair<double, false>(reinterpret_cast<const double*>(&P), xa, xb, ra, rb);
+    r0 = 0.5 * (ra[0] + rb[2]);
+    r1 = 0.5 * (ra[1] + rb[1]);
+    r2 = 0.5 * (ra[2] + rb[0]);
+  } else {
+    constexpr bool B = M == M_SRBF16;
+    float xa[5], xb[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) xa[k] = B ? bf16r((float)f[k]) : (float)f[k];
+    xb[0] = xa[2];
+    xb[1] = xa[1];
+    xb[2] = xa[0];
+    xb[3] = xa[3];
+    xb[4] = xa[4];
+    float ra[3], rb[3];
+    mlp_pair<float, B>(reinterpret_cast<const float*>(&P), xa, xb, ra, rb);
+    r0 = 0.5 * ((double)ra[0] + (double)rb[2]);
+    r1 = 0.5 * ((double)ra[1] + (double)rb[1]);
+    r2 = 0.5 * ((double)ra[2] + (double)rb[0]);
+  }
+  out.a0 = 1.0 / (3.0 * r0 + 1.0e-12);
+  out.a1 = 1.0 / (3.0 * r1 + 1.0e-12);
+  out.a2 = 1.0 / (3.0 * r2 + 1.0e-12);
+  return isfinite(out.a0) && isfinite(out.a1) && isfinite(out.a2);
+}
+
+// Weights of one stencil for one head, whatever the method.
+template <int M>
+__device__ __forceinline__ void head_weights(const StencilW& s, int head, bool eno_cutoff, double w[3]) {
+  Lin3 d = linear_weights(head);
+  if (M == M_JS)
+    js_head_weights(s, d, w);
+  else
+    sr_head_weights(s, d, eno_cutoff, w);
+}
+
+__device__ __forceinline__ double combine(const double w[3], const double s[3]) {
+  return w[0] * s[0] + w[1] * s[1] + w[2] * s[2];
+}
+
+}  // namespace wsr

@@ -1,0 +1,391 @@
+// extern "C" entry points of libwsr.so (declared in include/wsr.h).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "../../include/wsr.h"
+#include "euler2d.cuh"
+
+using namespace wsr;
+
+struct wsr_ctx {
+  int device;
+  bool have_closure;
+  Mlp5d p64;
+  Mlp5f p32;
+  Mlp5f pbf16;
+  char err[512];
+  double* host_pinned;  // small pinned mailbox for control-block reads
+};
+
+namespace {
+
+int fail(wsr_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+    va_end(ap);
+  }
+  return code;
+}
+
+#define WSR_CUDA(ctx, call)                                                                    \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(ctx, WSR_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define WSR_LAUNCHED(ctx, what)                                                                \
+  do {                                                                                         \
+    cudaError_t e_ = cudaGetLastError();                                                       \
+    if (e_ != cudaSuccess) return fail(ctx, WSR_ERR_CUDA, "launch %s: %s", what, cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr size_t kAlign = 256;
+constexpr int kDtsRing = 64;  // dt records kept on the device between host polls
+
+size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+bool misaligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; }
+
+struct Ws2d {
+  StepCtl* ctl;
+  int* fallbacks;
+  double* dts;  // ring of kDtsRing
+  double *xl, *xr, *yl, *yr, *fx, *fy;
+};
+
+size_t cells_bytes(size_t n) { return align_up(n * 4 * sizeof(double)); }
+
+size_t ws_bytes(int nx, int ny) {
+  size_t b = align_up(sizeof(StepCtl)) + align_up(sizeof(int)) + align_up(kDtsRing * sizeof(double));
+  b += 2 * cells_bytes((size_t)(ny + 6) * (nx + 2));
+  b += 2 * cells_bytes((size_t)(ny + 2) * (nx + 6));
+  b += cells_bytes((size_t)ny * (nx + 1));
+  b += cells_bytes((size_t)(ny + 1) * nx);
+  return b;
+}
+
+Ws2d carve(void* base, int nx, int ny) {
+  char* p = static_cast<char*>(base);
+  Ws2d w;
+  w.ctl = reinterpret_cast<StepCtl*>(p);
+  p += align_up(sizeof(StepCtl));
+  w.fallbacks = reinterpret_cast<int*>(p);
+  p += align_up(sizeof(int));
+  w.dts = reinterpret_cast<double*>(p);
+  p += align_up(kDtsRing * sizeof(double));
+  w.xl = reinterpret_cast<double*>(p);
+  p += cells_bytes((size_t)(ny + 6) * (nx + 2));
+  w.xr = reinterpret_cast<double*>(p);
+  p += cells_bytes((size_t)(ny + 6) * (nx + 2));
+  w.yl = reinterpret_cast<double*>(p);
+  p += cells_bytes((size_t)(ny + 2) * (nx + 6));
+  w.yr = reinterpret_cast<double*>(p);
+  p += cells_bytes((size_t)(ny + 2) * (nx + 6));
+  w.fx = reinterpret_cast<double*>(p);
+  p += cells_bytes((size_t)ny * (nx + 1));
+  w.fy = reinterpret_cast<double*>(p);
+  return w;
+}
+
+int check_2d(wsr_ctx* ctx, int nx, int ny, int method, int bc, int flux, void* ws, size_t wsb) {
+  if (!ctx) return WSR_ERR_ARG;
+  if (nx < 3 || ny < 3) return fail(ctx, WSR_ERR_ARG, "nx and ny must be >= 3 (got %d, %d)", nx, ny);
+  if ((long long)(nx + 6) * (ny + 6) > (1ll << 31) / 4)
+    return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
+  if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC) return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
+  if (flux != WSR_FLUX_HLLC && flux != WSR_FLUX_FORCE) return fail(ctx, WSR_ERR_ARG, "bad flux %d", flux);
+  if (method != WSR_METHOD_JS && !ctx->have_closure)
+    return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before wsr_closure_upload");
+  if (!ws) return fail(ctx, WSR_ERR_ARG, "workspace is NULL");
+  if (reinterpret_cast<uintptr_t>(ws) % kAlign) return fail(ctx, WSR_ERR_ARG, "workspace must be 256-byte aligned");
+  if (wsb < ws_bytes(nx, ny))
+    return fail(ctx, WSR_ERR_ARG, "workspace too small: %zu < %zu bytes", wsb, ws_bytes(nx, ny));
+  return WSR_OK;
+}
+
+template <int M>
+const typename ClosureParams<M>::type& params_of(const wsr_ctx* ctx);
+template <>
+const NoParams& params_of<M_JS>(const wsr_ctx*) {
+  static const NoParams np{};
+  return np;
+}
+template <>
+const Mlp5d& params_of<M_SR64>(const wsr_ctx* ctx) {
+  return ctx->p64;
+}
+template <>
+const Mlp5f& params_of<M_SR32>(const wsr_ctx* ctx) {
+  return ctx->p32;
+}
+template <>
+const Mlp5f& params_of<M_SRBF16>(const wsr_ctx* ctx) {
+  return ctx->pbf16;
+}
+
+struct StageArgs {
+  const double* u_stage;
+  const double* u0;
+  double* u_out;
+  int nx, ny, bc, flux, opts, rk;
+  double dx, dy, g;
+};
+
+// One stage = 5 launches. dt/dx and dt/dy are read from ws.ctl on the device.
+template <int M>
+int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
+  const auto& P = params_of<M>(ctx);
+  const dim3 blk(64, 2);
+  {
+    dim3 grd((a.nx + 2 + blk.x - 1) / blk.x, (a.ny + 5 + blk.y - 1) / blk.y);
+    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, P);
+    WSR_LAUNCHED(ctx, "k_normal<x>");
+  }
+  {
+    dim3 grd((a.nx + 5 + blk.x - 1) / blk.x, (a.ny + 2 + blk.y - 1) / blk.y);
+    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, P);
+    WSR_LAUNCHED(ctx, "k_normal<y>");
+  }
+  {
+    dim3 grd((a.nx + 1 + blk.x - 1) / blk.x, (a.ny + blk.y - 1) / blk.y);
+    k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, P);
+    WSR_LAUNCHED(ctx, "k_flux<x>");
+  }
+  {
+    dim3 grd((a.nx + blk.x - 1) / blk.x, (a.ny + 1 + blk.y - 1) / blk.y);
+    k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, P);
+    WSR_LAUNCHED(ctx, "k_flux<y>");
+  }
+  {
+    dim3 grd((a.nx + 255) / 256, a.ny);
+    k_update<<<grd, 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk, a.g, w.ctl);
+    WSR_LAUNCHED(ctx, "k_update");
+  }
+  return WSR_OK;
+}
+
+int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
+  switch (method) {
+    case WSR_METHOD_JS:
+      return launch_stage<M_JS>(ctx, a, w, st);
+    case WSR_METHOD_SR_F64:
+      return launch_stage<M_SR64>(ctx, a, w, st);
+    case WSR_METHOD_SR_F32:
+      return launch_stage<M_SR32>(ctx, a, w, st);
+    default:
+      return launch_stage<M_SRBF16>(ctx, a, w, st);
+  }
+}
+
+__global__ void k_init_ctl(StepCtl* ctl, int* fallbacks, double t_start, double t_end, double dt, double dx, double dy, double cfl,
+                           double hmin, int check_health, int check_interval, int max_steps) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  ctl->t = t_start;
+  ctl->t_end = t_end;
+  ctl->dt = dt;
+  ctl->dt_dx = dt / dx;
+  ctl->dt_dy = dt / dy;
+  ctl->max_speed_bits = 0ull;
+  ctl->steps = 0;
+  ctl->done = 0;
+  ctl->health_bad = 0;
+  ctl->fallbacks = 0;
+  ctl->check_health = check_health;
+  ctl->check_interval = check_interval;
+  ctl->max_steps = max_steps;
+  ctl->cfl = cfl;
+  ctl->hmin = hmin;
+  *fallbacks = 0;
+}
+
+// Variant of k_step_begin that writes into a ring of kDtsRing records.
+__global__ void k_step_begin_ring(StepCtl* ctl, double* ring) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (ctl->done) return;
+  if (ctl->check_health && ctl->health_bad &&
+      (ctl->steps == 1 || (ctl->check_interval > 0 && ctl->steps % ctl->check_interval == 0))) {
+    ctl->done = 1;
+    return;
+  }
+  if (!(ctl->t < ctl->t_end - 1.0e-14) || ctl->steps >= ctl->max_steps) {
+    ctl->done = 1;
+    return;
+  }
+  double ms = __longlong_as_double((long long)ctl->max_speed_bits);
+  double dt = ms < 1.0e-15 ? 1.0e10 : ctl->cfl * ctl->hmin / ms;
+  double rem = ctl->t_end - ctl->t;
+  dt = dt < rem ? dt : rem;
+  if (!isfinite(dt) || dt <= 0.0) {
+    ctl->done = 1;
+    return;
+  }
+  ctl->dt = dt;
+  ctl->max_speed_bits = 0ull;
+  ctl->health_bad = 0;
+  ring[ctl->steps % kDtsRing] = dt;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wsr_ctx_create(int device, wsr_ctx** out) {
+  if (!out) return WSR_ERR_ARG;
+  *out = nullptr;
+  wsr_ctx* ctx = new (std::nothrow) wsr_ctx();
+  if (!ctx) return WSR_ERR_ARG;
+  std::memset(ctx, 0, sizeof(*ctx));
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&ctx->host_pinned), 4096);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return WSR_ERR_CUDA;
+  }
+  *out = ctx;
+  return WSR_OK;
+}
+
+void wsr_ctx_destroy(wsr_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  delete ctx;
+}
+
+const char* wsr_last_error(const wsr_ctx* ctx) { return ctx ? ctx->err : "null context"; }
+
+int wsr_closure_upload(wsr_ctx* ctx, int kind, const double* packed, int n) {
+  if (!ctx) return WSR_ERR_ARG;
+  if (kind != 5) return fail(ctx, WSR_ERR_ARG, "closure kind %d not supported by the 2D path (5 = WENO5)", kind);
+  if (!packed || n != kParams5) return fail(ctx, WSR_ERR_ARG, "expected %d WENO5 parameters, got %d", kParams5, n);
+  for (int k = 0; k < kParams5; ++k) {
+    ctx->p64.p[k] = packed[k];
+    ctx->p32.p[k] = static_cast<float>(packed[k]);
+    ctx->pbf16.p[k] = __bfloat162float(__float2bfloat16_rn(static_cast<float>(packed[k])));
+  }
+  ctx->have_closure = true;
+  return WSR_OK;
+}
+
+size_t wsr_euler2d_workspace_bytes(int nx, int ny) {
+  if (nx < 1 || ny < 1) return 0;
+  return ws_bytes(nx, ny);
+}
+
+int wsr_euler2d_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, double* u_out, int nx, int ny,
+                      double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux, int opts,
+                      void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (!u_stage || !u0 || !u_out) return fail(ctx, WSR_ERR_ARG, "null state pointer");
+  if (misaligned(u_stage) || misaligned(u0) || misaligned(u_out))
+    return fail(ctx, WSR_ERR_ARG, "state arrays must be 16-byte aligned");
+  if (rk < 1 || rk > 3) return fail(ctx, WSR_ERR_ARG, "rk must be 1, 2 or 3 (got %d)", rk);
+  if (!(dt > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return fail(ctx, WSR_ERR_ARG, "dt, dx, dy must be positive");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
+  WSR_LAUNCHED(ctx, "k_init_ctl");
+  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma};
+  return dispatch_stage(ctx, method, a, w, st);
+}
+
+int wsr_euler2d_max_speed(wsr_ctx* ctx, const double* u, int nx, int ny, double gamma, double* out_host,
+                          void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_2d(ctx, nx, ny, WSR_METHOD_JS, WSR_BC_TRANSMISSIVE, WSR_FLUX_HLLC, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (!u || !out_host) return fail(ctx, WSR_ERR_ARG, "null pointer");
+  if (misaligned(u)) return fail(ctx, WSR_ERR_ARG, "state array must be 16-byte aligned");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  WSR_CUDA(ctx, cudaMemsetAsync(&w.ctl->max_speed_bits, 0, sizeof(unsigned long long), st));
+  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, &w.ctl->max_speed_bits);
+  WSR_LAUNCHED(ctx, "k_max_speed");
+  unsigned long long bits = 0;
+  WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, &w.ctl->max_speed_bits, sizeof(bits), cudaMemcpyDeviceToHost, st));
+  WSR_CUDA(ctx, cudaStreamSynchronize(st));
+  std::memcpy(&bits, ctx->host_pinned, sizeof(bits));
+  double v;
+  std::memcpy(&v, &bits, sizeof(v));
+  *out_host = v;
+  return WSR_OK;
+}
+
+int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx, double dy, double gamma, double cfl,
+                    double t_start, double t_end, int method, int bc, int flux, int opts, int check_health, int check_interval,
+                    int fixed_steps, int max_steps, double* dts_host, int* steps_out, double* t_out, int* final_slot,
+                    int* fallbacks_out, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (!u || !u[0] || !u[1] || !u[2] || !u[3]) return fail(ctx, WSR_ERR_ARG, "null state buffer");
+  if (misaligned(u[0]) || misaligned(u[1]) || misaligned(u[2]) || misaligned(u[3]))
+    return fail(ctx, WSR_ERR_ARG, "state arrays must be 16-byte aligned");
+  if (max_steps < 1) return fail(ctx, WSR_ERR_ARG, "max_steps must be >= 1");
+  if (!(cfl > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return fail(ctx, WSR_ERR_ARG, "cfl, dx, dy must be positive");
+  if (fixed_steps > 0) {
+    t_end = 1.0e300;
+    max_steps = fixed_steps;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  const double hmin = dx < dy ? dx : dy;
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, fixed_steps > 0 ? 0.0 : t_start, t_end, 0.0, dx, dy, cfl, hmin,
+                              check_health, check_interval,
+                              max_steps);
+  WSR_LAUNCHED(ctx, "k_init_ctl");
+  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u[0], nx, ny, gamma, &w.ctl->max_speed_bits);
+  WSR_LAUNCHED(ctx, "k_max_speed");
+  const int batch = 16;  // steps launched between host polls (<= kDtsRing)
+  int host_steps = 0;    // steps the host has launched
+  int seen_steps = 0;    // steps whose dt has been copied out
+  int done = 0;
+  StepCtl snap;
+  while (!done) {
+    for (int b = 0; b < batch; ++b) {
+      const int s = host_steps + b;
+      double* in = (s & 1) ? u[3] : u[0];
+      double* out = (s & 1) ? u[0] : u[3];
+      k_step_begin_ring<<<1, 1, 0, st>>>(w.ctl, w.dts);
+      WSR_LAUNCHED(ctx, "k_step_begin");
+      k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
+      WSR_LAUNCHED(ctx, "k_set_dt_ratios");
+      StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma};
+      StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma};
+      StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma};
+      if ((rc = dispatch_stage(ctx, method, a1, w, st))) return rc;
+      if ((rc = dispatch_stage(ctx, method, a2, w, st))) return rc;
+      if ((rc = dispatch_stage(ctx, method, a3, w, st))) return rc;
+      k_step_end<<<1, 1, 0, st>>>(w.ctl);
+      WSR_LAUNCHED(ctx, "k_step_end");
+    }
+    host_steps += batch;
+    WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, w.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+    WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned + 128, w.dts, kDtsRing * sizeof(double), cudaMemcpyDeviceToHost, st));
+    WSR_CUDA(ctx, cudaStreamSynchronize(st));
+    std::memcpy(&snap, ctx->host_pinned, sizeof(StepCtl));
+    for (int s = seen_steps; s < snap.steps; ++s)
+      if (dts_host && s < max_steps) dts_host[s] = ctx->host_pinned[128 + (s % kDtsRing)];
+    seen_steps = snap.steps;
+    done = snap.done;
+  }
+  int fb = 0;
+  WSR_CUDA(ctx, cudaMemcpy(&fb, w.fallbacks, sizeof(int), cudaMemcpyDeviceToHost));
+  if (steps_out) *steps_out = snap.steps;
+  if (t_out) *t_out = snap.t;
+  if (final_slot) *final_slot = (snap.steps & 1) ? 3 : 0;
+  if (fallbacks_out) *fallbacks_out = fb;
+  return WSR_OK;
+}
+
+}  // extern "C"
