@@ -98,6 +98,35 @@ int wsr_euler2d_run(wsr_ctx *ctx, double *const u[4], int nx, int ny, double dx,
                     double *t_out, int *final_slot, int *fallbacks_out, void *workspace, size_t workspace_bytes,
                     void *stream);
 
+/* ---- measurement hooks (no counterpart in the reference, which times whole runs with
+ * time.perf_counter in for_paper_results/run_weno5_timing.py:111-140) ---- */
+
+/* Kernel classes reported by wsr_profile_read. */
+#define WSR_PROF_NORMAL_X 0
+#define WSR_PROF_NORMAL_Y 1
+#define WSR_PROF_FLUX_X 2
+#define WSR_PROF_FLUX_Y 3
+#define WSR_PROF_UPDATE 4
+#define WSR_PROF_CONTROL 5
+#define WSR_PROF_KINDS 6
+
+/* Bracket every kernel launched through this context with CUDA events on its stream (on != 0), and
+ * reset the totals. */
+int wsr_profile_enable(wsr_ctx *ctx, int on);
+/* Synchronise the recorded events and return, per kernel class, the summed device time in ms and the
+ * launch count (arrays of WSR_PROF_KINDS). */
+int wsr_profile_read(wsr_ctx *ctx, double *ms, long long *launches);
+
+/* Closure tallies of the last run/stage made with WSR_OPT_COUNT, per kernel class k = normal x,
+ * normal y, flux x, flux y: out_host[2k] = stencils that ran the MLP pair, out_host[2k+1] = plateau
+ * stencils that took the linear weights (out_host holds 8 values). */
+#define WSR_OPT_COUNT 4
+int wsr_euler2d_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny,
+                         unsigned long long *out_host);
+
+/* Measured FMA throughput of this GPU in TFLOP/s (bits = 32 or 64; 2 flops per FMA). */
+int wsr_probe_peak_flops(wsr_ctx *ctx, int bits, double *tflops, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,7 +18,8 @@ WSR_OK, WSR_ERR_ARG, WSR_ERR_CUDA, WSR_ERR_NO_CLOSURE = 0, 1, 2, 3
 METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3}
 BC = {"transmissive": 0, "periodic": 1}
 FLUX = {"hllc": 0, "force": 1}
-OPT_ENO_CUTOFF, OPT_JS_FALLBACK = 1, 2
+OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT = 1, 2, 4
+PROF_KINDS = ("normal_x", "normal_y", "flux_x", "flux_y", "update", "control")
 N_PARAMS5 = 189
 PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")
 
@@ -52,13 +53,18 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
                                           C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
                                           vp, sz, vp]
+            L.wsr_profile_enable.argtypes = [vp, i]
+            L.wsr_profile_read.argtypes = [vp, C.POINTER(d), C.POINTER(C.c_longlong)]
+            L.wsr_euler2d_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
+            L.wsr_probe_peak_flops.argtypes = [vp, i, C.POINTER(d), vp]
             _lib = L
     return _lib
 
 
 def exported_symbols() -> list[str]:
     return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
-            "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run"]
+            "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run",
+            "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops"]
 
 
 def pack_params(params) -> np.ndarray:
@@ -100,6 +106,20 @@ class Context:
         if rc == WSR_ERR_ARG:
             raise ValueError(msg)
         raise RuntimeError(f"libwsr status {rc}: {msg}")
+
+    def profile_enable(self, on: bool = True) -> None:
+        self.check(lib().wsr_profile_enable(self.handle, int(on)))
+
+    def profile_read(self) -> dict:
+        ms = (C.c_double * len(PROF_KINDS))()
+        n = (C.c_longlong * len(PROF_KINDS))()
+        self.check(lib().wsr_profile_read(self.handle, ms, n))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(PROF_KINDS)}
+
+    def peak_tflops(self, bits: int, stream=None) -> float:
+        out = C.c_double(0.0)
+        self.check(lib().wsr_probe_peak_flops(self.handle, bits, C.byref(out), stream))
+        return out.value
 
     def upload_closure(self, packed: np.ndarray) -> None:
         packed = np.ascontiguousarray(packed, dtype=np.float64)

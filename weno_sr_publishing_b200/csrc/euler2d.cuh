@@ -28,8 +28,25 @@ constexpr int kGhost = 3;
 enum Bc { BC_TRANSMISSIVE = 0, BC_PERIODIC = 1 };
 enum Flux { FLUX_HLLC = 0, FLUX_FORCE = 1 };
 
-// Options bitmask.
-enum : int { OPT_ENO_CUTOFF = 1, OPT_JS_FALLBACK = 2 };
+// Options bitmask. OPT_COUNT makes the reconstruction kernels count closure evaluations (SR stencils
+// that ran the MLP pair, and plateau stencils that took the linear weights) for the roofline tally.
+enum : int { OPT_ENO_CUTOFF = 1, OPT_JS_FALLBACK = 2, OPT_COUNT = 4 };
+
+// Per-thread tallies, flushed with one atomic each when OPT_COUNT is set.
+struct Tally {
+  int fallbacks = 0;
+  int mlp = 0;
+  int plateau = 0;
+};
+
+__device__ __forceinline__ void flush_tally(const Tally& t, int opts, int* fallbacks,
+                                            unsigned long long* counters) {
+  if (t.fallbacks) atomicAdd(fallbacks, t.fallbacks);
+  if ((opts & OPT_COUNT) && counters) {
+    if (t.mlp) atomicAdd(&counters[0], (unsigned long long)t.mlp);
+    if (t.plateau) atomicAdd(&counters[1], (unsigned long long)t.plateau);
+  }
+}
 
 // Device-resident time-step control block (one per run).
 struct StepCtl {
@@ -85,14 +102,18 @@ __device__ __forceinline__ bool stencil_weights(const double q[5], const typenam
 // fallback option is set.
 template <int M>
 __device__ __forceinline__ double recon_one(const double q[5], int head, const typename ClosureParams<M>::type& P,
-                                            int opts, int* fallback_count) {
+                                            int opts, Tally& tally) {
   StencilW s;
   bool ok = stencil_weights<M>(q, P, s);
+  if (M != M_JS) {
+    tally.mlp += s.linear ? 0 : 1;
+    tally.plateau += s.linear ? 1 : 0;
+  }
   double w[3], c[3];
   if (!ok && (opts & OPT_JS_FALLBACK)) {
     StencilW js = js_stencil(q);
     js_head_weights(js, linear_weights(head), w);
-    ++*fallback_count;
+    ++tally.fallbacks;
   } else {
     head_weights<M>(s, head, (opts & OPT_ENO_CUTOFF) != 0, w);
   }
@@ -120,6 +141,7 @@ template <int M, int DIR>
 __global__ void __launch_bounds__(128) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
                                                 double* __restrict__ out_r, int nx, int ny, int bc, double g,
                                                 const StepCtl* __restrict__ ctl, int opts, int* __restrict__ fallbacks,
+                                                unsigned long long* __restrict__ counters,
                                                 const __grid_constant__ typename ClosureParams<M>::type P) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = blockIdx.y * blockDim.y + threadIdx.y;
@@ -132,7 +154,7 @@ __global__ void __launch_bounds__(128) k_normal(const double* __restrict__ u, do
   }
   if (r < r0 || r >= r1 || c < c0 || c >= c1) return;
   if (ctl != nullptr && ctl->done) return;
-  int nfb = 0;
+  Tally tally;
   d4 q[5];
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
@@ -162,7 +184,7 @@ __global__ void __launch_bounds__(128) k_normal(const double* __restrict__ u, do
     double cf[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 1
     for (int f = 0; f < 4; ++f) {
-      double v = recon_one<M>(ch[0], head, P, opts, &nfb);
+      double v = recon_one<M>(ch[0], head, P, opts, tally);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         cf[a] = cf[a + 1];
@@ -188,26 +210,30 @@ __global__ void __launch_bounds__(128) k_normal(const double* __restrict__ u, do
           jf[f] = combine(w, cc);
         }
         face = char_to_con<DIR>(jf, J);
-        ++nfb;
+        ++tally.fallbacks;
       }
     }
     store_cell(side == 0 ? out_l : out_r, oidx, face);
   }
-  if (nfb) atomicAdd(fallbacks, nfb);
+  flush_tally(tally, opts, fallbacks, counters);
 }
 
 // Transverse reconstruction of one conserved component at both Gauss points (heads 2 and 3) from a
 // single closure evaluation.
 template <int M>
 __device__ __forceinline__ void gauss_pair(const double q[5], const typename ClosureParams<M>::type& P, int opts,
-                                           int* nfb, double& g1, double& g2) {
+                                           Tally& tally, double& g1, double& g2) {
   StencilW s;
   bool ok = stencil_weights<M>(q, P, s);
+  if (M != M_JS) {
+    tally.mlp += s.linear ? 0 : 1;
+    tally.plateau += s.linear ? 1 : 0;
+  }
   double w[3], c[3];
   const bool fb = !ok && (opts & OPT_JS_FALLBACK);
   if (fb) {
     s = js_stencil(q);
-    ++*nfb;
+    ++tally.fallbacks;
   }
 #pragma unroll
   for (int h = 2; h <= 3; ++h) {
@@ -233,6 +259,7 @@ template <int M, int DIR>
 __global__ void __launch_bounds__(128) k_flux(const double* __restrict__ fl, const double* __restrict__ fr,
                                               double* __restrict__ fout, int nx, int ny, double g, int flux,
                                               const StepCtl* __restrict__ ctl, int opts, int* __restrict__ fallbacks,
+                                              unsigned long long* __restrict__ counters,
                                               const __grid_constant__ typename ClosureParams<M>::type P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -240,7 +267,7 @@ __global__ void __launch_bounds__(128) k_flux(const double* __restrict__ fl, con
   if (i >= nfx || j >= nfy) return;
   if (ctl->done) return;
   const double dt_h = DIR == 1 ? ctl->dt_dx : ctl->dt_dy;
-  int nfb = 0;
+  Tally tally;
   // Eight stencils per face: n = 2*comp + side, side 0 -> u_R (from the lr=2 faces fl), side 1 -> u_L.
   // Results rotate through g1/g2 so that indices stay constant inside the rolled loop.
   double g1[8], g2[8];
@@ -259,7 +286,7 @@ __global__ void __launch_bounds__(128) k_flux(const double* __restrict__ fl, con
       for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
     }
     double a, b;
-    gauss_pair<M>(s, P, opts, &nfb, a, b);
+    gauss_pair<M>(s, P, opts, tally, a, b);
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
       g1[k] = g1[k + 1];
@@ -282,7 +309,7 @@ __global__ void __launch_bounds__(128) k_flux(const double* __restrict__ fl, con
 #pragma unroll
   for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] * dt_h + f2.v[k] * dt_h;
   store_cell(fout, (size_t)j * nfx + i, o);
-  if (nfb) atomicAdd(fallbacks, nfb);
+  flush_tally(tally, opts, fallbacks, counters);
 }
 
 __device__ __forceinline__ unsigned long long speed_bits(const d4& q, double g) {

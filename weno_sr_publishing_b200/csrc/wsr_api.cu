@@ -12,6 +12,9 @@
 
 using namespace wsr;
 
+constexpr int kProfKinds = 6;  // normal x, normal y, flux x, flux y, update, control
+constexpr int kProfEvents = 512;
+
 struct wsr_ctx {
   int device;
   bool have_closure;
@@ -20,6 +23,14 @@ struct wsr_ctx {
   Mlp5f pbf16;
   char err[512];
   double* host_pinned;  // small pinned mailbox for control-block reads
+  // per-kernel CUDA-event timing (off unless wsr_profile_enable)
+  bool prof_on;
+  bool prof_created;
+  cudaEvent_t ev_a[kProfEvents], ev_b[kProfEvents];
+  int ev_kind[kProfEvents];
+  int n_ev;
+  double prof_ms[kProfKinds];
+  long long prof_count[kProfKinds];
 };
 
 namespace {
@@ -56,6 +67,8 @@ bool misaligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) !
 struct Ws2d {
   StepCtl* ctl;
   int* fallbacks;
+  unsigned long long* counters;  // per kernel class k (normal x, normal y, flux x, flux y): [2k] MLP closure
+                                 // evaluations, [2k+1] plateau stencils
   double* dts;  // ring of kDtsRing
   double *xl, *xr, *yl, *yr, *fx, *fy;
 };
@@ -63,7 +76,8 @@ struct Ws2d {
 size_t cells_bytes(size_t n) { return align_up(n * 4 * sizeof(double)); }
 
 size_t ws_bytes(int nx, int ny) {
-  size_t b = align_up(sizeof(StepCtl)) + align_up(sizeof(int)) + align_up(kDtsRing * sizeof(double));
+  size_t b = align_up(sizeof(StepCtl)) + align_up(sizeof(int)) + align_up(8 * sizeof(unsigned long long)) +
+             align_up(kDtsRing * sizeof(double));
   b += 2 * cells_bytes((size_t)(ny + 6) * (nx + 2));
   b += 2 * cells_bytes((size_t)(ny + 2) * (nx + 6));
   b += cells_bytes((size_t)ny * (nx + 1));
@@ -78,6 +92,8 @@ Ws2d carve(void* base, int nx, int ny) {
   p += align_up(sizeof(StepCtl));
   w.fallbacks = reinterpret_cast<int*>(p);
   p += align_up(sizeof(int));
+  w.counters = reinterpret_cast<unsigned long long*>(p);
+  p += align_up(8 * sizeof(unsigned long long));
   w.dts = reinterpret_cast<double*>(p);
   p += align_up(kDtsRing * sizeof(double));
   w.xl = reinterpret_cast<double*>(p);
@@ -131,6 +147,36 @@ const Mlp5f& params_of<M_SRBF16>(const wsr_ctx* ctx) {
   return ctx->pbf16;
 }
 
+int prof_flush(wsr_ctx* ctx) {
+  if (ctx->n_ev == 0) return WSR_OK;
+  WSR_CUDA(ctx, cudaEventSynchronize(ctx->ev_b[ctx->n_ev - 1]));
+  for (int k = 0; k < ctx->n_ev; ++k) {
+    float ms = 0.f;
+    WSR_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev_a[k], ctx->ev_b[k]));
+    ctx->prof_ms[ctx->ev_kind[k]] += ms;
+    ctx->prof_count[ctx->ev_kind[k]] += 1;
+  }
+  ctx->n_ev = 0;
+  return WSR_OK;
+}
+
+// Brackets one launch with events when profiling is on.
+struct ProfScope {
+  wsr_ctx* ctx;
+  cudaStream_t st;
+  int slot;
+  ProfScope(wsr_ctx* c, cudaStream_t s, int kind) : ctx(c), st(s), slot(-1) {
+    if (!ctx->prof_on) return;
+    if (ctx->n_ev == kProfEvents && prof_flush(ctx) != WSR_OK) return;
+    slot = ctx->n_ev++;
+    ctx->ev_kind[slot] = kind;
+    cudaEventRecord(ctx->ev_a[slot], st);
+  }
+  ~ProfScope() {
+    if (slot >= 0) cudaEventRecord(ctx->ev_b[slot], st);
+  }
+};
+
 struct StageArgs {
   const double* u_stage;
   const double* u0;
@@ -145,30 +191,39 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t s
   const auto& P = params_of<M>(ctx);
   const dim3 blk(64, 2);
   {
+    ProfScope ps(ctx, st, 0);
     dim3 grd((a.nx + 2 + blk.x - 1) / blk.x, (a.ny + 5 + blk.y - 1) / blk.y);
-    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, P);
-    WSR_LAUNCHED(ctx, "k_normal<x>");
+    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks,
+                                        w.counters + 0, P);
   }
+  WSR_LAUNCHED(ctx, "k_normal<x>");
   {
+    ProfScope ps(ctx, st, 1);
     dim3 grd((a.nx + 5 + blk.x - 1) / blk.x, (a.ny + 2 + blk.y - 1) / blk.y);
-    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, P);
-    WSR_LAUNCHED(ctx, "k_normal<y>");
+    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks,
+                                        w.counters + 2, P);
   }
+  WSR_LAUNCHED(ctx, "k_normal<y>");
   {
+    ProfScope ps(ctx, st, 2);
     dim3 grd((a.nx + 1 + blk.x - 1) / blk.x, (a.ny + blk.y - 1) / blk.y);
-    k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, P);
-    WSR_LAUNCHED(ctx, "k_flux<x>");
+    k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks,
+                                      w.counters + 4, P);
   }
+  WSR_LAUNCHED(ctx, "k_flux<x>");
   {
+    ProfScope ps(ctx, st, 3);
     dim3 grd((a.nx + blk.x - 1) / blk.x, (a.ny + 1 + blk.y - 1) / blk.y);
-    k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, P);
-    WSR_LAUNCHED(ctx, "k_flux<y>");
+    k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks,
+                                      w.counters + 6, P);
   }
+  WSR_LAUNCHED(ctx, "k_flux<y>");
   {
+    ProfScope ps(ctx, st, 4);
     dim3 grd((a.nx + 255) / 256, a.ny);
     k_update<<<grd, 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk, a.g, w.ctl);
-    WSR_LAUNCHED(ctx, "k_update");
   }
+  WSR_LAUNCHED(ctx, "k_update");
   return WSR_OK;
 }
 
@@ -185,7 +240,7 @@ int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, 
   }
 }
 
-__global__ void k_init_ctl(StepCtl* ctl, int* fallbacks, double t_start, double t_end, double dt, double dx, double dy, double cfl,
+__global__ void k_init_ctl(StepCtl* ctl, int* fallbacks, unsigned long long* counters, double t_start, double t_end, double dt, double dx, double dy, double cfl,
                            double hmin, int check_health, int check_interval, int max_steps) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   ctl->t = t_start;
@@ -204,6 +259,7 @@ __global__ void k_init_ctl(StepCtl* ctl, int* fallbacks, double t_start, double 
   ctl->cfl = cfl;
   ctl->hmin = hmin;
   *fallbacks = 0;
+  for (int k = 0; k < 8; ++k) counters[k] = 0ull;
 }
 
 // Variant of k_step_begin that writes into a ring of kDtsRing records.
@@ -257,6 +313,11 @@ int wsr_ctx_create(int device, wsr_ctx** out) {
 void wsr_ctx_destroy(wsr_ctx* ctx) {
   if (!ctx) return;
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  if (ctx->prof_created)
+    for (int k = 0; k < kProfEvents; ++k) {
+      cudaEventDestroy(ctx->ev_a[k]);
+      cudaEventDestroy(ctx->ev_b[k]);
+    }
   delete ctx;
 }
 
@@ -293,7 +354,7 @@ int wsr_euler2d_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, dou
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
   Ws2d w = carve(workspace, nx, ny);
-  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
   WSR_LAUNCHED(ctx, "k_init_ctl");
   StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma};
   return dispatch_stage(ctx, method, a, w, st);
@@ -340,7 +401,7 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
   Ws2d w = carve(workspace, nx, ny);
   const double hmin = dx < dy ? dx : dy;
-  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, fixed_steps > 0 ? 0.0 : t_start, t_end, 0.0, dx, dy, cfl, hmin,
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, fixed_steps > 0 ? 0.0 : t_start, t_end, 0.0, dx, dy, cfl, hmin,
                               check_health, check_interval,
                               max_steps);
   WSR_LAUNCHED(ctx, "k_init_ctl");
@@ -352,24 +413,32 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   int done = 0;
   StepCtl snap;
   while (!done) {
-    for (int b = 0; b < batch; ++b) {
+    // a fixed-step run launches exactly its steps; a t_end run polls every `batch` steps
+    const int nb = fixed_steps > 0 ? (max_steps - host_steps < batch ? max_steps - host_steps : batch) : batch;
+    if (nb <= 0) break;
+    for (int b = 0; b < nb; ++b) {
       const int s = host_steps + b;
       double* in = (s & 1) ? u[3] : u[0];
       double* out = (s & 1) ? u[0] : u[3];
-      k_step_begin_ring<<<1, 1, 0, st>>>(w.ctl, w.dts);
+      {
+        ProfScope ps(ctx, st, 5);
+        k_step_begin_ring<<<1, 1, 0, st>>>(w.ctl, w.dts);
+        k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
+      }
       WSR_LAUNCHED(ctx, "k_step_begin");
-      k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
-      WSR_LAUNCHED(ctx, "k_set_dt_ratios");
       StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma};
       StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma};
       StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma};
       if ((rc = dispatch_stage(ctx, method, a1, w, st))) return rc;
       if ((rc = dispatch_stage(ctx, method, a2, w, st))) return rc;
       if ((rc = dispatch_stage(ctx, method, a3, w, st))) return rc;
-      k_step_end<<<1, 1, 0, st>>>(w.ctl);
+      {
+        ProfScope ps(ctx, st, 5);
+        k_step_end<<<1, 1, 0, st>>>(w.ctl);
+      }
       WSR_LAUNCHED(ctx, "k_step_end");
     }
-    host_steps += batch;
+    host_steps += nb;
     WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, w.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
     WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned + 128, w.dts, kDtsRing * sizeof(double), cudaMemcpyDeviceToHost, st));
     WSR_CUDA(ctx, cudaStreamSynchronize(st));
@@ -388,4 +457,102 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   return WSR_OK;
 }
 
+int wsr_profile_enable(wsr_ctx* ctx, int on) {
+  if (!ctx) return WSR_ERR_ARG;
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (on && !ctx->prof_created) {
+    for (int k = 0; k < kProfEvents; ++k) {
+      WSR_CUDA(ctx, cudaEventCreate(&ctx->ev_a[k]));
+      WSR_CUDA(ctx, cudaEventCreate(&ctx->ev_b[k]));
+    }
+    ctx->prof_created = true;
+  }
+  if (ctx->prof_on) {
+    int rc = prof_flush(ctx);
+    if (rc) return rc;
+  }
+  ctx->prof_on = on != 0;
+  ctx->n_ev = 0;
+  for (int k = 0; k < kProfKinds; ++k) {
+    ctx->prof_ms[k] = 0.0;
+    ctx->prof_count[k] = 0;
+  }
+  return WSR_OK;
+}
+
+int wsr_profile_read(wsr_ctx* ctx, double* ms, long long* launches) {
+  if (!ctx || !ms || !launches) return WSR_ERR_ARG;
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  int rc = prof_flush(ctx);
+  if (rc) return rc;
+  for (int k = 0; k < kProfKinds; ++k) {
+    ms[k] = ctx->prof_ms[k];
+    launches[k] = ctx->prof_count[k];
+  }
+  return WSR_OK;
+}
+
+int wsr_euler2d_counters(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, int nx, int ny,
+                         unsigned long long* out_host) {
+  if (!ctx || !workspace || !out_host) return WSR_ERR_ARG;
+  if (workspace_bytes < ws_bytes(nx, ny)) return fail(ctx, WSR_ERR_ARG, "workspace too small");
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return WSR_OK;
+}
+
 }  // extern "C"
+
+namespace {
+// Independent FMA chains for the peak-throughput probe (8 per thread).
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b) {
+  T x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int k = 0; k < iters; ++k) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      x0 = x0 * a + b; x1 = x1 * a + b; x2 = x2 * a + b; x3 = x3 * a + b;
+      x4 = x4 * a + b; x5 = x5 * a + b; x6 = x6 * a + b; x7 = x7 * a + b;
+    }
+  }
+  T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == T(-12345.678)) out[blockIdx.x] = s;  // keeps the chains live
+}
+}  // namespace
+
+extern "C" int wsr_probe_peak_flops(wsr_ctx* ctx, int bits, double* tflops, void* stream) {
+  if (!ctx || !tflops || (bits != 32 && bits != 64)) return WSR_ERR_ARG;
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int sms = 0;
+  WSR_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  const int blocks = sms * 8, threads = 256, iters = bits == 32 ? 4096 : 2048;
+  void* out = nullptr;
+  WSR_CUDA(ctx, cudaMallocAsync(&out, blocks * sizeof(double), st));
+  cudaEvent_t e0, e1;
+  WSR_CUDA(ctx, cudaEventCreate(&e0));
+  WSR_CUDA(ctx, cudaEventCreate(&e1));
+  double best = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {
+    WSR_CUDA(ctx, cudaEventRecord(e0, st));
+    if (bits == 32)
+      k_fma_probe<float><<<blocks, threads, 0, st>>>(static_cast<float*>(out), iters, 0.9999f, 1e-4f);
+    else
+      k_fma_probe<double><<<blocks, threads, 0, st>>>(static_cast<double*>(out), iters, 0.9999, 1e-4);
+    WSR_CUDA(ctx, cudaEventRecord(e1, st));
+    WSR_CUDA(ctx, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    WSR_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    double tf = flops / (ms * 1e-3) / 1e12;
+    if (rep > 0 && tf > best) best = tf;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  WSR_CUDA(ctx, cudaFreeAsync(out, st));
+  WSR_CUDA(ctx, cudaStreamSynchronize(st));
+  *tflops = best;
+  return WSR_OK;
+}
+

@@ -102,6 +102,15 @@ def compute_dt(u: torch.Tensor, params: Params, ws: Workspace | None = None) -> 
     return params.cfl * min(params.dx, params.dy) / m
 
 
+def counters(ws: Workspace) -> dict[str, tuple[int, int]]:
+    """Per kernel class: (MLP closure evaluations, plateau stencils) of the last call made with OPT_COUNT."""
+    out = (C.c_ulonglong * 8)()
+    ctx = N.context(ws.buf.device.index)
+    ctx.check(N.lib().wsr_euler2d_counters(ctx.handle, C.c_void_p(ws.ptr), ws.nbytes, ws.nx, ws.ny, out))
+    return {k: (int(out[2 * i]), int(out[2 * i + 1])) for i, k in enumerate(("normal_x", "normal_y", "flux_x",
+                                                                              "flux_y"))}
+
+
 @dataclass
 class RunResult:
     final_slot: int
@@ -135,3 +144,17 @@ def run(bufs: list, params: Params, t_end: float, method: str, boundary: str, ml
         int(check_interval), int(fixed_steps), int(cap), dts.ctypes.data_as(C.POINTER(C.c_double)), C.byref(steps),
         C.byref(t), C.byref(slot), C.byref(fb), C.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(dev)))
     return RunResult(slot.value, [float(x) for x in dts[:steps.value]], steps.value, t.value, fb.value)
+
+
+def advance_host(u_host: np.ndarray, params: Params, steps: int, method: str, boundary: str, mlp_params=None,
+                 bufs: list | None = None, ws: Workspace | None = None, device="cuda") -> np.ndarray:
+    """Host-buffer entry: copy the padded state to the device, run `steps` full CFL steps, copy it back
+    into u_host (in place). Pinned host memory makes both copies asynchronous DMA."""
+    dev = torch.device(device)
+    if bufs is None:
+        bufs = [torch.empty(params.padded_shape, dtype=torch.float64, device=dev) for _ in range(4)]
+    host = torch.from_numpy(u_host) if isinstance(u_host, np.ndarray) else u_host
+    bufs[0].copy_(host, non_blocking=True)
+    res = run(bufs, params, 1.0e300, method, boundary, mlp_params=mlp_params, fixed_steps=steps, ws=ws)
+    host.copy_(bufs[res.final_slot], non_blocking=True)
+    return u_host
