@@ -127,6 +127,23 @@ int wsr_euler2d_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, 
 /* Measured FMA throughput of this GPU in TFLOP/s (bits = 32 or 64; 2 flops per FMA). */
 int wsr_probe_peak_flops(wsr_ctx *ctx, int bits, double *tflops, void *stream);
 
+/* ---- stage without any allocation (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc (a host that owns all device memory through its own pool,
+ * or a step that must not pay cudaMalloc's implicit synchronisation). Same result as
+ * wsr_euler2d_stage, but the scratch lives in a static device array of WSR_NOALLOC_SCRATCH_BYTES
+ * (32 MiB, enough for grids up to 400 x 400) that every GPU loading the library holds until exit.
+ * No context: `closure_params` is a HOST array of the 189 packed parameters (NULL for WSR_METHOD_JS).
+ * Runs on the calling thread's current device; `stream` must belong to it. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and must come before any stream capture
+ * on that device. Grids whose workspace exceeds the array return WSR_ERR_SCRATCH_LIMIT. All calls on
+ * a device share the array: calls that overlap on the GPU race and must be serialised by the caller.
+ * Returns status codes only (no message). */
+#define WSR_ERR_SCRATCH_LIMIT 4
+#define WSR_NOALLOC_SCRATCH_BYTES (32u << 20)
+int wsr_euler2d_stage_noalloc(const double *u_stage, const double *u0, double *u_out, int nx, int ny, double dx,
+                              double dy, double gamma, double dt, int rk, int method, int bc, int flux, int opts,
+                              const double *closure_params, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

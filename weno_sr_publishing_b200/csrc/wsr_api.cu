@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "../../include/wsr.h"
@@ -556,3 +557,99 @@ extern "C" int wsr_probe_peak_flops(wsr_ctx* ctx, int bits, double* tflops, void
   return WSR_OK;
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// No-allocation stage (wsr_euler2d_stage_noalloc).
+//
+// Some callers cannot call cudaMalloc: a host application that owns every byte of device memory
+// through its own pool, or a solver step that must not pay cudaMalloc's implicit device
+// synchronisation. For them the stage's scratch (face values, fluxes, step-control block) lives in
+// the file-scope array below instead of a caller workspace. Every GPU that loads libwsr.so holds
+// these WSR_NOALLOC_SCRATCH_BYTES until the process exits. All calls on a device share the array and
+// it keeps the previous call's contents: the control block and counters are re-initialised by every
+// call, and every face/flux value a call reads is written earlier in the same call, so nothing
+// carries over; but calls that overlap on the GPU (e.g. on two streams at once) race on the array
+// and must be serialised by the caller.
+// ---------------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[WSR_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoallocMaxDevices];  // device address of g_noalloc_scratch, per device
+
+// Host code may not pass &g_noalloc_scratch to a kernel (it is a host-side stand-in, not a device
+// address): the device address is looked up once per device, with that device current.
+int noalloc_scratch_for(int dev, void** out) {
+  if (dev < 0 || dev >= kNoallocMaxDevices) return WSR_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return WSR_ERR_CUDA;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return WSR_OK;
+}
+
+template <int M>
+int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
+  const dim3 blk(64, 2);
+  k_normal<M, 1><<<dim3((a.nx + 2 + blk.x - 1) / blk.x, (a.ny + 5 + blk.y - 1) / blk.y), blk, 0, st>>>(
+      a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
+  k_normal<M, 2><<<dim3((a.nx + 5 + blk.x - 1) / blk.x, (a.ny + 2 + blk.y - 1) / blk.y), blk, 0, st>>>(
+      a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
+  k_flux<M, 1><<<dim3((a.nx + 1 + blk.x - 1) / blk.x, (a.ny + blk.y - 1) / blk.y), blk, 0, st>>>(
+      w.xl, w.xr, w.fx, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P);
+  k_flux<M, 2><<<dim3((a.nx + blk.x - 1) / blk.x, (a.ny + 1 + blk.y - 1) / blk.y), blk, 0, st>>>(
+      w.yl, w.yr, w.fy, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P);
+  k_update<<<dim3((a.nx + 255) / 256, a.ny), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk,
+                                                          a.g, w.ctl);
+  return cudaGetLastError() == cudaSuccess ? WSR_OK : WSR_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int wsr_euler2d_stage_noalloc(const double* u_stage, const double* u0, double* u_out, int nx, int ny,
+                                         double dx, double dy, double gamma, double dt, int rk, int method, int bc,
+                                         int flux, int opts, const double* closure_params, void* stream) {
+  if (nx < 3 || ny < 3) return WSR_ERR_ARG;
+  if (ws_bytes(nx, ny) > (size_t)WSR_NOALLOC_SCRATCH_BYTES) return WSR_ERR_SCRATCH_LIMIT;
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return WSR_ERR_ARG;
+  if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC) return WSR_ERR_ARG;
+  if (flux != WSR_FLUX_HLLC && flux != WSR_FLUX_FORCE) return WSR_ERR_ARG;
+  if (rk < 1 || rk > 3 || !(dt > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return WSR_ERR_ARG;
+  if (!u_stage || !u0 || !u_out || misaligned(u_stage) || misaligned(u0) || misaligned(u_out)) return WSR_ERR_ARG;
+  if (method != WSR_METHOD_JS && !closure_params) return WSR_ERR_NO_CLOSURE;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return WSR_ERR_CUDA;
+  void* scratch = nullptr;
+  int rc = noalloc_scratch_for(dev, &scratch);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Ws2d w = carve(scratch, nx, ny);
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
+  if (cudaGetLastError() != cudaSuccess) return WSR_ERR_CUDA;
+  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma};
+  switch (method) {
+    case WSR_METHOD_JS:
+      return noalloc_launch<M_JS>(NoParams{}, a, w, st);
+    case WSR_METHOD_SR_F64: {
+      Mlp5d P;
+      for (int k = 0; k < kParams5; ++k) P.p[k] = closure_params[k];
+      return noalloc_launch<M_SR64>(P, a, w, st);
+    }
+    case WSR_METHOD_SR_F32: {
+      Mlp5f P;
+      for (int k = 0; k < kParams5; ++k) P.p[k] = static_cast<float>(closure_params[k]);
+      return noalloc_launch<M_SR32>(P, a, w, st);
+    }
+    default: {
+      Mlp5f P;
+      for (int k = 0; k < kParams5; ++k)
+        P.p[k] = __bfloat162float(__float2bfloat16_rn(static_cast<float>(closure_params[k])));
+      return noalloc_launch<M_SRBF16>(P, a, w, st);
+    }
+  }
+}
