@@ -110,13 +110,13 @@ __device__ __forceinline__ StencilW js_stencil(const double q[5]) {
   return s;
 }
 
-// JS: w_k = d_k rcp_k^2 / sum   (wh:557-568)
+// JS: w_k = d_k rcp_k^2 / sum   (wh:557-568); one reciprocal of the sum instead of three divisions.
 __device__ __forceinline__ void js_head_weights(const StencilW& s, const Lin3& d, double w[3]) {
   double a0 = d.d0 * s.a0 * s.a0, a1 = d.d1 * s.a1 * s.a1, a2 = d.d2 * s.a2 * s.a2;
-  double sum = a0 + a1 + a2;
-  w[0] = a0 / sum;
-  w[1] = a1 / sum;
-  w[2] = a2 / sum;
+  double inv = 1.0 / (a0 + a1 + a2);
+  w[0] = a0 * inv;
+  w[1] = a1 * inv;
+  w[2] = a2 * inv;
 }
 
 // SR: alpha_k = d_k / (3 r_k + 1e-12)^2; w = alpha / max(sum, 1e-300); optional ENO cutoff
@@ -335,6 +335,101 @@ __device__ __forceinline__ void head_weights(const StencilW& s, int head, bool e
 
 __device__ __forceinline__ double combine(const double w[3], const double s[3]) {
   return w[0] * s[0] + w[1] * s[1] + w[2] * s[2];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Split closure for the compacted kernels: phase A decides plateau vs MLP from the cheap sensors,
+// phase B evaluates the MLP pair of the queued stencils densely, phase C forms the weights.
+// ---------------------------------------------------------------------------------------------
+
+// delta_k, delta_max and q_scale (DEPLOY:76-93, 123-131) without the gamma ratios, which only the
+// MLP needs.
+struct Sens {
+  double d0, d1, d2, dmax, qscale;
+};
+
+__device__ __forceinline__ Sens sensors5(const double q[5]) {
+  double d20 = q[0] - 2.0 * q[1] + q[2], d21 = q[1] - 2.0 * q[2] + q[3], d22 = q[2] - 2.0 * q[3] + q[4];
+  Sens s;
+  s.d0 = (13.0 / 12.0) * fabs(d20) + 0.25 * fabs(q[0] - 4.0 * q[1] + 3.0 * q[2]);
+  s.d1 = (13.0 / 12.0) * fabs(d21) + 0.25 * fabs(q[1] - q[3]);
+  s.d2 = (13.0 / 12.0) * fabs(d22) + 0.25 * fabs(3.0 * q[2] - 4.0 * q[3] + q[4]);
+  s.dmax = fmax(fmax(s.d0, s.d1), s.d2);
+  double qs = fmax(fmax(fmax(fabs(q[0]), fabs(q[1])), fmax(fabs(q[2]), fabs(q[3]))), fabs(q[4]));
+  s.qscale = fmax(qs, 1.0);
+  return s;
+}
+
+__device__ __forceinline__ bool is_plateau(const Sens& s) { return s.dmax <= 1.0e-13 * s.qscale; }
+
+__device__ __forceinline__ double gamma_s(const double q[5]) {
+  const double eps = 1.0e-15;
+  double d20 = q[0] - 2.0 * q[1] + q[2], d21 = q[1] - 2.0 * q[2] + q[3], d22 = q[2] - 2.0 * q[3] + q[4];
+  double g0 = fabs(d20) / (fabs(q[1] - q[0]) + fabs(q[2] - q[1]) + eps);
+  double g1 = fabs(d21) / (fabs(q[2] - q[1]) + fabs(q[3] - q[2]) + eps);
+  double g2 = fabs(d22) / (fabs(q[3] - q[2]) + fabs(q[4] - q[3]) + eps);
+  return fmin(1.0, fmax(fmax(g0, g1), g2));
+}
+
+// The five MLP inputs of a non-plateau stencil (direct orientation), FP64.
+__device__ __forceinline__ void features_of(const double q[5], const Sens& s, double f[5]) {
+  double inv = 1.0 / fmax(s.dmax, 1.0e-15);
+  double rel = fmax(s.dmax / s.qscale, 1.0e-30);
+  double l10 = log(rel) / 2.302585092994046;
+  f[0] = s.d0 * inv;
+  f[1] = s.d1 * inv;
+  f[2] = s.d2 * inv;
+  f[3] = gamma_s(q);
+  f[4] = fmin(1.0, fmax(0.0, (l10 + 4.0) / 4.0));
+}
+
+// Queue element types: MLP inputs in the closure precision.
+template <int M>
+struct QIn {
+  using T = float;
+};
+template <>
+struct QIn<M_SR64> {
+  using T = double;
+};
+
+// Phase B: reflection-averaged ratios of one queued stencil -> reciprocal scaled betas.
+template <int M>
+__device__ __forceinline__ void closure_from_features(const typename QIn<M>::T* x, const typename ClosureParams<M>::type& P,
+                                                      double& a0, double& a1, double& a2) {
+  double r0, r1, r2;
+  if constexpr (M == M_SR64) {
+    double xa[5] = {x[0], x[1], x[2], x[3], x[4]};
+    double xb[5] = {x[2], x[1], x[0], x[3], x[4]};
+    double ra[3], rb[3];
+    mlp_pair<double, false>(reinterpret_cast<const double*>(&P), xa, xb, ra, rb);
+    r0 = 0.5 * (ra[0] + rb[2]);
+    r1 = 0.5 * (ra[1] + rb[1]);
+    r2 = 0.5 * (ra[2] + rb[0]);
+  } else {
+    constexpr bool B = M == M_SRBF16;
+    float xa[5] = {x[0], x[1], x[2], x[3], x[4]};
+    float xb[5] = {x[2], x[1], x[0], x[3], x[4]};
+    float ra[3], rb[3];
+    mlp_pair<float, B>(reinterpret_cast<const float*>(&P), xa, xb, ra, rb);
+    r0 = 0.5 * ((double)ra[0] + (double)rb[2]);
+    r1 = 0.5 * ((double)ra[1] + (double)rb[1]);
+    r2 = 0.5 * ((double)ra[2] + (double)rb[0]);
+  }
+  a0 = 1.0 / (3.0 * r0 + 1.0e-12);
+  a1 = 1.0 / (3.0 * r1 + 1.0e-12);
+  a2 = 1.0 / (3.0 * r2 + 1.0e-12);
+}
+
+// Cast FP64 features to the queue type (BF16 inputs are rounded to bfloat16, as the oracle does).
+template <int M>
+__device__ __forceinline__ typename QIn<M>::T to_queue(double f) {
+  if constexpr (M == M_SR64)
+    return f;
+  else if constexpr (M == M_SRBF16)
+    return bf16r((float)f);
+  else
+    return (float)f;
 }
 
 }  // namespace wsr

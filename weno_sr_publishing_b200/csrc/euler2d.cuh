@@ -87,40 +87,6 @@ __device__ __forceinline__ void store_cell(double* __restrict__ u, size_t idx, c
   p[1] = make_double2(q.v[2], q.v[3]);
 }
 
-template <int M>
-__device__ __forceinline__ bool stencil_weights(const double q[5], const typename ClosureParams<M>::type& P,
-                                                StencilW& s) {
-  if constexpr (M == M_JS) {
-    s = js_stencil(q);
-    return true;
-  } else {
-    return sr_stencil<M>(q, P, s);
-  }
-}
-
-// Reconstruct one stencil at `head`, falling back to JS weights if the closure is not finite and the
-// fallback option is set.
-template <int M>
-__device__ __forceinline__ double recon_one(const double q[5], int head, const typename ClosureParams<M>::type& P,
-                                            int opts, Tally& tally) {
-  StencilW s;
-  bool ok = stencil_weights<M>(q, P, s);
-  if (M != M_JS) {
-    tally.mlp += s.linear ? 0 : 1;
-    tally.plateau += s.linear ? 1 : 0;
-  }
-  double w[3], c[3];
-  if (!ok && (opts & OPT_JS_FALLBACK)) {
-    StencilW js = js_stencil(q);
-    js_head_weights(js, linear_weights(head), w);
-    ++tally.fallbacks;
-  } else {
-    head_weights<M>(s, head, (opts & OPT_ENO_CUTOFF) != 0, w);
-  }
-  candidates(q, head, c);
-  return combine(w, c);
-}
-
 __device__ __forceinline__ bool admissible(const d4& q, double g) {
   double rho = q.v[0];
   if (!(rho > 0.0)) return false;
@@ -130,120 +96,200 @@ __device__ __forceinline__ bool admissible(const d4& q, double g) {
 }
 
 // -------------------------------------------------------------------------------------------
-// Normal (characteristic) reconstruction.
-// DIR=1: cell (r, c), r in [1, ny+5), c in [0, nx+2): stencil padded (r, c..c+4), output xl/xr[r][c]
-//        of a [ny+6][nx+2] cell array.
-// DIR=2: cell (r, c), r in [0, ny+2), c in [1, nx+5): stencil padded (r..r+4, c), output yl/yr[r][c]
-//        of a [ny+2][nx+6] cell array.
-// The left face (lr=2, head 1) uses Roe(q1, q2); the right face (lr=1, head 0) uses Roe(q2, q3).
+// Closure work is compacted per block. Phase A: every thread forms its 8 stencils and the cheap
+// plateau sensors; plateau stencils take the linear weights at once; the others push their stencil id
+// (n * 128 + thread) onto a block queue in shared memory. Phase B: the 128 threads take queue entries
+// in turn and, for each, evaluate features, the MLP pair, the weights and the reconstructed value(s),
+// so the closure runs at full SIMT width wherever the wave fronts fall. Per-thread stencil state
+// lives in shared memory, which keeps every loop rolled (a small instruction footprint) and the
+// register count low.
+// -------------------------------------------------------------------------------------------
+constexpr int kBlock = 128;
+constexpr int kStencilsPerThread = 8;
+
+// Pushes the stencils of this warp that need the closure onto the block queue (warp-aggregated).
+__device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q, int* count) {
+  const unsigned m = __ballot_sync(0xffffffffu, need);
+  if (m == 0u) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == __ffs(m) - 1) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  if (need) q[base + __popc(m & ((1u << lane) - 1u))] = (unsigned short)id;
+}
+
+// SR closure of one non-plateau stencil -> reciprocal scaled betas (features FP64 as in DEPLOY:96-120,
+// the MLP in the closure precision, ratios averaged and inverted in FP64 as in DEPLOY:234-247).
+template <int M>
+__device__ __forceinline__ void sr_betas(const double s[5], const typename ClosureParams<M>::type& P,
+                                         double& a0, double& a1, double& a2) {
+  const Sens se = sensors5(s);
+  double f[5];
+  const double inv = 1.0 / fmax(se.dmax, 1.0e-15);
+  f[0] = se.d0 * inv;
+  f[1] = se.d1 * inv;
+  f[2] = se.d2 * inv;
+  f[3] = gamma_s(s);
+  // clip((log10(rel) + 4)/4, 0, 1): the logarithm is needed only when rel is strictly inside (1e-4, 1)
+  const double rel = fmax(se.dmax / se.qscale, 1.0e-30);
+  f[4] = rel >= 1.0 ? 1.0 : (rel <= 1.0e-4 ? 0.0 : fmin(1.0, fmax(0.0, (log(rel) / 2.302585092994046 + 4.0) / 4.0)));
+  typename QIn<M>::T x[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) x[k] = to_queue<M>(f[k]);
+  closure_from_features<M>(x, P, a0, a1, a2);
+}
+
+template <int M>
+__device__ __forceinline__ double sr_value(const double s[5], int head, double a0, double a1, double a2, int opts,
+                                           Tally& tally) {
+  double w[3], c[3];
+  const Lin3 d = linear_weights(head);
+  if (!(isfinite(a0) && isfinite(a1) && isfinite(a2)) && (opts & OPT_JS_FALLBACK)) {
+    js_head_weights(js_stencil(s), d, w);
+    ++tally.fallbacks;
+  } else {
+    StencilW sw;
+    sw.a0 = a0;
+    sw.a1 = a1;
+    sw.a2 = a2;
+    sw.linear = false;
+    sr_head_weights(sw, d, (opts & OPT_ENO_CUTOFF) != 0, w);
+  }
+  candidates(s, head, c);
+  return combine(w, c);
+}
+
+__device__ __forceinline__ double linear_value(const double s[5], int head) {
+  const Lin3 d = linear_weights(head);
+  double c[3];
+  candidates(s, head, c);
+  return d.d0 * c[0] + d.d1 * c[1] + d.d2 * c[2];
+}
+
+__device__ __forceinline__ double js_value(const double s[5], int head) {
+  double w[3], c[3];
+  js_head_weights(js_stencil(s), linear_weights(head), w);
+  candidates(s, head, c);
+  return combine(w, c);
+}
+
+// -------------------------------------------------------------------------------------------
+// Normal (characteristic) reconstruction, one thread per face: the Roe average of the two cells
+// next to the face and its eigenvectors serve both face values that use them -- the lr=1 value of
+// the cell on the left (stencil cells 0..4 of the six) and the lr=2 value of the cell on the right
+// (cells 1..5) -- so each Roe average and projection is computed once (the reference computes each
+// twice, once from each cell; DEPLOY:479-592).
+// DIR=1: face thread (r, c), r in [1, ny+5), c in [0, nx]: padded row r, columns c..c+5; writes
+//        out_r[r][c] (lr=1 of the cell centred at column c+2) and out_l[r][c+1] (lr=2 of column c+3),
+//        arrays [ny+6][nx+2].
+// DIR=2: face thread (r, c), r in [0, ny], c in [1, nx+5): padded column c, rows r..r+5; writes
+//        out_r[r][c] and out_l[r+1][c], arrays [ny+2][nx+6].
+// Stencil n = 2 f + side of a face: characteristic field f; side 0 -> cells 0..4 with head 0 (lr=1),
+// side 1 -> cells 1..5 with head 1 (lr=2).
 // -------------------------------------------------------------------------------------------
 template <int M, int DIR>
-__global__ void __launch_bounds__(128) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
-                                                double* __restrict__ out_r, int nx, int ny, int bc, double g,
-                                                const StepCtl* __restrict__ ctl, int opts, int* __restrict__ fallbacks,
-                                                unsigned long long* __restrict__ counters,
-                                                const __grid_constant__ typename ClosureParams<M>::type P) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+__global__ void __launch_bounds__(kBlock, 4) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
+                                                      double* __restrict__ out_r, int nx, int ny, int bc, double g,
+                                                      const StepCtl* __restrict__ ctl, int opts,
+                                                      int* __restrict__ fallbacks,
+                                                      unsigned long long* __restrict__ counters,
+                                                      const __grid_constant__ typename ClosureParams<M>::type P) {
+  __shared__ double s_ch[4][6][kBlock];                  // characteristic values, [field][cell][thread]
+  __shared__ double s_val[kStencilsPerThread][kBlock];   // reconstructed characteristic face values
+  __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
+  __shared__ int s_count;
+  if (ctl != nullptr && ctl->done) return;  // uniform across the launch
+  const int t = threadIdx.x;
+  const int c = blockIdx.x * kBlock + t;
+  const int r = blockIdx.y;
   const int nxt = nx + 2 * kGhost;
-  int r0, r1, c0, c1, ncols;
-  if (DIR == 1) {
-    r0 = 1; r1 = ny + 5; c0 = 0; c1 = nx + 2; ncols = nx + 2;
-  } else {
-    r0 = 0; r1 = ny + 2; c0 = 1; c1 = nx + 5; ncols = nx + 6;
-  }
-  if (r < r0 || r >= r1 || c < c0 || c >= c1) return;
-  if (ctl != nullptr && ctl->done) return;
+  const bool active = DIR == 1 ? (r >= 1 && r < ny + 5 && c <= nx) : (r <= ny && c >= 1 && c < nx + 5);
+  if (t == 0) s_count = 0;
   Tally tally;
-  d4 q[5];
+  RoeJ J;
+  {
+    d4 qc[6];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    int pj = DIR == 1 ? r : r + k;
-    int pi = DIR == 1 ? c + k : c;
-    q[k] = load_cell(u, nxt, map_index(pj, ny, bc), map_index(pi, nx, bc));
-  }
-  const size_t oidx = (size_t)r * ncols + c;
-#pragma unroll 1
-  for (int side = 0; side < 2; ++side) {
-    const int head = side == 0 ? 1 : 0;
-    d4 qa, qb;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      qa.v[k] = side == 0 ? q[1].v[k] : q[2].v[k];
-      qb.v[k] = side == 0 ? q[2].v[k] : q[3].v[k];
+    for (int k = 0; k < 6; ++k) {
+      if (active) {
+        const int pj = DIR == 1 ? r : r + k;
+        const int pi = DIR == 1 ? c + k : c;
+        qc[k] = load_cell(u, nxt, map_index(pj, ny, bc), map_index(pi, nx, bc));
+      } else {
+        qc[k] = d4{{1.0, 0.0, 0.0, 2.5}};  // inert filler for threads past the edge
+      }
     }
-    RoeJ J = roe_jacobian(qa, qb, g);
-    CharL L = char_left<DIR>(J, g);
-    // ch[f][k]: characteristic field f of stencil cell k. The field loop below stays rolled (one
-    // inlined closure) and rotates the rows so that every register-array index is a constant.
-    double ch[4][5];
+    J = roe_jacobian(qc[2], qc[3], g);
+    const CharL L = char_left<DIR>(J, g);
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
-      for (int k = 0; k < 5; ++k) ch[f][k] = project<DIR>(L, f, q[k]);
-    double cf[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int k = 0; k < 6; ++k) s_ch[f][k][t] = project<DIR>(L, f, qc[k]);
+  }
+  __syncthreads();
+  // Phase A
 #pragma unroll 1
-    for (int f = 0; f < 4; ++f) {
-      double v = recon_one<M>(ch[0], head, P, opts, tally);
+  for (int n = 0; n < kStencilsPerThread; ++n) {
+    const int f = n >> 1, side = n & 1;
+    double s[5];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        cf[a] = cf[a + 1];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) ch[a][k] = ch[a + 1][k];
-      }
-      cf[3] = v;
+    for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][t];
+    bool need = false;
+    if constexpr (M == M_JS) {
+      s_val[n][t] = js_value(s, side);
+    } else {
+      need = active && !is_plateau(sensors5(s));
+      if (!need) s_val[n][t] = linear_value(s, side);
+      if (active) ++(need ? tally.mlp : tally.plateau);
+      queue_push(need, n * kBlock + t, s_q, &s_count);
     }
-    d4 face = char_to_con<DIR>(cf, J);
-    if constexpr (M != M_JS) {
-      if ((opts & OPT_JS_FALLBACK) && !admissible(face, g)) {
-        // positivity fallback: redo this face with JS weights
-        double jf[4];
+  }
+  // Phase B
+  if constexpr (M != M_JS) {
+    __syncthreads();
+    const int count = s_count;
+#pragma unroll 1
+    for (int e = t; e < count; e += kBlock) {
+      const int id = s_q[e];
+      const int n = id / kBlock, o = id % kBlock, f = n >> 1, side = n & 1;
+      double s[5];
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          double s[5];
+      for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][o];
+      double a0, a1, a2;
+      sr_betas<M>(s, P, a0, a1, a2);
+      s_val[n][o] = sr_value<M>(s, side, a0, a1, a2, opts, tally);
+    }
+  }
+  __syncthreads();
+  if (active) {
 #pragma unroll
-          for (int k = 0; k < 5; ++k) s[k] = project<DIR>(L, f, q[k]);
-          StencilW js = js_stencil(s);
-          double w[3], cc[3];
-          js_head_weights(js, linear_weights(head), w);
-          candidates(s, head, cc);
-          jf[f] = combine(w, cc);
+    for (int side = 0; side < 2; ++side) {
+      double cf[4] = {s_val[side][t], s_val[2 + side][t], s_val[4 + side][t], s_val[6 + side][t]};
+      d4 face = char_to_con<DIR>(cf, J);
+      if constexpr (M != M_JS) {
+        if ((opts & OPT_JS_FALLBACK) && !admissible(face, g)) {
+          // positivity fallback: redo this face value with JS weights
+          double jf[4];
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            double s[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][t];
+            jf[f] = js_value(s, side);
+          }
+          face = char_to_con<DIR>(jf, J);
+          ++tally.fallbacks;
         }
-        face = char_to_con<DIR>(jf, J);
-        ++tally.fallbacks;
       }
+      size_t idx;
+      if (DIR == 1)
+        idx = (size_t)r * (nx + 2) + c + side;
+      else
+        idx = (size_t)(r + side) * (nx + 6) + c;
+      store_cell(side == 0 ? out_r : out_l, idx, face);
     }
-    store_cell(side == 0 ? out_l : out_r, oidx, face);
   }
   flush_tally(tally, opts, fallbacks, counters);
-}
-
-// Transverse reconstruction of one conserved component at both Gauss points (heads 2 and 3) from a
-// single closure evaluation.
-template <int M>
-__device__ __forceinline__ void gauss_pair(const double q[5], const typename ClosureParams<M>::type& P, int opts,
-                                           Tally& tally, double& g1, double& g2) {
-  StencilW s;
-  bool ok = stencil_weights<M>(q, P, s);
-  if (M != M_JS) {
-    tally.mlp += s.linear ? 0 : 1;
-    tally.plateau += s.linear ? 1 : 0;
-  }
-  double w[3], c[3];
-  const bool fb = !ok && (opts & OPT_JS_FALLBACK);
-  if (fb) {
-    s = js_stencil(q);
-    ++tally.fallbacks;
-  }
-#pragma unroll
-  for (int h = 2; h <= 3; ++h) {
-    if (fb)
-      js_head_weights(s, linear_weights(h), w);
-    else
-      head_weights<M>(s, h, (opts & OPT_ENO_CUTOFF) != 0, w);
-    candidates(q, h, c);
-    (h == 2 ? g1 : g2) = combine(w, c);
-  }
 }
 
 template <int DIR>
@@ -251,64 +297,112 @@ __device__ __forceinline__ d4 riemann(const d4& ul, const d4& ur, int flux, doub
   return flux == FLUX_FORCE ? force_flux<DIR>(ul, ur, dt_h, g) : hllc_flux<DIR>(ul, ur, g);
 }
 
+// Transverse reconstruction and flux, one thread per face.
 // x faces: face (j, i), j in [0, ny), i in [0, nx]: u_R from xl[j+1..j+5][i+1], u_L from xr[j+1..j+5][i]
 // (REFSYM:127-195). Output fx[j][i] of a [ny][nx+1] face array: (F(g1) + F(g2)) dt/dx.
 // y faces: face (j, i), j in [0, ny], i in [0, nx): u_R from yl[j+1][i+1..i+5], u_L from yr[j][i+1..i+5]
 // (REFSYM:198-266). Output fy[j][i] of a [ny+1][nx] face array.
+// Each of the 8 stencils (4 components x 2 sides) evaluates its closure once for both Gauss points.
+template <int DIR>
+__device__ __forceinline__ void load_transverse(const double* __restrict__ fl, const double* __restrict__ fr, int nx,
+                                                int i, int j, int n, bool active, double s[5]) {
+  const int comp = n >> 1, side = n & 1;
+  const double* src = side == 0 ? fl : fr;
+  if (!active) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s[k] = 0.0;
+    return;
+  }
+  if (DIR == 1) {
+    const int ncols = nx + 2, col = side == 0 ? i + 1 : i;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)(j + 1 + k) * ncols + col) * 4 + comp);
+  } else {
+    const int ncols = nx + 6, row = side == 0 ? j + 1 : j;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
+  }
+}
+
 template <int M, int DIR>
-__global__ void __launch_bounds__(128) k_flux(const double* __restrict__ fl, const double* __restrict__ fr,
-                                              double* __restrict__ fout, int nx, int ny, double g, int flux,
-                                              const StepCtl* __restrict__ ctl, int opts, int* __restrict__ fallbacks,
-                                              unsigned long long* __restrict__ counters,
-                                              const __grid_constant__ typename ClosureParams<M>::type P) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
-  if (i >= nfx || j >= nfy) return;
-  if (ctl->done) return;
+__global__ void __launch_bounds__(kBlock, 4) k_flux(const double* __restrict__ fl, const double* __restrict__ fr,
+                                                    double* __restrict__ fout, int nx, int ny, double g, int flux,
+                                                    const StepCtl* __restrict__ ctl, int opts,
+                                                    int* __restrict__ fallbacks,
+                                                    unsigned long long* __restrict__ counters,
+                                                    const __grid_constant__ typename ClosureParams<M>::type P) {
+  __shared__ double s_g[2][kStencilsPerThread][kBlock];  // values at Gauss points 1 and 2
+  __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
+  __shared__ int s_count;
+  if (ctl->done) return;  // uniform across the launch
+  const int t = threadIdx.x;
+  const int i0 = blockIdx.x * kBlock;
+  const int i = i0 + t;
+  const int j = blockIdx.y;
+  const int nfx = DIR == 1 ? nx + 1 : nx;
+  const bool active = i < nfx;
   const double dt_h = DIR == 1 ? ctl->dt_dx : ctl->dt_dy;
+  if (t == 0) s_count = 0;
+  __syncthreads();
   Tally tally;
-  // Eight stencils per face: n = 2*comp + side, side 0 -> u_R (from the lr=2 faces fl), side 1 -> u_L.
-  // Results rotate through g1/g2 so that indices stay constant inside the rolled loop.
-  double g1[8], g2[8];
+  // Phase A. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L (lr=1 faces fr).
 #pragma unroll 1
-  for (int n = 0; n < 8; ++n) {
-    const int comp = n >> 1, side = n & 1;
-    const double* src = side == 0 ? fl : fr;
+  for (int n = 0; n < kStencilsPerThread; ++n) {
     double s[5];
-    if (DIR == 1) {
-      const int ncols = nx + 2, col = side == 0 ? i + 1 : i;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)(j + 1 + k) * ncols + col) * 4 + comp);
+    load_transverse<DIR>(fl, fr, nx, i, j, n, active, s);
+    bool need = false;
+    if constexpr (M == M_JS) {
+      const StencilW js = js_stencil(s);
+      double w[3], c[3];
+      js_head_weights(js, linear_weights(2), w);
+      candidates(s, 2, c);
+      s_g[0][n][t] = combine(w, c);
+      js_head_weights(js, linear_weights(3), w);
+      candidates(s, 3, c);
+      s_g[1][n][t] = combine(w, c);
     } else {
-      const int ncols = nx + 6, row = side == 0 ? j + 1 : j;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
+      need = active && !is_plateau(sensors5(s));
+      if (!need) {
+        s_g[0][n][t] = linear_value(s, 2);
+        s_g[1][n][t] = linear_value(s, 3);
+      }
+      if (active) ++(need ? tally.mlp : tally.plateau);
+      queue_push(need, n * kBlock + t, s_q, &s_count);
     }
-    double a, b;
-    gauss_pair<M>(s, P, opts, tally, a, b);
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      g1[k] = g1[k + 1];
-      g2[k] = g2[k + 1];
+  }
+  // Phase B: one closure evaluation per queued stencil serves both Gauss points.
+  if constexpr (M != M_JS) {
+    __syncthreads();
+    const int count = s_count;
+#pragma unroll 1
+    for (int e = t; e < count; e += kBlock) {
+      const int id = s_q[e];
+      const int n = id / kBlock, o = id % kBlock;
+      double s[5];
+      load_transverse<DIR>(fl, fr, nx, i0 + o, j, n, true, s);
+      double a0, a1, a2;
+      sr_betas<M>(s, P, a0, a1, a2);
+      s_g[0][n][o] = sr_value<M>(s, 2, a0, a1, a2, opts, tally);
+      s_g[1][n][o] = sr_value<M>(s, 3, a0, a1, a2, opts, tally);
     }
-    g1[7] = a;
-    g2[7] = b;
   }
-  d4 ur1, ul1, ur2, ul2;
+  __syncthreads();
+  if (active) {
+    d4 ur1, ul1, ur2, ul2;
 #pragma unroll
-  for (int comp = 0; comp < 4; ++comp) {
-    ur1.v[comp] = g1[2 * comp];
-    ul1.v[comp] = g1[2 * comp + 1];
-    ur2.v[comp] = g2[2 * comp];
-    ul2.v[comp] = g2[2 * comp + 1];
+    for (int comp = 0; comp < 4; ++comp) {
+      ur1.v[comp] = s_g[0][2 * comp][t];
+      ul1.v[comp] = s_g[0][2 * comp + 1][t];
+      ur2.v[comp] = s_g[1][2 * comp][t];
+      ul2.v[comp] = s_g[1][2 * comp + 1][t];
+    }
+    d4 f1 = riemann<DIR>(ul1, ur1, flux, dt_h, g);
+    d4 f2 = riemann<DIR>(ul2, ur2, flux, dt_h, g);
+    d4 o;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] * dt_h + f2.v[k] * dt_h;
+    store_cell(fout, (size_t)j * nfx + i, o);
   }
-  d4 f1 = riemann<DIR>(ul1, ur1, flux, dt_h, g);
-  d4 f2 = riemann<DIR>(ul2, ur2, flux, dt_h, g);
-  d4 o;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] * dt_h + f2.v[k] * dt_h;
-  store_cell(fout, (size_t)j * nfx + i, o);
   flush_tally(tally, opts, fallbacks, counters);
 }
 
