@@ -87,7 +87,7 @@ __device__ __forceinline__ void store_cell(double* __restrict__ u, size_t idx, c
   p[1] = make_double2(q.v[2], q.v[3]);
 }
 
-__device__ __forceinline__ bool admissible(const d4& q, double g) {
+__device__ __forceinline__ bool admissible(const d4& q, double g) {  // rho > 0 and p > 0
   double rho = q.v[0];
   if (!(rho > 0.0)) return false;
   double u = q.v[1] / rho, v = q.v[2] / rho;
@@ -106,6 +106,9 @@ __device__ __forceinline__ bool admissible(const d4& q, double g) {
 // -------------------------------------------------------------------------------------------
 constexpr int kBlock = 128;
 constexpr int kStencilsPerThread = 8;
+// Resident blocks per SM the register budget targets: the FP64 MLP needs more registers.
+template <int M>
+constexpr int min_blocks() { return M == M_SR64 ? 3 : 4; }
 
 // Pushes the stencils of this warp that need the closure onto the block queue (warp-aggregated).
 __device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q, int* count) {
@@ -124,14 +127,40 @@ template <int M>
 __device__ __forceinline__ void sr_betas(const double s[5], const typename ClosureParams<M>::type& P,
                                          double& a0, double& a1, double& a2) {
   const Sens se = sensors5(s);
+#if WSR_FEATURES_F32
+  if constexpr (M != M_SR64) {
+    // FP32 closure: the differences are FP64 (they cancel), the normalisation, gamma and the scale
+    // feature are formed in FP32 (the MLP consumes FP32 inputs; dmax >= 1e-13 here, so every value is
+    // a normal float).
+    const double d20 = s[0] - 2.0 * s[1] + s[2], d21 = s[1] - 2.0 * s[2] + s[3], d22 = s[2] - 2.0 * s[3] + s[4];
+    const float inv = 1.0f / (float)se.dmax;
+    const float e = 1.0e-15f;
+    float x[5];
+    x[0] = (float)se.d0 * inv;
+    x[1] = (float)se.d1 * inv;
+    x[2] = (float)se.d2 * inv;
+    const float g0 = fabsf((float)d20) / ((float)(fabs(s[1] - s[0]) + fabs(s[2] - s[1])) + e);
+    const float g1 = fabsf((float)d21) / ((float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
+    const float g2 = fabsf((float)d22) / ((float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
+    x[3] = fminf(1.0f, fmaxf(fmaxf(g0, g1), g2));
+    const float rel = (float)(se.dmax / se.qscale);
+    x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (log10f(rel) + 4.0f) * 0.25f)));
+    if constexpr (M == M_SRBF16) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) x[k] = bf16r(x[k]);
+    }
+    closure_from_features<M>(x, P, a0, a1, a2);
+    return;
+  }
+#endif
   double f[5];
-  const double inv = 1.0 / fmax(se.dmax, 1.0e-15);
+  const double inv = rcp64(fmax(se.dmax, 1.0e-15));
   f[0] = se.d0 * inv;
   f[1] = se.d1 * inv;
   f[2] = se.d2 * inv;
   f[3] = gamma_s(s);
   // clip((log10(rel) + 4)/4, 0, 1): the logarithm is needed only when rel is strictly inside (1e-4, 1)
-  const double rel = fmax(se.dmax / se.qscale, 1.0e-30);
+  const double rel = fmax(se.dmax * rcp64(se.qscale), 1.0e-30);
   f[4] = rel >= 1.0 ? 1.0 : (rel <= 1.0e-4 ? 0.0 : fmin(1.0, fmax(0.0, (log(rel) / 2.302585092994046 + 4.0) / 4.0)));
   typename QIn<M>::T x[5];
 #pragma unroll
@@ -188,8 +217,8 @@ __device__ __forceinline__ double js_value(const double s[5], int head) {
 // side 1 -> cells 1..5 with head 1 (lr=2).
 // -------------------------------------------------------------------------------------------
 template <int M, int DIR>
-__global__ void __launch_bounds__(kBlock, 4) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
-                                                      double* __restrict__ out_r, int nx, int ny, int bc, double g,
+__global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
+                                                      double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
                                                       const StepCtl* __restrict__ ctl, int opts,
                                                       int* __restrict__ fallbacks,
                                                       unsigned long long* __restrict__ counters,
@@ -219,30 +248,33 @@ __global__ void __launch_bounds__(kBlock, 4) k_normal(const double* __restrict__
         qc[k] = d4{{1.0, 0.0, 0.0, 2.5}};  // inert filler for threads past the edge
       }
     }
-    J = roe_jacobian(qc[2], qc[3], g);
-    const CharL L = char_left<DIR>(J, g);
+    J = roe_jacobian(qc[2], qc[3], gas);
+    const CharL L = char_left<DIR>(J, gas);
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
       for (int k = 0; k < 6; ++k) s_ch[f][k][t] = project<DIR>(L, f, qc[k]);
   }
+  const bool work = active;
   __syncthreads();
   // Phase A
 #pragma unroll 1
   for (int n = 0; n < kStencilsPerThread; ++n) {
     const int f = n >> 1, side = n & 1;
-    double s[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][t];
     bool need = false;
-    if constexpr (M == M_JS) {
-      s_val[n][t] = js_value(s, side);
-    } else {
-      need = active && !is_plateau(sensors5(s));
-      if (!need) s_val[n][t] = linear_value(s, side);
-      if (active) ++(need ? tally.mlp : tally.plateau);
-      queue_push(need, n * kBlock + t, s_q, &s_count);
+    if (work) {
+      double s[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][t];
+      if constexpr (M == M_JS) {
+        s_val[n][t] = js_value(s, side);
+      } else {
+        need = !is_plateau(sensors5(s));
+        if (!need) s_val[n][t] = linear_value(s, side);
+        ++(need ? tally.mlp : tally.plateau);
+      }
     }
+    if constexpr (M != M_JS) queue_push(need, n * kBlock + t, s_q, &s_count);
   }
   // Phase B
   if constexpr (M != M_JS) {
@@ -267,7 +299,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_normal(const double* __restrict__
       double cf[4] = {s_val[side][t], s_val[2 + side][t], s_val[4 + side][t], s_val[6 + side][t]};
       d4 face = char_to_con<DIR>(cf, J);
       if constexpr (M != M_JS) {
-        if ((opts & OPT_JS_FALLBACK) && !admissible(face, g)) {
+        if ((opts & OPT_JS_FALLBACK) && !admissible(face, gas.g)) {
           // positivity fallback: redo this face value with JS weights
           double jf[4];
 #pragma unroll
@@ -293,8 +325,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_normal(const double* __restrict__
 }
 
 template <int DIR>
-__device__ __forceinline__ d4 riemann(const d4& ul, const d4& ur, int flux, double dt_h, double g) {
-  return flux == FLUX_FORCE ? force_flux<DIR>(ul, ur, dt_h, g) : hllc_flux<DIR>(ul, ur, g);
+__device__ __forceinline__ d4 riemann(const d4& ul, const d4& ur, int flux, double dt_h, const Gas& gas) {
+  return flux == FLUX_FORCE ? force_flux<DIR>(ul, ur, dt_h, gas.g) : hllc_flux<DIR>(ul, ur, gas);
 }
 
 // Transverse reconstruction and flux, one thread per face.
@@ -325,8 +357,8 @@ __device__ __forceinline__ void load_transverse(const double* __restrict__ fl, c
 }
 
 template <int M, int DIR>
-__global__ void __launch_bounds__(kBlock, 4) k_flux(const double* __restrict__ fl, const double* __restrict__ fr,
-                                                    double* __restrict__ fout, int nx, int ny, double g, int flux,
+__global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* __restrict__ fl, const double* __restrict__ fr,
+                                                    double* __restrict__ fout, int nx, int ny, Gas gas, int flux,
                                                     const StepCtl* __restrict__ ctl, int opts,
                                                     int* __restrict__ fallbacks,
                                                     unsigned long long* __restrict__ counters,
@@ -345,13 +377,16 @@ __global__ void __launch_bounds__(kBlock, 4) k_flux(const double* __restrict__ f
   if (t == 0) s_count = 0;
   __syncthreads();
   Tally tally;
+  const bool work = active;
   // Phase A. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L (lr=1 faces fr).
 #pragma unroll 1
   for (int n = 0; n < kStencilsPerThread; ++n) {
     double s[5];
-    load_transverse<DIR>(fl, fr, nx, i, j, n, active, s);
+    load_transverse<DIR>(fl, fr, nx, i, j, n, work, s);
     bool need = false;
-    if constexpr (M == M_JS) {
+    if (!work) {
+      // nothing to reconstruct
+    } else if constexpr (M == M_JS) {
       const StencilW js = js_stencil(s);
       double w[3], c[3];
       js_head_weights(js, linear_weights(2), w);
@@ -361,14 +396,14 @@ __global__ void __launch_bounds__(kBlock, 4) k_flux(const double* __restrict__ f
       candidates(s, 3, c);
       s_g[1][n][t] = combine(w, c);
     } else {
-      need = active && !is_plateau(sensors5(s));
+      need = !is_plateau(sensors5(s));
       if (!need) {
         s_g[0][n][t] = linear_value(s, 2);
         s_g[1][n][t] = linear_value(s, 3);
       }
-      if (active) ++(need ? tally.mlp : tally.plateau);
-      queue_push(need, n * kBlock + t, s_q, &s_count);
+      ++(need ? tally.mlp : tally.plateau);
     }
+    if constexpr (M != M_JS) queue_push(need, n * kBlock + t, s_q, &s_count);
   }
   // Phase B: one closure evaluation per queued stencil serves both Gauss points.
   if constexpr (M != M_JS) {
@@ -396,8 +431,8 @@ __global__ void __launch_bounds__(kBlock, 4) k_flux(const double* __restrict__ f
       ur2.v[comp] = s_g[1][2 * comp][t];
       ul2.v[comp] = s_g[1][2 * comp + 1][t];
     }
-    d4 f1 = riemann<DIR>(ul1, ur1, flux, dt_h, g);
-    d4 f2 = riemann<DIR>(ul2, ur2, flux, dt_h, g);
+    const d4 f1 = riemann<DIR>(ul1, ur1, flux, dt_h, gas);
+    const d4 f2 = riemann<DIR>(ul2, ur2, flux, dt_h, gas);
     d4 o;
 #pragma unroll
     for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] * dt_h + f2.v[k] * dt_h;

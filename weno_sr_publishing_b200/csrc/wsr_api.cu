@@ -194,28 +194,28 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t s
   {
     ProfScope ps(ctx, st, 0);
     dim3 grd((a.nx + 1 + 127) / 128, a.ny + 5);
-    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks,
+    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks,
                                         w.counters + 0, P);
   }
   WSR_LAUNCHED(ctx, "k_normal<x>");
   {
     ProfScope ps(ctx, st, 1);
     dim3 grd((a.nx + 5 + 127) / 128, a.ny + 1);
-    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks,
+    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks,
                                         w.counters + 2, P);
   }
   WSR_LAUNCHED(ctx, "k_normal<y>");
   {
     ProfScope ps(ctx, st, 2);
     dim3 grd((a.nx + 1 + 127) / 128, a.ny);
-    k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks,
+    k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
                                       w.counters + 4, P);
   }
   WSR_LAUNCHED(ctx, "k_flux<x>");
   {
     ProfScope ps(ctx, st, 3);
     dim3 grd((a.nx + 127) / 128, a.ny + 1);
-    k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks,
+    k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
                                       w.counters + 6, P);
   }
   WSR_LAUNCHED(ctx, "k_flux<y>");
@@ -597,13 +597,13 @@ template <int M>
 int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
   const dim3 blk(128);
   k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny + 5), blk, 0, st>>>(
-      a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
+      a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
   k_normal<M, 2><<<dim3((a.nx + 5 + 127) / 128, a.ny + 1), blk, 0, st>>>(
-      a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, a.g, w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
+      a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
   k_flux<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny), blk, 0, st>>>(
-      w.xl, w.xr, w.fx, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P);
+      w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P);
   k_flux<M, 2><<<dim3((a.nx + 127) / 128, a.ny + 1), blk, 0, st>>>(
-      w.yl, w.yr, w.fy, a.nx, a.ny, a.g, a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P);
+      w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P);
   k_update<<<dim3((a.nx + 255) / 256, a.ny), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk,
                                                           a.g, w.ctl);
   return cudaGetLastError() == cudaSuccess ? WSR_OK : WSR_ERR_CUDA;

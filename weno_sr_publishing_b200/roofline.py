@@ -25,34 +25,32 @@ HEAD64_PLATEAU = 20
 JS_STENCIL64 = 30
 JS_HEAD64 = 31
 
-# Non-closure FP64 per normal-reconstruction cell (two faces: Roe 72, eigenvectors 20,
-# 5 x 4 projections 140, back-projection 25) and per flux face (two HLLC 2 x 100, scaling 12).
-NORMAL_CELL64 = 2 * (72 + 20 + 140 + 25)
-FLUX_FACE64 = 2 * 100 + 12
+# Non-closure FP64 per normal-reconstruction face (Roe 60, eigenvectors 24, 6 cells x 4 fields of
+# projections 168, two back-projections 50) and per flux face (two HLLC 2 x 90, scaling 12).
+NORMAL_FACE64 = 60 + 24 + 168 + 50
+FLUX_FACE64 = 2 * 90 + 12
 UPDATE_CELL64 = 24
 
 BYTES_PER_CELL = {"normal_x": 96, "normal_y": 96, "flux_x": 96, "flux_y": 96, "update": 160}
 
 
-def kernel_work(kind: str, method: str, nx: int, ny: int, mlp: int = 0, plateau: int = 0) -> dict:
+def faces(kind: str, nx: int, ny: int) -> int:
+    return {"normal_x": (ny + 4) * (nx + 1), "normal_y": (ny + 1) * (nx + 4),
+            "flux_x": (nx + 1) * ny, "flux_y": nx * (ny + 1)}[kind]
+
+
+def kernel_work(kind: str, method: str, nx: int, ny: int, mlp: float = 0, plateau: float = 0) -> dict:
     """Work of ONE launch of kernel class `kind` on an nx x ny grid.
 
     mlp / plateau: closure tallies of that launch (device counters; 0 for JS)."""
-    cells_normal = (ny + 4) * (nx + 2) if kind == "normal_x" else (ny + 2) * (nx + 4)
-    faces = (nx + 1) * ny if kind == "flux_x" else nx * (ny + 1)
-    w32 = w64 = 0.0
-    if kind in ("normal_x", "normal_y"):
-        stencils = 8 * cells_normal
-        heads = 1
-        w64 += cells_normal * NORMAL_CELL64
-    elif kind in ("flux_x", "flux_y"):
-        stencils = 8 * faces
-        heads = 2
-        w64 += faces * FLUX_FACE64
-    else:
+    if kind == "update":
         return {"w32": 0.0, "w64": float(nx * ny * UPDATE_CELL64), "bytes": float(nx * ny * BYTES_PER_CELL[kind])}
+    work_faces = faces(kind, nx, ny)
+    w32 = w64 = 0.0
+    heads = 1 if kind.startswith("normal") else 2
+    w64 += work_faces * (NORMAL_FACE64 if kind.startswith("normal") else FLUX_FACE64)
     if method == "js":
-        w64 += stencils * (JS_STENCIL64 + heads * JS_HEAD64)
+        w64 += 8 * work_faces * (JS_STENCIL64 + heads * JS_HEAD64)
     else:
         pairs = mlp * MLP_PAIR_FLOPS
         if method == "sr_f64":
