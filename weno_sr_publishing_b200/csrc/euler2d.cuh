@@ -104,11 +104,14 @@ __device__ __forceinline__ bool admissible(const d4& q, double g) {  // rho > 0 
 // lives in shared memory, which keeps every loop rolled (a small instruction footprint) and the
 // register count low.
 // -------------------------------------------------------------------------------------------
+#ifndef WSR_MIN_BLOCKS
+#define WSR_MIN_BLOCKS 6
+#endif
 constexpr int kBlock = 128;
 constexpr int kStencilsPerThread = 8;
 // Resident blocks per SM the register budget targets: the FP64 MLP needs more registers.
 template <int M>
-constexpr int min_blocks() { return M == M_SR64 ? 3 : 4; }
+constexpr int min_blocks() { return M == M_SR64 ? 3 : WSR_MIN_BLOCKS; }
 
 // Pushes the stencils of this warp that need the closure onto the block queue (warp-aggregated).
 __device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q, int* count) {
@@ -133,18 +136,18 @@ __device__ __forceinline__ void sr_betas(const double s[5], const typename Closu
     // feature are formed in FP32 (the MLP consumes FP32 inputs; dmax >= 1e-13 here, so every value is
     // a normal float).
     const double d20 = s[0] - 2.0 * s[1] + s[2], d21 = s[1] - 2.0 * s[2] + s[3], d22 = s[2] - 2.0 * s[3] + s[4];
-    const float inv = 1.0f / (float)se.dmax;
+    const float inv = __frcp_rn((float)se.dmax);
     const float e = 1.0e-15f;
     float x[5];
     x[0] = (float)se.d0 * inv;
     x[1] = (float)se.d1 * inv;
     x[2] = (float)se.d2 * inv;
-    const float g0 = fabsf((float)d20) / ((float)(fabs(s[1] - s[0]) + fabs(s[2] - s[1])) + e);
-    const float g1 = fabsf((float)d21) / ((float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
-    const float g2 = fabsf((float)d22) / ((float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
+    const float g0 = __fdividef(fabsf((float)d20), (float)(fabs(s[1] - s[0]) + fabs(s[2] - s[1])) + e);
+    const float g1 = __fdividef(fabsf((float)d21), (float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
+    const float g2 = __fdividef(fabsf((float)d22), (float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
     x[3] = fminf(1.0f, fmaxf(fmaxf(g0, g1), g2));
-    const float rel = (float)(se.dmax / se.qscale);
-    x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (log10f(rel) + 4.0f) * 0.25f)));
+    const float rel = (float)se.dmax * __frcp_rn((float)se.qscale);
+    x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (__log10f(rel) + 4.0f) * 0.25f)));
     if constexpr (M == M_SRBF16) {
 #pragma unroll
       for (int k = 0; k < 5; ++k) x[k] = bf16r(x[k]);
@@ -237,23 +240,22 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
   Tally tally;
   RoeJ J;
   {
-    d4 qc[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      if (active) {
-        const int pj = DIR == 1 ? r : r + k;
-        const int pi = DIR == 1 ? c + k : c;
-        qc[k] = load_cell(u, nxt, map_index(pj, ny, bc), map_index(pi, nx, bc));
-      } else {
-        qc[k] = d4{{1.0, 0.0, 0.0, 2.5}};  // inert filler for threads past the edge
-      }
-    }
-    J = roe_jacobian(qc[2], qc[3], gas);
+    // cells are loaded one at a time for the projection (L1 hits after the first touch), which keeps
+    // the six-cell stencil out of the register budget
+    auto cell = [&](int k) {
+      if (!active) return d4{{1.0, 0.0, 0.0, 2.5}};  // inert filler for threads past the edge
+      const int pj = DIR == 1 ? r : r + k;
+      const int pi = DIR == 1 ? c + k : c;
+      return load_cell(u, nxt, map_index(pj, ny, bc), map_index(pi, nx, bc));
+    };
+    J = roe_jacobian(cell(2), cell(3), gas);
     const CharL L = char_left<DIR>(J, gas);
+#pragma unroll 1
+    for (int k = 0; k < 6; ++k) {
+      const d4 qk = cell(k);
 #pragma unroll
-    for (int f = 0; f < 4; ++f)
-#pragma unroll
-      for (int k = 0; k < 6; ++k) s_ch[f][k][t] = project<DIR>(L, f, qc[k]);
+      for (int f = 0; f < 4; ++f) s_ch[f][k][t] = project<DIR>(L, f, qk);
+    }
   }
   const bool work = active;
   __syncthreads();
