@@ -113,6 +113,15 @@ constexpr int kStencilsPerThread = 8;
 template <int M>
 constexpr int min_blocks() { return M == M_SR64 ? 3 : WSR_MIN_BLOCKS; }
 
+// Thread tiling of a 128-thread block: kernels whose stencils run along y use 32 x 4 tiles so that the
+// rows a block reads are shared in L1; kernels whose stencils run along x use 128 x 1.
+template <bool TALL>
+struct Tile {
+  static constexpr int bx = TALL ? 32 : kBlock, by = TALL ? 4 : 1;
+  __device__ static int x(int t) { return blockIdx.x * bx + (TALL ? (t & 31) : t); }
+  __device__ static int y(int t) { return blockIdx.y * by + (TALL ? (t >> 5) : 0); }
+};
+
 // Pushes the stencils of this warp that need the closure onto the block queue (warp-aggregated).
 __device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q, int* count) {
   const unsigned m = __ballot_sync(0xffffffffu, need);
@@ -231,9 +240,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
   __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
   __shared__ int s_count;
   if (ctl != nullptr && ctl->done) return;  // uniform across the launch
+  using TL = Tile<DIR == 2>;
   const int t = threadIdx.x;
-  const int c = blockIdx.x * kBlock + t;
-  const int r = blockIdx.y;
+  const int c = TL::x(t);
+  const int r = TL::y(t);
   const int nxt = nx + 2 * kGhost;
   const bool active = DIR == 1 ? (r >= 1 && r < ny + 5 && c <= nx) : (r <= ny && c >= 1 && c < nx + 5);
   if (t == 0) s_count = 0;
@@ -369,12 +379,12 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
   __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
   __shared__ int s_count;
   if (ctl->done) return;  // uniform across the launch
+  using TL = Tile<DIR == 1>;
   const int t = threadIdx.x;
-  const int i0 = blockIdx.x * kBlock;
-  const int i = i0 + t;
-  const int j = blockIdx.y;
-  const int nfx = DIR == 1 ? nx + 1 : nx;
-  const bool active = i < nfx;
+  const int i = TL::x(t);
+  const int j = TL::y(t);
+  const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
+  const bool active = i < nfx && j < nfy;
   const double dt_h = DIR == 1 ? ctl->dt_dx : ctl->dt_dy;
   if (t == 0) s_count = 0;
   __syncthreads();
@@ -416,7 +426,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       const int id = s_q[e];
       const int n = id / kBlock, o = id % kBlock;
       double s[5];
-      load_transverse<DIR>(fl, fr, nx, i0 + o, j, n, true, s);
+      load_transverse<DIR>(fl, fr, nx, TL::x(o), TL::y(o), n, true, s);
       double a0, a1, a2;
       sr_betas<M>(s, P, a0, a1, a2);
       s_g[0][n][o] = sr_value<M>(s, 2, a0, a1, a2, opts, tally);

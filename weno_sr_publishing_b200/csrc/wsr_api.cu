@@ -200,14 +200,14 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t s
   WSR_LAUNCHED(ctx, "k_normal<x>");
   {
     ProfScope ps(ctx, st, 1);
-    dim3 grd((a.nx + 5 + 127) / 128, a.ny + 1);
+    dim3 grd((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4);
     k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks,
                                         w.counters + 2, P);
   }
   WSR_LAUNCHED(ctx, "k_normal<y>");
   {
     ProfScope ps(ctx, st, 2);
-    dim3 grd((a.nx + 1 + 127) / 128, a.ny);
+    dim3 grd((a.nx + 1 + 31) / 32, (a.ny + 3) / 4);
     k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
                                       w.counters + 4, P);
   }
@@ -598,9 +598,9 @@ int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a,
   const dim3 blk(128);
   k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny + 5), blk, 0, st>>>(
       a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
-  k_normal<M, 2><<<dim3((a.nx + 5 + 127) / 128, a.ny + 1), blk, 0, st>>>(
+  k_normal<M, 2><<<dim3((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4), blk, 0, st>>>(
       a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
-  k_flux<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny), blk, 0, st>>>(
+  k_flux<M, 1><<<dim3((a.nx + 1 + 31) / 32, (a.ny + 3) / 4), blk, 0, st>>>(
       w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P);
   k_flux<M, 2><<<dim3((a.nx + 127) / 128, a.ny + 1), blk, 0, st>>>(
       w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P);
