@@ -63,10 +63,10 @@ void wsr_ctx_destroy(wsr_ctx *ctx);
 /* Message of the last failed call on this context (static storage inside the context). */
 const char *wsr_last_error(const wsr_ctx *ctx);
 
-/* Closure parameters: `packed` is a HOST array of n = 189 values in the order
- * w1[5][10] b1[10] w2[10][6] b2[6] w3[6][6] b3[6] w4[6][3] b4[3] ([in][out] row-major, the .npz
- * arrays without their leading dimension). The FP64, FP32 and BF16 methods use the values rounded
- * to their precision. `kind` must be 5 (WENO5). */
+/* Closure parameters: `packed` is a HOST array in the order w1 b1 w2 b2 w3 b3 w4 b4 ([in][out]
+ * row-major, the .npz arrays without their leading dimension): kind 5 (WENO5, 5->10->6->6->3) takes
+ * n = 189 values, kind 7 (WENO7, 6->24->16->16->4) n = 908. The FP64, FP32 and BF16 methods use the
+ * values rounded to their precision. */
 int wsr_closure_upload(wsr_ctx *ctx, int kind, const double *packed, int n);
 
 /* Bytes of device workspace the 2D functions need for an nx x ny interior. */
@@ -97,6 +97,28 @@ int wsr_euler2d_run(wsr_ctx *ctx, double *const u[4], int nx, int ny, double dx,
                     int check_interval, int fixed_steps, int max_steps, double *dts_host, int *steps_out,
                     double *t_out, int *final_slot, int *fallbacks_out, void *workspace, size_t workspace_bytes,
                     void *stream);
+
+/* ---- batched 1D periodic linear advection u_t + a u_x = 0 ----
+ * Replaces the reference's torch steppers (teacherfree_lab_weno5_v20_distance_balanced_mlp_f32_fast/
+ * rk3_advection.py:118-186 ssprk3_step_signed / rollout_distance; teacherfree_lab_weno7_rk4_distance_
+ * balanced_fast/rk4_advection.py:137-220 shu_rk4_step_signed / rollout_signed; for_paper_results/
+ * run_gste.py:103-118 integrate_ssprk3) for a ragged batch of B independent trajectories packed in u:
+ * trajectory b occupies u[offsets[b] .. offsets[b+1]) (n_b cells on a periodic grid of spacing dx[b]),
+ * advects with velocity[b] (its sign picks the upwind side), and takes n_full[b] steps of dt_full[b]
+ * followed, when dt_last[b] > 0, by one step of dt_last[b] (the reference's CFL schedule; the GSTE
+ * schedule is n_full steps of t/n_full). u is updated in place. order (optional, B entries) is the
+ * visiting order of trajectories (longest first balances the launch). nmax >= every n_b, at most 2048.
+ * scheme 5: WENO5 (5-point stencils, closure kind 5); scheme 7: WENO7 (7-point stencils, closure kind 7).
+ * All array arguments are device pointers. fallbacks_out, errors_out and counters_out (2 values: MLP
+ * evaluations, plateau stencils when opts has WSR_OPT_COUNT) are host pointers or NULL; when any is
+ * given the call synchronises `stream`. */
+#define WSR_INTEG_SSPRK3 0
+#define WSR_INTEG_SHU_RK4 1
+size_t wsr_adv1d_workspace_bytes(void);
+int wsr_adv1d_run(wsr_ctx *ctx, double *u, const long long *offsets, const int *order, const double *velocity,
+                  const double *dx, const int *n_full, const double *dt_full, const double *dt_last, int B, int nmax,
+                  int scheme, int method, int integrator, int opts, int *fallbacks_out, int *errors_out,
+                  unsigned long long *counters_out, void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- measurement hooks (no counterpart in the reference, which times whole runs with
  * time.perf_counter in for_paper_results/run_weno5_timing.py:111-140) ---- */

@@ -53,6 +53,10 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
                                           C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
                                           vp, sz, vp]
+            L.wsr_adv1d_workspace_bytes.argtypes = []
+            L.wsr_adv1d_workspace_bytes.restype = sz
+            L.wsr_adv1d_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, C.POINTER(i), C.POINTER(i),
+                                        C.POINTER(C.c_ulonglong), vp, sz, vp]
             L.wsr_profile_enable.argtypes = [vp, i]
             L.wsr_profile_read.argtypes = [vp, C.POINTER(d), C.POINTER(C.c_longlong)]
             L.wsr_euler2d_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
@@ -64,7 +68,8 @@ def lib() -> C.CDLL:
 def exported_symbols() -> list[str]:
     return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
             "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run",
-            "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops"]
+            "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops",
+            "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_euler2d_stage_noalloc"]
 
 
 def pack_params(params) -> np.ndarray:
@@ -91,7 +96,7 @@ class Context:
         if rc != WSR_OK:
             raise RuntimeError(f"wsr_ctx_create failed with status {rc}")
         self.handle = h
-        self._closure_key = None
+        self._closure_keys: dict[int, bytes] = {}
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -122,13 +127,16 @@ class Context:
         return out.value
 
     def upload_closure(self, packed: np.ndarray) -> None:
+        self.upload_closure_kind(5, packed)
+
+    def upload_closure_kind(self, kind: int, packed: np.ndarray) -> None:
         packed = np.ascontiguousarray(packed, dtype=np.float64)
         key = packed.tobytes()
-        if key == self._closure_key:
+        if self._closure_keys.get(kind) == key:
             return
-        self.check(lib().wsr_closure_upload(self.handle, 5, packed.ctypes.data_as(C.POINTER(C.c_double)),
+        self.check(lib().wsr_closure_upload(self.handle, kind, packed.ctypes.data_as(C.POINTER(C.c_double)),
                                             int(packed.size)))
-        self._closure_key = key
+        self._closure_keys[kind] = key
 
 
 _contexts: dict[int, Context] = {}

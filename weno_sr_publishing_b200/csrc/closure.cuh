@@ -56,6 +56,26 @@ struct ClosureParams<M_SRBF16> {
   using type = Mlp5f;  // pre-rounded to bfloat16 on upload
 };
 
+// Options bitmask. OPT_COUNT makes the reconstruction kernels count closure evaluations (SR stencils
+// that ran the MLP pair, and plateau stencils that took the linear weights) for the roofline tally.
+enum : int { OPT_ENO_CUTOFF = 1, OPT_JS_FALLBACK = 2, OPT_COUNT = 4 };
+
+// Per-thread tallies, flushed with one atomic each when OPT_COUNT is set.
+struct Tally {
+  int fallbacks = 0;
+  int mlp = 0;
+  int plateau = 0;
+};
+
+__device__ __forceinline__ void flush_tally(const Tally& t, int opts, int* fallbacks,
+                                            unsigned long long* counters) {
+  if (t.fallbacks) atomicAdd(fallbacks, t.fallbacks);
+  if ((opts & OPT_COUNT) && counters) {
+    if (t.mlp) atomicAdd(&counters[0], (unsigned long long)t.mlp);
+    if (t.plateau) atomicAdd(&counters[1], (unsigned long long)t.plateau);
+  }
+}
+
 // Heads: 0 face lr=1 (x_{i+1/2}^-), 1 face lr=2 (x_{i-1/2}^+), 2 Gauss loca=1, 3 Gauss loca=2.
 struct Lin3 {
   double d0, d1, d2;

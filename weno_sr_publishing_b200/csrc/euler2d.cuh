@@ -28,26 +28,6 @@ constexpr int kGhost = 3;
 enum Bc { BC_TRANSMISSIVE = 0, BC_PERIODIC = 1 };
 enum Flux { FLUX_HLLC = 0, FLUX_FORCE = 1 };
 
-// Options bitmask. OPT_COUNT makes the reconstruction kernels count closure evaluations (SR stencils
-// that ran the MLP pair, and plateau stencils that took the linear weights) for the roofline tally.
-enum : int { OPT_ENO_CUTOFF = 1, OPT_JS_FALLBACK = 2, OPT_COUNT = 4 };
-
-// Per-thread tallies, flushed with one atomic each when OPT_COUNT is set.
-struct Tally {
-  int fallbacks = 0;
-  int mlp = 0;
-  int plateau = 0;
-};
-
-__device__ __forceinline__ void flush_tally(const Tally& t, int opts, int* fallbacks,
-                                            unsigned long long* counters) {
-  if (t.fallbacks) atomicAdd(fallbacks, t.fallbacks);
-  if ((opts & OPT_COUNT) && counters) {
-    if (t.mlp) atomicAdd(&counters[0], (unsigned long long)t.mlp);
-    if (t.plateau) atomicAdd(&counters[1], (unsigned long long)t.plateau);
-  }
-}
-
 // Device-resident time-step control block (one per run).
 struct StepCtl {
   double t;          // simulated time reached

@@ -9,6 +9,7 @@
 #include <new>
 
 #include "../../include/wsr.h"
+#include "adv1d.cuh"
 #include "euler2d.cuh"
 
 using namespace wsr;
@@ -22,6 +23,10 @@ struct wsr_ctx {
   Mlp5d p64;
   Mlp5f p32;
   Mlp5f pbf16;
+  bool have_closure7;
+  Mlp7d q64;
+  Mlp7f q32;
+  Mlp7f qbf16;
   char err[512];
   double* host_pinned;  // small pinned mailbox for control-block reads
   // per-kernel CUDA-event timing (off unless wsr_profile_enable)
@@ -326,7 +331,17 @@ const char* wsr_last_error(const wsr_ctx* ctx) { return ctx ? ctx->err : "null c
 
 int wsr_closure_upload(wsr_ctx* ctx, int kind, const double* packed, int n) {
   if (!ctx) return WSR_ERR_ARG;
-  if (kind != 5) return fail(ctx, WSR_ERR_ARG, "closure kind %d not supported by the 2D path (5 = WENO5)", kind);
+  if (kind == 7) {
+    if (!packed || n != kParams7) return fail(ctx, WSR_ERR_ARG, "expected %d WENO7 parameters, got %d", kParams7, n);
+    for (int k = 0; k < kParams7; ++k) {
+      ctx->q64.p[k] = packed[k];
+      ctx->q32.p[k] = static_cast<float>(packed[k]);
+      ctx->qbf16.p[k] = __bfloat162float(__float2bfloat16_rn(static_cast<float>(packed[k])));
+    }
+    ctx->have_closure7 = true;
+    return WSR_OK;
+  }
+  if (kind != 5) return fail(ctx, WSR_ERR_ARG, "closure kind %d not supported (5 = WENO5, 7 = WENO7)", kind);
   if (!packed || n != kParams5) return fail(ctx, WSR_ERR_ARG, "expected %d WENO5 parameters, got %d", kParams5, n);
   for (int k = 0; k < kParams5; ++k) {
     ctx->p64.p[k] = packed[k];
@@ -504,6 +519,126 @@ int wsr_euler2d_counters(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Batched 1D advection
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+template <int SCHEME, int M>
+const typename AdvParams<SCHEME, M>::type& adv_params_of(const wsr_ctx* ctx);
+template <>
+const NoParams& adv_params_of<5, M_JS>(const wsr_ctx*) {
+  static const NoParams np{};
+  return np;
+}
+template <>
+const NoParams& adv_params_of<7, M_JS>(const wsr_ctx*) {
+  static const NoParams np{};
+  return np;
+}
+template <>
+const Mlp5d& adv_params_of<5, M_SR64>(const wsr_ctx* c) { return c->p64; }
+template <>
+const Mlp5f& adv_params_of<5, M_SR32>(const wsr_ctx* c) { return c->p32; }
+template <>
+const Mlp5f& adv_params_of<5, M_SRBF16>(const wsr_ctx* c) { return c->pbf16; }
+template <>
+const Mlp7d& adv_params_of<7, M_SR64>(const wsr_ctx* c) { return c->q64; }
+template <>
+const Mlp7f& adv_params_of<7, M_SR32>(const wsr_ctx* c) { return c->q32; }
+template <>
+const Mlp7f& adv_params_of<7, M_SRBF16>(const wsr_ctx* c) { return c->qbf16; }
+
+struct AdvArgs {
+  double* u;
+  const long long* offsets;
+  const int* order;
+  const double *vel, *dx;
+  const int* nfull;
+  const double *dtf, *dtl;
+  int B, nmax, opts;
+  int *fallbacks, *errors;
+  unsigned long long* counters;
+};
+
+template <int SCHEME, int M, int INTEG>
+int adv_launch(wsr_ctx* ctx, const AdvArgs& a, cudaStream_t st) {
+  const size_t smem = adv_smem_bytes<INTEG>(a.nmax);
+  auto kern = k_adv1d<SCHEME, M, INTEG>;
+  WSR_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<a.B, kAdvThreads, smem, st>>>(a.u, a.offsets, a.order, a.vel, a.dx, a.nfull, a.dtf, a.dtl, a.B, a.nmax,
+                                        a.opts, a.fallbacks, a.errors, a.counters, adv_params_of<SCHEME, M>(ctx));
+  WSR_LAUNCHED(ctx, "k_adv1d");
+  return WSR_OK;
+}
+
+template <int SCHEME, int INTEG>
+int adv_dispatch_m(wsr_ctx* ctx, int method, const AdvArgs& a, cudaStream_t st) {
+  switch (method) {
+    case WSR_METHOD_JS:
+      return adv_launch<SCHEME, M_JS, INTEG>(ctx, a, st);
+    case WSR_METHOD_SR_F64:
+      return adv_launch<SCHEME, M_SR64, INTEG>(ctx, a, st);
+    case WSR_METHOD_SR_F32:
+      return adv_launch<SCHEME, M_SR32, INTEG>(ctx, a, st);
+    default:
+      return adv_launch<SCHEME, M_SRBF16, INTEG>(ctx, a, st);
+  }
+}
+
+}  // namespace
+
+extern "C" size_t wsr_adv1d_workspace_bytes(void) { return 256; }
+
+extern "C" int wsr_adv1d_run(wsr_ctx* ctx, double* u, const long long* offsets, const int* order,
+                             const double* velocity, const double* dx, const int* n_full, const double* dt_full,
+                             const double* dt_last, int B, int nmax, int scheme, int method, int integrator, int opts,
+                             int* fallbacks_out, int* errors_out, unsigned long long* counters_out, void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  if (!ctx) return WSR_ERR_ARG;
+  if (B < 1) return fail(ctx, WSR_ERR_ARG, "B must be >= 1");
+  if (scheme != 5 && scheme != 7) return fail(ctx, WSR_ERR_ARG, "scheme must be 5 or 7 (got %d)", scheme);
+  if (integrator != WSR_INTEG_SSPRK3 && integrator != WSR_INTEG_SHU_RK4)
+    return fail(ctx, WSR_ERR_ARG, "bad integrator %d", integrator);
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
+  if (nmax < (scheme == 5 ? 5 : 7) || nmax > kAdvNmax)
+    return fail(ctx, WSR_ERR_ARG, "nmax must be in [%d, %d] (got %d)", scheme == 5 ? 5 : 7, kAdvNmax, nmax);
+  if (method != WSR_METHOD_JS && !(scheme == 5 ? ctx->have_closure : ctx->have_closure7))
+    return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before uploading a WENO%d closure", scheme);
+  if (!u || !offsets || !velocity || !dx || !n_full || !dt_full || !dt_last)
+    return fail(ctx, WSR_ERR_ARG, "null array argument");
+  if (!workspace || workspace_bytes < wsr_adv1d_workspace_bytes())
+    return fail(ctx, WSR_ERR_ARG, "workspace too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  int* fb = static_cast<int*>(workspace);
+  int* err = fb + 1;
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(static_cast<char*>(workspace) + 16);
+  WSR_CUDA(ctx, cudaMemsetAsync(workspace, 0, 32, st));
+  AdvArgs a{u, offsets, order, velocity, dx, n_full, dt_full, dt_last, B, nmax, opts, fb, err, cnt};
+  int rc;
+  if (scheme == 5)
+    rc = integrator == WSR_INTEG_SSPRK3 ? adv_dispatch_m<5, 0>(ctx, method, a, st) : adv_dispatch_m<5, 1>(ctx, method, a, st);
+  else
+    rc = integrator == WSR_INTEG_SSPRK3 ? adv_dispatch_m<7, 0>(ctx, method, a, st) : adv_dispatch_m<7, 1>(ctx, method, a, st);
+  if (rc) return rc;
+  if (fallbacks_out || errors_out || counters_out) {
+    int host[4];
+    unsigned long long hc[2];
+    WSR_CUDA(ctx, cudaMemcpyAsync(host, workspace, 16, cudaMemcpyDeviceToHost, st));
+    WSR_CUDA(ctx, cudaMemcpyAsync(hc, cnt, 16, cudaMemcpyDeviceToHost, st));
+    WSR_CUDA(ctx, cudaStreamSynchronize(st));
+    if (fallbacks_out) *fallbacks_out = host[0];
+    if (errors_out) *errors_out = host[1];
+    if (counters_out) {
+      counters_out[0] = hc[0];
+      counters_out[1] = hc[1];
+    }
+    if (host[1]) return fail(ctx, WSR_ERR_ARG, "%d trajectories had fewer cells than the stencil or more than nmax", host[1]);
+  }
+  return WSR_OK;
+}
 
 namespace {
 // Independent FMA chains for the peak-throughput probe (8 per thread).
