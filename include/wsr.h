@@ -120,6 +120,31 @@ int wsr_adv1d_run(wsr_ctx *ctx, double *u, const long long *offsets, const int *
                   int scheme, int method, int integrator, int opts, int *fallbacks_out, int *errors_out,
                   unsigned long long *counters_out, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- closure training through 1D advection trajectories (WENO5-SR + SSPRK3) ----
+ * Replaces the reference's autograd training objective (teacherfree_lab_weno5_v20_distance_balanced_
+ * mlp_f32_fast/fast_losses.py:412-648 fast_autoregressive_trajectory_loss and its loss.backward(),
+ * called from train.py:474-520) with the plain L1 loss
+ *     L = sum_{b, k = 1..steps, i} |u_{b,k,i} - e_{b,k,i}| / (B * steps * n)
+ * of B periodic trajectories of n cells (u0: B x n, row-major, device; NULL starts every trajectory from the
+ * exact cell averages of its profile), velocity[b] = +1 or -1, each taking
+ * `steps` SSPRK3 steps of dt on a grid of spacing dx, against the exact cell averages e of the advected
+ * profile desc[b] (B x WSR_PROFILE_LEN, device; layout of weno_sr_publishing_b200/profiles.py).
+ * method: WSR_METHOD_SR_F64 or WSR_METHOD_SR_F32 with the WENO5 closure of wsr_closure_upload.
+ * wsr_train1d_forward writes the loss to loss_out (1 double, device), the final states to u_final (B x n,
+ * device, or NULL), and keeps in the workspace the states of every ckpt_every-th step and the signs of
+ * u - e. wsr_train1d_backward then writes dL/dtheta (189 doubles, packed w1 b1 .. b4, device) to grad_out
+ * and, when grad_u0 is not NULL, dL/du0 (B x n, device): a hand-written adjoint that recomputes one
+ * checkpoint segment at a time. The backward call takes the same arguments and workspace as the forward
+ * call before it, with the closure unchanged in between. n <= 1024. The result is deterministic. */
+#define WSR_PROFILE_LEN 34
+size_t wsr_train1d_workspace_bytes(int B, int n, int steps, int ckpt_every);
+int wsr_train1d_forward(wsr_ctx *ctx, const double *u0, const double *desc, const double *velocity, int B, int n,
+                        double dx, double dt, int steps, int ckpt_every, int method, double *loss_out,
+                        double *u_final, void *workspace, size_t workspace_bytes, void *stream);
+int wsr_train1d_backward(wsr_ctx *ctx, const double *velocity, int B, int n, double dx, double dt, int steps,
+                         int ckpt_every, int method, double *grad_out, double *grad_u0, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
 /* ---- measurement hooks (no counterpart in the reference, which times whole runs with
  * time.perf_counter in for_paper_results/run_weno5_timing.py:111-140) ---- */
 

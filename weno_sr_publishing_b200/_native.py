@@ -57,6 +57,10 @@ def lib() -> C.CDLL:
             L.wsr_adv1d_workspace_bytes.restype = sz
             L.wsr_adv1d_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, C.POINTER(i), C.POINTER(i),
                                         C.POINTER(C.c_ulonglong), vp, sz, vp]
+            L.wsr_train1d_workspace_bytes.argtypes = [i, i, i, i]
+            L.wsr_train1d_workspace_bytes.restype = sz
+            L.wsr_train1d_forward.argtypes = [vp, vp, vp, vp, i, i, d, d, i, i, i, vp, vp, vp, sz, vp]
+            L.wsr_train1d_backward.argtypes = [vp, vp, i, i, d, d, i, i, i, vp, vp, vp, sz, vp]
             L.wsr_profile_enable.argtypes = [vp, i]
             L.wsr_profile_read.argtypes = [vp, C.POINTER(d), C.POINTER(C.c_longlong)]
             L.wsr_euler2d_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
@@ -69,7 +73,8 @@ def exported_symbols() -> list[str]:
     return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
             "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run",
             "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops",
-            "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_euler2d_stage_noalloc"]
+            "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
+            "wsr_train1d_backward", "wsr_euler2d_stage_noalloc"]
 
 
 def pack_params(params) -> np.ndarray:
