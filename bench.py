@@ -11,6 +11,15 @@ One JSON line on rank 0. Multi-GPU (torchrun): every rank advances its own repli
 (weak scaling; the step has no cross-replica exchange), timed as the max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--method sr_f32|sr_f64|js]
+
+Secondary workloads (--workload):
+  adv1d   4096 independent periodic 1D advection trajectories, N ~ U{100..1000}, a = +-1, distance
+          ~ {2, 8, 64, 128, 256, 512, 1024} cells at CFL 0.5, seeded profile families; WENO5-SR + SSPRK3
+          (--scheme 5) or WENO7-SR + Shu RK4 (--scheme 7). A step is one pass over the whole batch;
+          metric: cell-steps/s = sum_i N_i steps_i / time.
+  train1d closure training: one step is one forward + adjoint over B = 1024 trajectories of N = 256 cells
+          at one distance, the K timed steps walking the shuffled distance cycle; metric: trajectory
+          cell-steps/s (B N steps per training step / time).
 """
 from __future__ import annotations
 
@@ -42,6 +51,10 @@ def parse():
     ap.add_argument("--t0", type=float, default=0.125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-extras", action="store_true", help="no JS arm, e2e, CPU baseline (profiling runs)")
+    ap.add_argument("--workload", default="euler2d", choices=["euler2d", "adv1d", "train1d"],
+                    help="euler2d: the headline 2D step; adv1d: 4096 ragged 1D trajectories; train1d: closure "
+                         "training steps (B=1024, N=256)")
+    ap.add_argument("--scheme", type=int, default=5, choices=[5, 7], help="adv1d: WENO5/SSPRK3 or WENO7/Shu RK4")
     return ap.parse_args()
 
 
@@ -183,6 +196,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload != "euler2d":
+        bench_1d(args, world, rank, local)
+        return
     if args.impl == "reference":
         run_reference(args, rank)
         return
@@ -331,6 +347,305 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+DIST_CYCLE = (2, 8, 64, 128, 256, 512, 1024)
+
+
+def adv1d_batch(seed=0, B=4096):
+    """Ragged batch of the 1D inference workload: (initial states, velocities, N, steps)."""
+    from weno_sr_publishing_b200 import profiles as P
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(100, 1001, B)
+    dist = rng.choice(np.asarray(DIST_CYCLE), B)
+    vel = np.where(rng.random(B) < 0.5, -1.0, 1.0)
+    states = [None] * B
+    for n in np.unique(ns):
+        idx = np.flatnonzero(ns == n)
+        desc, _ = P.make_profiles(rng, idx.size, int(n))
+        u = P.cell_averages(desc, int(n), 0.0)
+        for j, b in enumerate(idx):
+            states[b] = u[j]
+    return states, vel, ns, 2 * dist
+
+
+def _closure(scheme, method):
+    from weno_sr_publishing_b200 import adv1d as A1
+    from weno_sr_publishing_b200.checkpoint import MODELS_DIR
+    from weno_sr_publishing_b200._native import pack_params
+    if method == "js":
+        return "classical"
+    name = {5: {"sr_f64": "weno5_sr_fp64_step012250.npz"}, 7: {}}.get(scheme, {}).get(
+        method, "weno5_sr_fp32_step016500.npz" if scheme == 5 else "weno7_sr_fp64_step016750.npz")
+    data = np.load(MODELS_DIR / name)
+    if scheme == 5:
+        packed = pack_params({k: data[k] for k in ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")})
+    else:
+        packed = np.concatenate([data[k].reshape(-1).astype(np.float64) for k in ("w1", "b1", "w2", "b2", "w3", "b3",
+                                                                                 "w4", "b4")])
+    return A1.Closure(scheme, packed, {"sr_f64": "f64", "sr_f32": "f32", "sr_bf16": "bf16"}[method])
+
+
+def _adv1d_cpu(states, vel, ns, steps, scheme, closure, budget_s):
+    """The oracle (numpy port of the reference's torch stepper) on a bounded sample of trajectories."""
+    from oracle import adv1d_oracle as AO
+    cl = None if closure == "classical" else (closure.kind, closure.precision, closure.packed)
+    integ = "ssprk3" if scheme == 5 else "shu_rk4"
+    work, t0, count = 0, time.perf_counter(), 0
+    for b in range(len(states)):
+        k = 4
+        AO.run(states[b], vel[b], 1.0 / ns[b], [0.5 / ns[b]] * k, scheme, cl, integ)
+        work += int(ns[b]) * k
+        count += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": work / el, "unit": "cell-steps/s", "cores": 1, "kind": "port",
+            "sample": f"4 steps of each of the first {count} trajectories ({work} cell-steps), numpy oracle, {el:.1f} s"}
+
+
+def _train_cpu(budget_s):
+    """The torch autograd oracle (forward + backward on the CPU) on B = 8 trajectories of N = 256."""
+    import torch
+    from oracle import train1d_oracle as TO
+    from weno_sr_publishing_b200 import profiles as P
+    from weno_sr_publishing_b200 import train1d as T1
+    rng = np.random.default_rng(5)
+    n, B, steps = 256, 8, 8
+    desc, _ = P.make_profiles(rng, B, n)
+    vel = T1.balanced_velocities(B)
+    u0 = P.cell_averages(desc, n, 0.0)
+    tg = np.stack([P.cell_averages(desc, n, vel * (k * 0.5 / n)) for k in range(1, steps + 1)], axis=1)
+    packed = T1.ClosureMLP(seed=83, dtype=torch.float32).packed().detach().double().numpy()
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        TO.loss_and_grads(packed, u0, tg, vel, 0.5 / n, float(n), "f32")
+        reps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": reps * B * n * steps / el, "unit": "cell-steps/s", "cores": torch.get_num_threads(),
+            "kind": "port", "sample": f"{reps} forward+backward of B={B}, N={n}, {steps} steps (torch autograd "
+                                      f"oracle, FP32 closure), {el:.1f} s"}
+
+
+def bench_1d(args, world, rank, local):
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+    if args.workload == "adv1d":
+        method = args.method
+        metric = f"1D batched advection cell-steps/s, WENO{args.scheme}-SR ({method}), 4096 ragged trajectories"
+        cfg = {"workload": "4096 periodic 1D advection trajectories, N~U{100..1000}, a=+-1, distance~"
+                           "{2,8,64,128,256,512,1024} cells, CFL 0.5, seeded profile families (seed 0)",
+               "scheme": f"WENO{args.scheme}", "integrator": "SSPRK3" if args.scheme == 5 else "Shu RK4",
+               "method": method, "l2_policy": "the 4096 trajectories stay in shared memory; HBM traffic is the "
+                                              "initial and final states only"}
+    else:
+        method = "sr_f32" if args.method not in ("sr_f32", "sr_f64") else args.method
+        metric = f"closure training cell-steps/s (forward + adjoint), WENO5-SR {method}, B=1024, N=256"
+        cfg = {"workload": "closure training, B=1024 trajectories of N=256 cells, distances cycling through "
+                           "{2,8,64,128,256,512,1024} cells at CFL 0.5, checkpoint every 32 steps",
+               "method": method, "loss": "mean L1 to exact cell averages at every completed step",
+               "l2_policy": "inputs larger than L2 for the long distances (checkpoints + stage scratch)"}
+    cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        if args.workload == "adv1d":
+            st, vel, ns, steps = adv1d_batch()
+            base = _adv1d_cpu(st, vel, ns, steps, args.scheme, _closure(args.scheme, method), args.cpu_seconds)
+        else:
+            base = _train_cpu(args.cpu_seconds)
+        line = {"metric": metric, "value": base["value"], "unit": base["unit"], "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                "impl": "reference", "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": base["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    from weno_sr_publishing_b200 import _native as N
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    stream = torch.cuda.current_stream(dev)
+    K, W = args.steps, max(args.warmup, 0)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def max_over_ranks(ms):
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return ms
+
+    line = {"metric": metric, "unit": "cell-steps/s", "n_gpus": world, "steps": K, "warmup": W,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfg}
+    if args.workload == "adv1d":
+        from weno_sr_publishing_b200 import adv1d as A1
+        states, vel, ns, steps = adv1d_batch()
+        closure = _closure(args.scheme, method)
+        cl = A1.as_closure(closure)
+        ctx = N.context(local)
+        if cl is not None:
+            ctx.upload_closure_kind(cl.kind, cl.packed)
+        B = len(states)
+        flat0 = torch.as_tensor(np.concatenate(states), device=dev)
+        flat = flat0.clone()
+        offs = torch.as_tensor(np.concatenate([[0], np.cumsum(ns)]), dtype=torch.int64, device=dev)
+        cost = ns * steps
+        order = torch.as_tensor(np.argsort(-cost, kind="stable").astype(np.int32), device=dev)
+        velt = torch.as_tensor(vel, device=dev)
+        dxs = torch.as_tensor(1.0 / ns, device=dev)
+        nf = torch.as_tensor(steps.astype(np.int32), device=dev)
+        dtf = torch.as_tensor(0.5 / ns, device=dev)
+        dtl = torch.zeros(B, dtype=torch.float64, device=dev)
+        wsb = int(N.lib().wsr_adv1d_workspace_bytes())
+        ws = torch.zeros(wsb + 256, dtype=torch.uint8, device=dev)
+        wp = (ws.data_ptr() + 255) // 256 * 256
+        P_ = C.c_void_p
+        meth = N.METHOD[method]
+        integ = 0 if args.scheme == 5 else 1
+        cnt = (C.c_ulonglong * 2)()
+
+        def launch(opts=0, counters=None):
+            ctx.check(N.lib().wsr_adv1d_run(ctx.handle, P_(flat.data_ptr()), P_(offs.data_ptr()),
+                                            P_(order.data_ptr()), P_(velt.data_ptr()), P_(dxs.data_ptr()),
+                                            P_(nf.data_ptr()), P_(dtf.data_ptr()), P_(dtl.data_ptr()), B,
+                                            int(ns.max()), args.scheme, meth, integ, opts, None, None, counters,
+                                            P_(wp), wsb, P_(stream.cuda_stream)))
+        for _ in range(W):
+            flat.copy_(flat0)
+            launch()
+        ms = 0.0
+        with ClockSampler(local) as clk:
+            for _ in range(K):
+                flat.copy_(flat0)
+                if world > 1:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                launch()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms += e0.elapsed_time(e1)
+        ms = max_over_ranks(ms)
+        work = float(np.sum(ns * steps))
+        line.update({"value": world * work * K / (ms * 1e-3), "ms_per_step": ms / K, "clocks": clk.summary(),
+                     "gpu_launches": K})
+        flat.copy_(flat0)
+        launch(N.OPT_COUNT, cnt)
+        mlp_n, plat_n = int(cnt[0]), int(cnt[1])
+        line["closure_tally_per_step"] = {"mlp": mlp_n, "plateau": plat_n}
+        # end to end through the public API: host arrays in, host arrays out, every step
+        integ_name = "ssprk3" if args.scheme == 5 else "shu_rk4"
+        A1.run_batched(states, vel, 1.0 / ns, steps, 0.5 / ns, scheme=args.scheme, model=closure,
+                       integrator=integ_name, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            outs, _ = A1.run_batched(states, vel, 1.0 / ns, steps, 0.5 / ns, scheme=args.scheme, model=closure,
+                                     integrator=integ_name, device=dev)
+            host = [o.cpu() for o in outs]
+        el = time.perf_counter() - t0
+        nbytes = int(np.sum(ns)) * 8
+        line["e2e"] = {"value": world * work * K / el, "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+                       "d2h_bytes_per_step": nbytes, "api": "weno_sr_publishing_b200.adv1d.run_batched (host arrays)"}
+        peak = ctx.peak_tflops(32 if method in ("sr_f32", "sr_bf16") else 64, C_stream(stream))
+        line["roofline"] = _roofline_1d(args.scheme, method, work, mlp_n, plat_n, ms / K, peak, ctx, stream)
+        if rank == 0 and world == 1:
+            line["cpu_baseline"] = _adv1d_cpu(states, vel, ns, steps, args.scheme, closure, args.cpu_seconds)
+    else:
+        from weno_sr_publishing_b200 import profiles as P1
+        from weno_sr_publishing_b200 import train1d as T1
+        rng = np.random.default_rng(83)
+        prec = "f32" if method == "sr_f32" else "f64"
+        model = T1.ClosureMLP(seed=83, dtype=torch.float32 if prec == "f32" else torch.float64)
+        with torch.no_grad():
+            g = torch.Generator().manual_seed(1)
+            for k in T1.PARAM_NAMES:
+                getattr(model, k).add_((0.2 * torch.randn(getattr(model, k).shape, generator=g,
+                                                          dtype=torch.float64)).to(getattr(model, k).dtype))
+        packed = model.packed().detach().double().numpy()
+        order = [DIST_CYCLE[T1.distance_index_for_step(s, 7, 83)] for s in range(1, K + W + 1)]
+        batches = [T1.TrajectoryBatch.sample(rng, 1024, 256, d, 0.5, dev, 32) for d in order]
+        ms, work, fwd_ms, bwd_ms = 0.0, 0.0, 0.0, 0.0
+        for b in batches[:W]:
+            r = T1._Run(b, packed, prec)
+            r.forward()
+            r.backward()
+        with ClockSampler(local) as clk:
+            for b in batches[W:]:
+                r = T1._Run(b, packed, prec)
+                if world > 1:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                e0, e1, e2 = ev(), ev(), ev()
+                e0.record(stream)
+                r.forward()
+                e1.record(stream)
+                r.backward()
+                e2.record(stream)
+                torch.cuda.synchronize()
+                fwd_ms += e0.elapsed_time(e1)
+                bwd_ms += e1.elapsed_time(e2)
+                work += b.B * b.n * b.steps
+        ms = max_over_ranks(fwd_ms + bwd_ms)
+        line.update({"value": world * work / (ms * 1e-3), "ms_per_step": ms / K, "clocks": clk.summary(),
+                     "gpu_launches": 4 * K, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                     "distances": [int(d) for d in order[W:]]})
+        # end to end through the autograd API: host profile descriptors in, host loss and gradient out
+        t0 = time.perf_counter()
+        for d in order[W:]:
+            desc, _ = P1.make_profiles(rng, 1024, 256)
+            b = T1.TrajectoryBatch(torch.as_tensor(desc).to(dev, non_blocking=True),
+                                   torch.as_tensor(T1.balanced_velocities(1024)).to(dev), 256,
+                                   T1.steps_for_distance(d, 0.5), 0.5 / 256)
+            model.zero_grad(set_to_none=True)
+            loss = T1.trajectory_loss(model.to(dev), b)
+            loss.backward()
+            _ = float(loss.detach()), model.w1.grad.cpu()
+        el = time.perf_counter() - t0
+        line["e2e"] = {"value": world * work / el, "unit": "cell-steps/s", "h2d_bytes_per_step": 1024 * 34 * 8 + 8192,
+                       "d2h_bytes_per_step": 8 + 189 * 8,
+                       "api": "weno_sr_publishing_b200.train1d.trajectory_loss(...).backward() with host profiles"}
+        if rank == 0 and world == 1:
+            line["cpu_baseline"] = _train_cpu(args.cpu_seconds)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _roofline_1d(scheme, method, work_cellsteps, mlp_n, plat_n, ms, peak, ctx, stream):
+    """Closure-bound roofline of the 1D step from the device tallies (3 stages per step; SSPRK3 for
+    WENO5): per MLP stencil the MLP pair in the closure precision plus the FP64 features and head, per
+    plateau stencil the sensors and linear head. Shu RK4 (WENO7) evaluates 4 right-hand sides with both
+    heads; its MLP is 6->24->16->16->4."""
+    from weno_sr_publishing_b200 import roofline as R
+    mlp_flops = R.MLP_PAIR_FLOPS if scheme == 5 else 2 * (2 * (6 * 24 + 24 * 16 + 16 * 16 + 16 * 4) + 56 * 3 + 25)
+    w_mlp = mlp_n * mlp_flops
+    w64 = mlp_n * (R.SENSORS64 + R.FEATURES64 + R.HEAD64) + plat_n * (R.SENSORS64 + R.HEAD64_PLATEAU)
+    w64 += work_cellsteps * 3 * 6
+    w32 = 0.0
+    if method == "sr_f64":
+        w64 += w_mlp
+    else:
+        w32 += w_mlp
+    peak64 = ctx.peak_tflops(64, C_stream(stream))
+    peak32 = ctx.peak_tflops(32, C_stream(stream))
+    b = R.bound({"w32": w32, "w64": w64, "bytes": 0.0}, ms * 1e-3, peak32, peak64, 6541.0)
+    return {"kernel": "k_adv1d", "bound": b["bound"], "achieved": b["achieved"], "peak": b["peak"], "unit": b["unit"],
+            "frac": b["frac"], "traffic": None,
+            "peak_source": {"fp32_tflops": f"measured FMA probe {peak32:.1f}",
+                            "fp64_tflops": f"measured FMA probe {peak64:.1f}"}}
 
 
 def C_stream(stream):

@@ -215,3 +215,39 @@ def test_invalid_arguments_raise():
         T.loss_and_grads(p, _batch(desc, [1.0, -1.0], 4, 2), "f64")  # n < 5
     with pytest.raises(ValueError):
         T.loss_and_grads(p, _batch(desc, [1.0, -1.0], 2048, 2), "f64")  # n > 1024
+
+
+def test_training_from_initialisation_beats_js(tmp_path):
+    """300 Adam steps from the reference's initialisation (FP32 closure, N = 96, B = 256, distances 2, 8,
+    64 cells) give a closure whose error under the reference's evaluation protocol (rk3_advection.py:533-560,
+    distance 20 cells, N = 96, balanced velocities) is below WENO5-JS for every profile family."""
+    cfg = T.TrainConfig(out_dir=tmp_path / "run", steps=300, grid=96, batch=256, distances=(2, 8, 64),
+                        precision="f32", lr=1e-3, lr_final=2e-4, log_interval=50, checkpoint_interval=1000,
+                        state_interval=1000, device=DEV)
+    out = T.train(cfg)
+    assert out["skipped"] == 0
+    rng = np.random.default_rng(104729)
+    ratios = []
+    for fam in P.FAMILIES:
+        desc, _ = P.make_profiles(rng, 8, 96, fam)
+        vel = T.balanced_velocities(8)
+        sr = T.final_state_error_signed(out["model"].closure(), desc, 96, 20.0, 0.5, vel, DEV)[0]
+        js = T.final_state_error_signed("classical", desc, 96, 20.0, 0.5, vel, DEV)[0]
+        ratios.append(sr / js)
+    assert max(ratios) < 1.0, ratios
+    assert float(np.mean(ratios)) < 0.7, ratios
+    # the written checkpoint is a reference-format closure
+    last = tmp_path / "run" / "checkpoints" / "model_step_000300.npz"
+    m = T.ClosureMLP.from_checkpoint(last, torch.float32)
+    assert torch.equal(m.packed(), out["model"].packed().detach().cpu())
+
+
+def test_resume_continues_bitwise(tmp_path):
+    """20 steps, then 20 more resumed from the saved state, equal 40 uninterrupted steps."""
+    kw = dict(steps=40, grid=64, batch=32, distances=(2, 8), precision="f64", lr=1e-3, lr_final=2e-4,
+              log_interval=10, checkpoint_interval=1000, state_interval=20, device=DEV)
+    a = T.train(T.TrainConfig(out_dir=tmp_path / "a", **kw))
+    T.train(T.TrainConfig(out_dir=tmp_path / "b", **kw), max_steps=20)
+    b = T.train(T.TrainConfig(out_dir=tmp_path / "b", **kw), resume=tmp_path / "b" / "state" / "latest.pt")
+    assert b["completed"] == 40
+    assert torch.equal(a["model"].packed(), b["model"].packed())
