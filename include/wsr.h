@@ -145,6 +145,33 @@ int wsr_train1d_backward(wsr_ctx *ctx, const double *velocity, int B, int n, dou
                          int ckpt_every, int method, double *grad_out, double *grad_u0, void *workspace,
                          size_t workspace_bytes, void *stream);
 
+/* ---- 3D Euler, WENO5 (JS / SR) with 2 x 2 Gauss-point transverse quadrature ----
+ * Replaces the reference's 3D Warp port (warp_weno5_3d_rk3/solver.py:165-329 Weno5Rk3Solver: _rk_stage,
+ * advance; kernels.py:776-1163). State layout: padded row-major q[nz+6][ny+6][nx+6][5] doubles, conserved
+ * (rho, rho u, rho v, rho w, E), ghost width 3, gamma 1.4 (config.py:45-52). Boundaries are transmissive;
+ * `inflow` (a HOST array of 5 conserved values, or NULL) instead fixes the x-low ghost cells.
+ * flux: WSR_FLUX3_EVILIN (the reference's interface state) or WSR_FLUX3_HLLC (HLLC in 3D, an addition).
+ * wsr_euler3d_stage runs one RK stage in place (stage 1 also saves the stage-start state in the workspace,
+ * which stages 2 and 3 use), with dt a host value. wsr_euler3d_run advances up to max_steps steps with dt
+ * = cfl min(dx, dy, dz) / max speed (1e10 below 1e-15) kept on the device, stopping at t_end (pass a huge
+ * t_end for a fixed number of steps); dts_host (capacity max_steps, or NULL) receives each step's dt. */
+#define WSR_FLUX3_EVILIN 0
+#define WSR_FLUX3_HLLC 1
+size_t wsr_euler3d_workspace_bytes(int nx, int ny, int nz);
+int wsr_euler3d_stage(wsr_ctx *ctx, double *q, int nx, int ny, int nz, double dx, double dy, double dz, double dt,
+                      int stage, int method, int flux, int opts, const double *inflow, void *workspace,
+                      size_t workspace_bytes, void *stream);
+int wsr_euler3d_max_speed(wsr_ctx *ctx, const double *q, int nx, int ny, int nz, double *out_host, void *workspace,
+                          size_t workspace_bytes, void *stream);
+int wsr_euler3d_run(wsr_ctx *ctx, double *q, int nx, int ny, int nz, double dx, double dy, double dz, double cfl,
+                    double t_start, double t_end, int max_steps, int method, int flux, int opts, const double *inflow,
+                    double *dts_host, int *steps_out, double *t_out, void *workspace, size_t workspace_bytes,
+                    void *stream);
+/* Closure tallies of the last 3D stage/run made with WSR_OPT_COUNT: out_host[6] = (MLP, plateau) stencils
+ * of the normal, first transverse and second transverse (flux) kernels. */
+int wsr_euler3d_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny, int nz,
+                         unsigned long long *out_host);
+
 /* ---- measurement hooks (no counterpart in the reference, which times whole runs with
  * time.perf_counter in for_paper_results/run_weno5_timing.py:111-140) ---- */
 

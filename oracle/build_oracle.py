@@ -1,4 +1,4 @@
-"""Build the CPU oracle shared library (test infrastructure; see euler2d_oracle.c).
+"""Build the CPU oracle shared library (test infrastructure; see euler2d_oracle.c and euler3d_oracle.c).
 
 Two builds are produced from the same sources:
 
@@ -15,7 +15,7 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SOURCES = ["euler2d_oracle.c"]
+SOURCES = ["euler2d_oracle.c", "euler3d_oracle.c"]
 
 
 def _cc(out: Path, flags: list[str]) -> None:

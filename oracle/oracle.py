@@ -47,6 +47,15 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_reconstruct_batch.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _fp, _dp]
         lib.or_mlp_ratios_batch.argtypes = [_dp, C.c_int, C.c_int, _dp, _fp, _dp]
         lib.or_num_threads.restype = C.c_int
+        _vp = C.c_void_p
+        lib.or_euler3d_run.restype = C.c_int
+        lib.or_euler3d_run.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _fp,
+                                       _vp, _dp, C.c_int]
+        lib.or_euler3d_max_speed.restype = C.c_double
+        lib.or_euler3d_max_speed.argtypes = [_dp, C.c_int, C.c_int, C.c_int]
+        lib.or_hllc5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
+        lib.or_evilin5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, _dp]
         _LIBS[name] = lib
     return _LIBS[name]
 
@@ -136,3 +145,42 @@ def euler2d_run(initial, nx, ny, dx, dy, cfl, t_end, method, bc="transmissive", 
 
 def num_threads(fast: bool = True) -> int:
     return int(_lib(fast).or_num_threads())
+
+
+FLUX3 = {"evilin": 0, "hllc": 1}
+
+
+def euler3d_run(q, nx, ny, nz, dx, dy, dz, cfl, steps, method, flux="evilin", params=None, inflow=None,
+                t_start=0.0, t_end=1.0e30, stage_only=False, fast=False):
+    """Advance the padded 3D state q[nz+6][ny+6][nx+6][5] by `steps` steps (a copy is returned with the
+    per-step dt). stage_only: only the first RK stage of the first step."""
+    out = np.array(q, dtype=np.float64, copy=True, order="C")
+    p64, p32 = _params(params)
+    dts = np.zeros(max(steps, 1))
+    inf = None if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64)
+    taken = _lib(fast).or_euler3d_run(out, nx, ny, nz, dx, dy, dz, cfl, t_start, t_end, steps, METHOD[method],
+                                      FLUX3[flux], p64, p32, None if inf is None else inf.ctypes.data, dts,
+                                      int(stage_only))
+    if taken < 0:
+        raise MemoryError("oracle allocation failed")
+    return out, dts[:taken]
+
+
+def euler3d_max_speed(q, nx, ny, nz) -> float:
+    return float(_lib().or_euler3d_max_speed(np.ascontiguousarray(q, dtype=np.float64), nx, ny, nz))
+
+
+def hllc5(ul, ur, direction: int) -> np.ndarray:
+    ul = np.ascontiguousarray(ul, dtype=np.float64).reshape(-1, 5)
+    ur = np.ascontiguousarray(ur, dtype=np.float64).reshape(-1, 5)
+    out = np.empty_like(ul)
+    _lib().or_hllc5_batch(ul, ur, ul.shape[0], direction, out)
+    return out
+
+
+def evilin5(ul, ur, direction: int, dt_dx: float) -> np.ndarray:
+    ul = np.ascontiguousarray(ul, dtype=np.float64).reshape(-1, 5)
+    ur = np.ascontiguousarray(ur, dtype=np.float64).reshape(-1, 5)
+    out = np.empty_like(ul)
+    _lib().or_evilin5_batch(ul, ur, ul.shape[0], direction, dt_dx, out)
+    return out

@@ -11,7 +11,8 @@ Semantics reproduced:
   scalars, so float32 arithmetic stays float32 (NEP 50 weak Python scalars).
 * vectors (``wp.vec4d``, ``wp.types.vector``) are fixed-length lists that cast on construction.
 * ``wp.launch`` runs the kernel body once per index of ``dim`` with ``wp.tid()`` returning it.
-* ``wp.atomic_add`` is a plain add (the launch loop is sequential).
+* ``wp.atomic_add`` / ``atomic_max`` / ``atomic_min`` are plain updates (the launch loop is sequential).
+* matrices (``wp.types.matrix``) are indexed ``m[row, column]``; arrays of any rank are numpy arrays.
 
 Known difference from the GPU build: Warp compiles through NVRTC, which contracts ``a*b+c`` into
 fused multiply-adds; Python does not. That changes FP64 results by a few ulp per operation.
@@ -62,7 +63,32 @@ vec4d = _vector_type(4, float64)
 vec3f = _vector_type(3, float32)
 vec4f = _vector_type(4, float32)
 
-types_ns = _types.SimpleNamespace(vector=lambda length, dtype: _vector_type(length, dtype))
+class _Mat:
+    SHAPE = (0, 0)
+    DTYPE = float
+
+    def __init__(self, *args):
+        r, c = self.SHAPE
+        self._v = [[self.DTYPE(0.0)] * c for _ in range(r)]
+        if len(args) == 1 and isinstance(args[0], _Mat):
+            self._v = [list(row) for row in args[0]._v]
+
+    def __getitem__(self, rc):
+        r, c = rc
+        return self._v[r][c]
+
+    def __setitem__(self, rc, value):
+        r, c = rc
+        self._v[r][c] = self.DTYPE(value)
+
+
+def _matrix_type(shape, dtype):
+    cast = float if dtype is float64 else float32
+    return type(f"mat{shape[0]}{shape[1]}", (_Mat,), {"SHAPE": tuple(shape), "DTYPE": staticmethod(cast)})
+
+
+types_ns = _types.SimpleNamespace(vector=lambda length, dtype: _vector_type(length, dtype),
+                                  matrix=lambda shape, dtype: _matrix_type(shape, dtype))
 
 
 def constant(x):
@@ -90,6 +116,19 @@ class _Array(np.ndarray):
     def numpy(self):
         return np.asarray(self).copy()
 
+    def __getitem__(self, idx):
+        # Warp does not bounds-check reads: some reference kernels load a default stencil before they
+        # pick the direction they use, reading one row past the array and discarding the value. Such a
+        # read returns 0 here instead of raising.
+        if isinstance(idx, tuple) and len(idx) == self.ndim and all(type(i) is int for i in idx):
+            if any(i < 0 or i >= n for i, n in zip(idx, self.shape)):
+                return 0.0
+        return super().__getitem__(idx)
+
+    def zero_(self):
+        self[...] = 0
+        return self
+
 
 def _np_dtype(dtype):
     return np.float32 if dtype is float32 else (np.int32 if dtype is int32 else np.float64)
@@ -112,6 +151,23 @@ def array2d(dtype=float64):
 
 
 array3d = array2d
+array4d = array2d
+
+
+def empty(shape, dtype=float64, device=None, requires_grad=False):
+    return zeros(shape, dtype, device, requires_grad)
+
+
+def get_device(_name=None):
+    return None
+
+
+def synchronize_device(_device=None):
+    return None
+
+
+def set_module_options(_options):
+    return None
 
 
 def launch(kernel_fn, dim, inputs, device=None, outputs=None):
@@ -133,11 +189,21 @@ def atomic_add(arr, index, value):
     arr[index] = arr[index] + value
 
 
+def atomic_max(arr, index, value):
+    if value > arr[index]:
+        arr[index] = value
+
+
+def atomic_min(arr, index, value):
+    if value < arr[index]:
+        arr[index] = value
+
+
 def _unary(f_np, f_math):
     def op(x):
-        if isinstance(x, np.floating):
+        if isinstance(x, np.float32):
             return f_np(x)
-        return f_math(x)
+        return f_math(float(x))
     return op
 
 

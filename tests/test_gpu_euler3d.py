@@ -1,0 +1,141 @@
+"""CUDA 3D Euler WENO5 step against the reference's own solver (fixtures), the C oracle and properties."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from weno_sr_publishing_b200 import euler3d as E3
+from weno_sr_publishing_b200 import problems as PR
+
+pytestmark = pytest.mark.gpu
+
+G = Path(__file__).resolve().parent / "golden"
+M = Path(__file__).resolve().parents[1] / "weno_sr_publishing_b200" / "models"
+DEV = "cuda:0"
+P64 = {k: v for k, v in np.load(M / "weno5_sr_fp64_step012250.npz").items() if k != "meta_json"}
+P32 = {k: v for k, v in np.load(M / "weno5_sr_fp32_step016500.npz").items() if k != "meta_json"}
+PARAMS = {"js": None, "sr_f64": P64, "sr_f32": P32}
+# relative max-norm tolerances against the reference / the oracle: the JS path is bitwise, the SR closures
+# differ in exp/log/reciprocal rounding (and the FP32 closure forms its features in FP32)
+TOL = {"js": 0.0, "sr_f64": 1e-12, "sr_f32": 2e-6}
+INNER = (slice(3, -3),) * 3
+
+
+def _rel(a, b):
+    a, b = np.asarray(a)[INNER], np.asarray(b)[INNER]
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def _fixture(case):
+    path = G / f"3d_{case}.npz"
+    if not path.exists():
+        pytest.skip(f"{path.name} not generated")
+    return np.load(path)
+
+
+@pytest.mark.parametrize("case,method", [("ic", "js"), ("js", "js"), ("sr_f64", "sr_f64"), ("sr_f32", "sr_f32")])
+def test_matches_reference_solver(case, method):
+    g = _fixture(case)
+    nx, ny, nz = int(g["nx"]), int(g["ny"]), int(g["nz"])
+    dx, dy, dz, cfl = float(g["dx"]), float(g["dy"]), float(g["dz"]), float(g["cfl"])
+    q = torch.as_tensor(g["q_init"], device=DEV).contiguous()
+    E3.stage(q, nx, ny, nz, dx, dy, dz, float(g["stage1_dt"]), 1, method, mlp_params=PARAMS[method])
+    assert _rel(q.cpu().numpy(), g["q_stage1"]) <= TOL[method]
+    q = torch.as_tensor(g["q_init"], device=DEV).contiguous()
+    t_end = 2.0e-5 if case == "ic" else 1.0
+    res = E3.run(q, nx, ny, nz, dx, dy, dz, cfl, method, mlp_params=PARAMS[method], t_end=t_end,
+                 steps=len(g["dts"]))
+    assert res.steps == len(g["dts"])
+    assert np.abs(res.dts - g["dts"]).max() <= TOL[method] * np.abs(g["dts"]).max()
+    assert _rel(q.cpu().numpy(), g[f"q_step{len(g['dts'])}"]) <= TOL[method]
+
+
+def _random_state(nx, ny, nz, seed):
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid((np.arange(nz) + 0.5) / nz, (np.arange(ny) + 0.5) / ny, (np.arange(nx) + 0.5) / nx,
+                          indexing="ij")
+    front = x + 0.3 * y - 0.4 * z + 0.1 * rng.uniform() > 0.6
+    rho = np.where(front, 0.7, 1.2) + 0.1 * np.sin(2 * np.pi * (y + z))
+    u = np.where(front, 0.1, 0.3)
+    v = 0.2 * np.cos(2 * np.pi * x)
+    w = 0.1 * np.sin(2 * np.pi * y)
+    p = np.where(front, 0.8, 1.2) + 0.05 * np.cos(2 * np.pi * z)
+    inner = np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], axis=-1)
+    return np.pad(inner, ((3, 3), (3, 3), (3, 3), (0, 0)), mode="edge")
+
+
+@pytest.mark.parametrize("flux", ["evilin", "hllc"])
+@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32"])
+def test_matches_oracle_ragged_grid(method, flux):
+    nx, ny, nz = 19, 11, 9
+    h = (1.0 / nx, 1.0 / ny, 0.8 / nz)
+    q0 = _random_state(nx, ny, nz, 3)
+    ref, dts = O.euler3d_run(q0, nx, ny, nz, *h, 0.3, 3, method, flux, PARAMS[method])
+    q = torch.as_tensor(q0, device=DEV).contiguous()
+    res = E3.run(q, nx, ny, nz, *h, 0.3, method, flux, PARAMS[method], steps=3)
+    assert np.abs(res.dts - dts).max() <= TOL[method] * dts.max()
+    assert _rel(q.cpu().numpy(), ref) <= TOL[method]
+
+
+def test_inflow_boundary_matches_oracle():
+    sb = PR.ShockBubble.seeded(1, 24, 10, 10)
+    q0 = sb.state()
+    dx, dy, dz = sb.spacing
+    ref, dts = O.euler3d_run(q0, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, 4, "js", "hllc", None, inflow=sb.inflow())
+    q = torch.as_tensor(q0, device=DEV).contiguous()
+    res = E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, "js", "hllc", inflow=sb.inflow(), steps=4)
+    assert np.array_equal(res.dts, dts)
+    assert np.array_equal(q.cpu().numpy()[INNER], ref[INNER])
+
+
+def test_uniform_flow_is_preserved():
+    nx, ny, nz = 12, 10, 8
+    inner = np.broadcast_to(np.array([1.3, 1.3 * 0.4, -1.3 * 0.2, 1.3 * 0.1, 2.0 / 0.4 + 0.5 * 1.3 * 0.21]),
+                            (nz, ny, nx, 5))
+    q0 = np.pad(inner, ((3, 3), (3, 3), (3, 3), (0, 0)), mode="edge")
+    for method in ("js", "sr_f64"):
+        q = torch.as_tensor(q0, device=DEV).contiguous()
+        E3.run(q, nx, ny, nz, 0.1, 0.1, 0.1, 0.4, method, "hllc", PARAMS[method], steps=3)
+        assert np.abs(q.cpu().numpy()[INNER] - q0[INNER]).max() <= 1e-13 * np.abs(q0).max()
+
+
+def test_planar_data_stays_planar():
+    """Data that vary along x only stay uniform on every y-z plane, bit for bit (every cell of a plane sees
+    the same inputs), for the SR closure and both fluxes."""
+    nx, ny, nz = 16, 7, 6
+    x = (np.arange(nx) + 0.5) / nx
+    rho = 1.0 + 0.4 * np.tanh((x - 0.5) * 20)
+    u, p = 0.3 + 0 * x, 1.0 + 0.2 * np.sin(2 * np.pi * x)
+    line = np.stack([rho, rho * u, 0 * x, 0 * x, p / 0.4 + 0.5 * rho * u * u], axis=-1)
+    q0 = np.pad(np.broadcast_to(line, (nz, ny, nx, 5)), ((3, 3), (3, 3), (3, 3), (0, 0)), mode="edge")
+    for flux in ("evilin", "hllc"):
+        q = torch.as_tensor(np.ascontiguousarray(q0), device=DEV)
+        E3.run(q, nx, ny, nz, 1.0 / nx, 0.1, 0.1, 0.4, "sr_f64", flux, P64, steps=3)
+        out = q.cpu().numpy()[INNER]
+        assert np.array_equal(out, np.broadcast_to(out[:1, :1], out.shape))
+        assert np.abs(out[..., 2:4]).max() == 0.0
+
+
+def test_max_speed_and_t_end_clipping():
+    nx, ny, nz = 8, 7, 6
+    q0 = _random_state(nx, ny, nz, 5)
+    q = torch.as_tensor(q0, device=DEV).contiguous()
+    assert E3.max_speed(q, nx, ny, nz) == O.euler3d_max_speed(q0, nx, ny, nz)
+    ref, dts = O.euler3d_run(q0, nx, ny, nz, 0.1, 0.1, 0.1, 0.4, 50, "js", "evilin", t_end=0.05)
+    res = E3.run(q, nx, ny, nz, 0.1, 0.1, 0.1, 0.4, "js", t_end=0.05)
+    assert res.steps == len(dts) and res.t == 0.05
+    assert np.array_equal(res.dts, dts)
+    assert np.array_equal(q.cpu().numpy()[INNER], ref[INNER])
+
+
+def test_invalid_arguments_raise():
+    q = torch.zeros((10, 10, 10, 5), dtype=torch.float64, device=DEV)
+    with pytest.raises(ValueError):
+        E3.run(q, 4, 4, 4, 0.1, 0.1, 0.1, 0.4, "js", steps=1)  # fewer than 5 cells
+    q = torch.zeros((11, 11, 11, 5), dtype=torch.float64, device=DEV)
+    with pytest.raises(ValueError):
+        E3.run(q, 5, 5, 5, 0.1, 0.1, 0.1, 0.4, "sr_f64", steps=1)  # SR without parameters

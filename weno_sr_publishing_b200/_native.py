@@ -18,6 +18,7 @@ WSR_OK, WSR_ERR_ARG, WSR_ERR_CUDA, WSR_ERR_NO_CLOSURE = 0, 1, 2, 3
 METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3}
 BC = {"transmissive": 0, "periodic": 1}
 FLUX = {"hllc": 0, "force": 1}
+FLUX3 = {"evilin": 0, "hllc": 1}
 OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT = 1, 2, 4
 PROF_KINDS = ("normal_x", "normal_y", "flux_x", "flux_y", "update", "control")
 N_PARAMS5 = 189
@@ -61,6 +62,13 @@ def lib() -> C.CDLL:
             L.wsr_train1d_workspace_bytes.restype = sz
             L.wsr_train1d_forward.argtypes = [vp, vp, vp, vp, i, i, d, d, i, i, i, vp, vp, vp, sz, vp]
             L.wsr_train1d_backward.argtypes = [vp, vp, i, i, d, d, i, i, i, vp, vp, vp, sz, vp]
+            L.wsr_euler3d_workspace_bytes.argtypes = [i, i, i]
+            L.wsr_euler3d_workspace_bytes.restype = sz
+            L.wsr_euler3d_stage.argtypes = [vp, vp, i, i, i, d, d, d, d, i, i, i, i, vp, vp, sz, vp]
+            L.wsr_euler3d_max_speed.argtypes = [vp, vp, i, i, i, C.POINTER(d), vp, sz, vp]
+            L.wsr_euler3d_run.argtypes = [vp, vp, i, i, i, d, d, d, d, d, d, i, i, i, i, vp, vp, C.POINTER(i),
+                                          C.POINTER(d), vp, sz, vp]
+            L.wsr_euler3d_counters.argtypes = [vp, vp, sz, i, i, i, C.POINTER(C.c_ulonglong)]
             L.wsr_profile_enable.argtypes = [vp, i]
             L.wsr_profile_read.argtypes = [vp, C.POINTER(d), C.POINTER(C.c_longlong)]
             L.wsr_euler2d_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
@@ -74,7 +82,8 @@ def exported_symbols() -> list[str]:
             "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run",
             "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops",
             "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
-            "wsr_train1d_backward", "wsr_euler2d_stage_noalloc"]
+            "wsr_train1d_backward", "wsr_euler3d_workspace_bytes", "wsr_euler3d_stage", "wsr_euler3d_max_speed",
+            "wsr_euler3d_run", "wsr_euler3d_counters", "wsr_euler2d_stage_noalloc"]
 
 
 def pack_params(params) -> np.ndarray:

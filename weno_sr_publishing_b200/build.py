@@ -13,7 +13,9 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libwsr.so"
-SOURCES = [CSRC / "wsr_api.cu"]
+SOURCES = [CSRC / "wsr_api.cu", CSRC / "euler3d.cu"]
+# euler3d.cu reproduces the reference's 3D Warp module, which is compiled without contraction
+EXTRA_FLAGS = {"euler3d.cu": ["-fmad=false"]}
 HEADERS = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "wsr.h"]
 
 NVCC_FLAGS = [
@@ -38,11 +40,24 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile each translation unit (in parallel) and link libwsr.so."""
     if force or stale():
-        cmd = [nvcc(), *NVCC_FLAGS, "-o", str(LIB), *map(str, SOURCES)]
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        subprocess.run(cmd, check=True)
+        compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+        objs, procs = [], []
+        for src in SOURCES:
+            obj = PKG / ("_" + src.stem + ".o")
+            cmd = [nvcc(), *compile_flags, *EXTRA_FLAGS.get(src.name, []), "-c", "-o", str(obj), str(src)]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            procs.append(subprocess.Popen(cmd))
+            objs.append(obj)
+        codes = [p.wait() for p in procs]
+        if any(codes):
+            raise subprocess.CalledProcessError(max(codes), "nvcc")
+        subprocess.run([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(LIB),
+                        *map(str, objs)], check=True)
+        for obj in objs:
+            obj.unlink(missing_ok=True)
     return LIB
 
 

@@ -237,6 +237,11 @@ __device__ __forceinline__ float div6(float x) { return x / 6.0f; }
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
+// Multiply-add with one rounding: what the compiler's contraction gives, written out so that a
+// translation unit built without contraction keeps it in the MLP.
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+
 template <typename T, bool BF16>
 __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5], const T xb[5], T ra[3], T rb[3]) {
   T ha[10], hb[10];
@@ -245,8 +250,8 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
     T za = P[kB1 + o], zb = P[kB1 + o];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
-      za = za + xa[k] * P[kW1 + k * 10 + o];
-      zb = zb + xb[k] * P[kW1 + k * 10 + o];
+      za = fma_t(xa[k], P[kW1 + k * 10 + o], za);
+      zb = fma_t(xb[k], P[kW1 + k * 10 + o], zb);
     }
     ha[o] = swish<T>(za);
     hb[o] = swish<T>(zb);
@@ -261,8 +266,8 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
     T za = P[kB2 + o], zb = P[kB2 + o];
 #pragma unroll
     for (int k = 0; k < 10; ++k) {
-      za = za + ha[k] * P[kW2 + k * 6 + o];
-      zb = zb + hb[k] * P[kW2 + k * 6 + o];
+      za = fma_t(ha[k], P[kW2 + k * 6 + o], za);
+      zb = fma_t(hb[k], P[kW2 + k * 6 + o], zb);
     }
     ga[o] = swish<T>(za);
     gb[o] = swish<T>(zb);
@@ -277,8 +282,8 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
     T za = P[kB3 + o], zb = P[kB3 + o];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      za = za + ga[k] * P[kW3 + k * 6 + o];
-      zb = zb + gb[k] * P[kW3 + k * 6 + o];
+      za = fma_t(ga[k], P[kW3 + k * 6 + o], za);
+      zb = fma_t(gb[k], P[kW3 + k * 6 + o], zb);
     }
     ka[o] = swish<T>(za);
     kb[o] = swish<T>(zb);
@@ -293,8 +298,8 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
     T za = P[kB4 + o], zb = P[kB4 + o];
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      za = za + ka[k] * P[kW4 + k * 3 + o];
-      zb = zb + kb[k] * P[kW4 + k * 3 + o];
+      za = fma_t(ka[k], P[kW4 + k * 3 + o], za);
+      zb = fma_t(kb[k], P[kW4 + k * 3 + o], zb);
     }
     ba[o] = T(6) * tanh_t(div6(za));
     bb[o] = T(6) * tanh_t(div6(zb));
@@ -403,6 +408,88 @@ __device__ __forceinline__ typename QIn<M>::T to_queue(double f) {
     return bf16r((float)f);
   else
     return (float)f;
+}
+
+
+// SR closure of one non-plateau stencil -> reciprocal scaled betas (features FP64 as in DEPLOY:96-120,
+// the MLP in the closure precision, ratios averaged and inverted in FP64 as in DEPLOY:234-247).
+template <int M>
+__device__ __forceinline__ void sr_betas(const double s[5], const typename ClosureParams<M>::type& P,
+                                         double& a0, double& a1, double& a2) {
+  const Sens se = sensors5(s);
+#if WSR_FEATURES_F32
+  if constexpr (M != M_SR64) {
+    // FP32 closure: the differences are FP64 (they cancel), the normalisation, gamma and the scale
+    // feature are formed in FP32 (the MLP consumes FP32 inputs; dmax >= 1e-13 here, so every value is
+    // a normal float).
+    const double d20 = s[0] - 2.0 * s[1] + s[2], d21 = s[1] - 2.0 * s[2] + s[3], d22 = s[2] - 2.0 * s[3] + s[4];
+    const float inv = __frcp_rn((float)se.dmax);
+    const float e = 1.0e-15f;
+    float x[5];
+    x[0] = (float)se.d0 * inv;
+    x[1] = (float)se.d1 * inv;
+    x[2] = (float)se.d2 * inv;
+    const float g0 = __fdividef(fabsf((float)d20), (float)(fabs(s[1] - s[0]) + fabs(s[2] - s[1])) + e);
+    const float g1 = __fdividef(fabsf((float)d21), (float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
+    const float g2 = __fdividef(fabsf((float)d22), (float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
+    x[3] = fminf(1.0f, fmaxf(fmaxf(g0, g1), g2));
+    const float rel = (float)se.dmax * __frcp_rn((float)se.qscale);
+    x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (__log10f(rel) + 4.0f) * 0.25f)));
+    if constexpr (M == M_SRBF16) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) x[k] = bf16r(x[k]);
+    }
+    closure_from_features<M>(x, P, a0, a1, a2);
+    return;
+  }
+#endif
+  double f[5];
+  const double inv = rcp64(fmax(se.dmax, 1.0e-15));
+  f[0] = se.d0 * inv;
+  f[1] = se.d1 * inv;
+  f[2] = se.d2 * inv;
+  f[3] = gamma_s(s);
+  // clip((log10(rel) + 4)/4, 0, 1): the logarithm is needed only when rel is strictly inside (1e-4, 1)
+  const double rel = fmax(se.dmax * rcp64(se.qscale), 1.0e-30);
+  f[4] = rel >= 1.0 ? 1.0 : (rel <= 1.0e-4 ? 0.0 : fmin(1.0, fmax(0.0, (log(rel) / 2.302585092994046 + 4.0) / 4.0)));
+  typename QIn<M>::T x[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) x[k] = to_queue<M>(f[k]);
+  closure_from_features<M>(x, P, a0, a1, a2);
+}
+
+template <int M>
+__device__ __forceinline__ double sr_value(const double s[5], int head, double a0, double a1, double a2, int opts,
+                                           Tally& tally) {
+  double w[3], c[3];
+  const Lin3 d = linear_weights(head);
+  if (!(isfinite(a0) && isfinite(a1) && isfinite(a2)) && (opts & OPT_JS_FALLBACK)) {
+    js_head_weights(js_stencil(s), d, w);
+    ++tally.fallbacks;
+  } else {
+    StencilW sw;
+    sw.a0 = a0;
+    sw.a1 = a1;
+    sw.a2 = a2;
+    sw.linear = false;
+    sr_head_weights(sw, d, (opts & OPT_ENO_CUTOFF) != 0, w);
+  }
+  candidates(s, head, c);
+  return combine(w, c);
+}
+
+__device__ __forceinline__ double linear_value(const double s[5], int head) {
+  const Lin3 d = linear_weights(head);
+  double c[3];
+  candidates(s, head, c);
+  return d.d0 * c[0] + d.d1 * c[1] + d.d2 * c[2];
+}
+
+__device__ __forceinline__ double js_value(const double s[5], int head) {
+  double w[3], c[3];
+  js_head_weights(js_stencil(s), linear_weights(head), w);
+  candidates(s, head, c);
+  return combine(w, c);
 }
 
 }  // namespace wsr

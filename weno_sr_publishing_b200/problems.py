@@ -8,6 +8,8 @@ drawn from a seeded generator: rho in [0.5, 2], u, v in [-1, 1], p in [0.1, 1.5]
 """
 from __future__ import annotations
 
+from dataclasses import dataclass
+
 import numpy as np
 
 GHOST = 3
@@ -97,3 +99,119 @@ def isentropic_vortex(nx: int, ny: int, t: float = 0.0, quadrature: int = 5, gam
             p = rho ** gamma
             state += 0.25 * float(wx) * float(wy) * conserved_from_primitive(rho, 1.0 + du, 1.0 + dv, p, gamma)
     return state
+
+
+# ------------------------------------------------------------------------------------------------
+# 3D shock-bubble interaction
+# ------------------------------------------------------------------------------------------------
+_GL3_NODES = (-0.77459666924148340427791481488384306430816650390625, 0.0,
+              0.77459666924148340427791481488384306430816650390625)
+_GL3_WEIGHTS = (0.55555555555555546920487586248782463371753692626953125,
+                0.88888888888888917261255073754000477492809295654296875,
+                0.55555555555555546920487586248782463371753692626953125)
+
+
+def _gauss27(value_fn, nx, ny, nz, x0, y0, z0, dx, dy, dz, ghost=3):
+    """0.125 sum_{a,b,c} w_a w_b w_c value(x_a, y_b, z_c) over every padded cell, in the reference's loop
+    order (warp_weno5_3d_rk3/kernels.py:747-773); value_fn returns the 5 conserved components."""
+    k, j, i = np.meshgrid(np.arange(nz + 2 * ghost), np.arange(ny + 2 * ghost), np.arange(nx + 2 * ghost),
+                          indexing="ij")
+    xc = x0 + ((i - ghost).astype(np.float64) + 0.5) * dx
+    yc = y0 + ((j - ghost).astype(np.float64) + 0.5) * dy
+    zc = z0 + ((k - ghost).astype(np.float64) + 0.5) * dz
+    total = np.zeros(xc.shape + (5,))
+    for a in range(3):
+        x = xc + 0.5 * dx * _GL3_NODES[a]
+        for b in range(3):
+            y = yc + 0.5 * dy * _GL3_NODES[b]
+            for c in range(3):
+                z = zc + 0.5 * dz * _GL3_NODES[c]
+                w = _GL3_WEIGHTS[a] * _GL3_WEIGHTS[b] * _GL3_WEIGHTS[c]
+                total = total + w * value_fn(x, y, z)
+    return 0.125 * total
+
+
+def _conserved5(rho, u, v, w, p, gamma=1.4):
+    return np.stack([rho, rho * u, rho * v, rho * w, 0.5 * rho * (u * u + v * v + w * w) + p / (gamma - 1.0)],
+                    axis=-1)
+
+
+def shockbubble_reference_state(nx: int = 224, ny: int = 88, nz: int = 88, x_end: float = 0.225,
+                                y_end: float = 0.089, z_end: float = 0.089) -> np.ndarray:
+    """The reference's Ma = 3 air/helium shock-bubble initial state (kernels.py:686-773, config.py):
+    post-shock air for x < 0.005 moving at 736.911, a helium sphere of radius 0.025 at (0.035, 0.0445,
+    0.0445) at the ambient pressure, 3 x 3 x 3 Gauss cell averages on every padded cell."""
+    gamma, mach, rho_air, p_air, rho_he = 1.4, 3.0, 1.29, 101325.0, 0.214
+    rho_post = (((gamma + 1.0) * mach * mach) / ((gamma - 1.0) * mach * mach + 2.0)) * rho_air
+    p_post = ((((2.0 * gamma) * mach * mach) - (gamma - 1.0)) / (gamma + 1.0)) * p_air
+
+    def value(x, y, z):
+        rho = np.full(x.shape, rho_air)
+        u = np.zeros(x.shape)
+        p = np.full(x.shape, p_air)
+        post = x < 0.005
+        rho = np.where(post, rho_post, rho)
+        u = np.where(post, 736.911, u)
+        p = np.where(post, p_post, p)
+        dxb, dyb, dzb = x - 0.035, y - 0.0445, z - 0.0445
+        inside = dxb * dxb + dyb * dyb + dzb * dzb <= 0.025 * 0.025
+        rho = np.where(inside, rho_he, rho)
+        u = np.where(inside, 0.0, u)
+        p = np.where(inside, p_air, p)
+        z0 = np.zeros(x.shape)
+        return _conserved5(rho, u, z0, z0, p, gamma)
+
+    return _gauss27(value, nx, ny, nz, 0.0, 0.0, 0.0, x_end / nx, y_end / ny, z_end / nz)
+
+
+@dataclass(frozen=True)
+class ShockBubble:
+    """A planar shock of Mach `mach` moving in +x into quiescent gas (rho 1, p 1) that holds a sphere of
+    radius 0.25 and density `density_ratio` at the same pressure, on [0, 2.545] x [0, 1] x [0, 1]."""
+    mach: float
+    density_ratio: float
+    nx: int = 224
+    ny: int = 88
+    nz: int = 88
+    length: tuple = (2.545, 1.0, 1.0)
+    shock_x: float = 0.2
+    centre: tuple = (0.6, 0.5, 0.5)
+    radius: float = 0.25
+    gamma: float = 1.4
+
+    @staticmethod
+    def seeded(seed: int, nx: int = 224, ny: int = 88, nz: int = 88) -> "ShockBubble":
+        rng = np.random.default_rng(seed)
+        return ShockBubble(float(rng.uniform(2.0, 3.0)), float(rng.uniform(0.1, 0.3)), nx, ny, nz)
+
+    @property
+    def spacing(self) -> tuple:
+        return (self.length[0] / self.nx, self.length[1] / self.ny, self.length[2] / self.nz)
+
+    def post_shock(self) -> tuple:
+        """Rankine-Hugoniot state behind the shock: (rho, u, p)."""
+        g, m = self.gamma, self.mach
+        rho2 = (g + 1.0) * m * m / ((g - 1.0) * m * m + 2.0)
+        p2 = (2.0 * g * m * m - (g - 1.0)) / (g + 1.0)
+        u2 = m * np.sqrt(g) * (1.0 - 1.0 / rho2)
+        return rho2, u2, p2
+
+    def inflow(self) -> np.ndarray:
+        rho, u, p = self.post_shock()
+        return _conserved5(np.array(rho), np.array(u), np.array(0.0), np.array(0.0), np.array(p), self.gamma)
+
+    def state(self) -> np.ndarray:
+        rho2, u2, p2 = self.post_shock()
+        cx, cy, cz = self.centre
+
+        def value(x, y, z):
+            post = x < self.shock_x
+            inside = (x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2 <= self.radius ** 2
+            rho = np.where(post, rho2, np.where(inside, self.density_ratio, 1.0))
+            u = np.where(post, u2, 0.0)
+            p = np.where(post, p2, 1.0)
+            z0 = np.zeros(x.shape)
+            return _conserved5(rho, u, z0, z0, p, self.gamma)
+
+        dx, dy, dz = self.spacing
+        return _gauss27(value, self.nx, self.ny, self.nz, 0.0, 0.0, 0.0, dx, dy, dz)
