@@ -20,6 +20,10 @@ Secondary workloads (--workload):
   train1d closure training: one step is one forward + adjoint over B = 1024 trajectories of N = 256 cells
           at one distance, the K timed steps walking the shuffled distance cycle; metric: trajectory
           cell-steps/s (B N steps per training step / time).
+  euler3d 3D shock-bubble interaction, 224x88x88 on [0,2.545]x[0,1]^2, planar shock of seeded Mach number in
+          [2,3] (seed 0) into gas at rest holding a sphere of radius 0.25 with seeded density ratio in [0.1,0.3],
+          post-shock inflow at x = 0, transmissive elsewhere; WENO5-SR (FP32 closure by default), HLLC,
+          SSPRK3, CFL 0.4. A step is one time step from the initial state; metric: cell-updates/s.
 """
 from __future__ import annotations
 
@@ -43,7 +47,7 @@ UNIT = "cell-updates/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="sr_f32", choices=["sr_f32", "sr_f64", "sr_bf16", "js"])
@@ -51,9 +55,9 @@ def parse():
     ap.add_argument("--t0", type=float, default=0.125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-extras", action="store_true", help="no JS arm, e2e, CPU baseline (profiling runs)")
-    ap.add_argument("--workload", default="euler2d", choices=["euler2d", "adv1d", "train1d"],
+    ap.add_argument("--workload", default="euler2d", choices=["euler2d", "adv1d", "train1d", "euler3d"],
                     help="euler2d: the headline 2D step; adv1d: 4096 ragged 1D trajectories; train1d: closure "
-                         "training steps (B=1024, N=256)")
+                         "training steps (B=1024, N=256); euler3d: the 224x88x88 shock-bubble step")
     ap.add_argument("--scheme", type=int, default=5, choices=[5, 7], help="adv1d: WENO5/SSPRK3 or WENO7/Shu RK4")
     return ap.parse_args()
 
@@ -116,7 +120,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -196,6 +200,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "euler3d":
+        bench_3d(args, world, rank, local)
+        return
     if args.workload != "euler2d":
         bench_1d(args, world, rank, local)
         return
@@ -617,6 +624,122 @@ def bench_1d(args, world, rank, local):
                        "api": "weno_sr_publishing_b200.train1d.trajectory_loss(...).backward() with host profiles"}
         if rank == 0 and world == 1:
             line["cpu_baseline"] = _train_cpu(args.cpu_seconds)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _oracle3d_sample(sb_seed, method, params, budget_s):
+    """The 3D C oracle (OpenMP, all host threads) on the same problem at a quarter of the resolution."""
+    from oracle import oracle as O
+    from weno_sr_publishing_b200 import problems as PR
+    sb = PR.ShockBubble.seeded(sb_seed, 56, 22, 22)
+    q0 = sb.state()
+    dx, dy, dz = sb.spacing
+    steps, t0, q = 0, time.perf_counter(), q0
+    while True:
+        q, _ = O.euler3d_run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, 1, method, "hllc", params, inflow=sb.inflow(),
+                             fast=True)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or steps >= 20:
+            break
+    cells = sb.nx * sb.ny * sb.nz
+    return {"value": cells * steps / el, "unit": UNIT, "cores": O.num_threads(True), "kind": "port",
+            "sample": f"{steps} step(s) of the same problem on 56x22x22 from t=0 (C oracle, OpenMP), {el:.1f} s"}
+
+
+def bench_3d(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from weno_sr_publishing_b200 import euler3d as E3
+    from weno_sr_publishing_b200 import problems as PR
+    from weno_sr_publishing_b200.checkpoint import MODELS_DIR
+    method = args.method
+    params = None
+    if method != "js":
+        name = "weno5_sr_fp64_step012250.npz" if method == "sr_f64" else "weno5_sr_fp32_step016500.npz"
+        params = {k: v for k, v in np.load(MODELS_DIR / name).items() if k != "meta_json"}
+    metric = f"3D Euler cell-updates/s, WENO5-SR ({method}) HLLC, 224x88x88 shock-bubble"
+    cfg = {"workload": "3D shock-bubble, 224x88x88 on [0,2.545]x[0,1]^2, seed 0 (Mach and density ratio), "
+                       "post-shock inflow, from t=0", "method": method, "flux": "hllc", "cfl": 0.4,
+           "time_integrator": "SSPRK3", "state_precision": "fp64",
+           "l2_policy": "state 81 MB, workspace 0.8 GB per step: larger than L2",
+           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    sb = PR.ShockBubble.seeded(0)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = _oracle3d_sample(0, method, params, args.cpu_seconds)
+        line = {"metric": metric, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "impl": "reference",
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    stream = torch.cuda.current_stream(dev)
+    q0 = torch.as_tensor(sb.state(), device=dev).contiguous()
+    dx, dy, dz = sb.spacing
+    ws = E3.workspace(sb.nx, sb.ny, sb.nz, dev)
+    K, W = args.steps, max(args.warmup, 0)
+    q = q0.clone()
+    if W:
+        E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=W, ws=ws)
+    q.copy_(q0)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        res = E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=K,
+                     ws=ws)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = sb.nx * sb.ny * sb.nz
+    finite = bool(torch.isfinite(q).all())
+    line = {"metric": metric, "value": world * cells * K / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": cfg, "clocks": clk.summary(),
+            "gpu_launches": 2 + K * (2 + 3 * 13), "t_reached": res.t, "state_finite": finite,
+            "shock": {"mach": sb.mach, "density_ratio": sb.density_ratio}}
+    # closure tallies over the same run
+    q.copy_(q0)
+    E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=K, ws=ws,
+           opts=4)
+    line["closure_tally_per_step"] = {k: {"mlp": v[0] / K, "plateau": v[1] / K} for k, v in E3.counters(ws).items()}
+    if not args.skip_extras:
+        # end to end: the padded state from pinned host memory, K steps, and back
+        host = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(q0.cpu())
+        torch.cuda.synchronize()
+        e0.record(stream)
+        q.copy_(host, non_blocking=True)
+        E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=K, ws=ws)
+        host.copy_(q, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1)
+        nbytes = int(q0.numel()) * 8
+        line["e2e"] = {"value": world * cells * K / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes / K,
+                       "d2h_bytes_per_step": nbytes / K,
+                       "api": "weno_sr_publishing_b200.euler3d.run on a tensor copied from / to pinned host memory"}
+        if rank == 0 and world == 1:
+            line["cpu_baseline"] = _oracle3d_sample(0, method, params, args.cpu_seconds)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
