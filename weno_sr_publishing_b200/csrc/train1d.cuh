@@ -27,8 +27,8 @@
 // MLP evaluation with the activations, the pair exchanges outputs and input adjoints with one shuffle each,
 // and the adjoint runs back through the weights, the reflection average, the MLP and the features to the
 // five stencil values. Each thread writes its activations and pre-activation adjoints as one row in shared
-// memory; after each chunk, thread p < 189 adds the outer-product term of parameter p over the rows into a
-// register that lives for the whole trajectory. k_train_reduce sums the per-trajectory partial losses and
+// memory; after each chunk, the threads add the outer-product terms of the rows into registers that live
+// for the whole trajectory (accumulate_rows). k_train_reduce sums the per-trajectory partial losses and
 // gradients in a fixed order, so the result is deterministic.
 //
 // Non-smooth points follow torch autograd's conventions, so that the gradient is the one autograd gives
@@ -541,43 +541,87 @@ __device__ __forceinline__ void pair_vjp(const double q[5], const double d[3], d
   feature_grad(q, d, dmax, qs, fb, qb);
 }
 
-// Row slot of parameter p in the packed w1 b1 w2 b2 w3 b3 w4 b4 layout: activation index (-1 for a bias)
-// and pre-activation adjoint index.
-__device__ __forceinline__ void param_slot(int p, int& ai, int& di) {
-  if (p < 50) {
-    ai = p / 10;
-    di = p % 10;
-  } else if (p < 60) {
-    ai = -1;
-    di = p - 50;
-  } else if (p < 120) {
-    ai = 5 + (p - 60) / 6;
-    di = 10 + (p - 60) % 6;
-  } else if (p < 126) {
-    ai = -1;
-    di = 10 + p - 120;
-  } else if (p < 162) {
-    ai = 15 + (p - 126) / 6;
-    di = 16 + (p - 126) % 6;
-  } else if (p < 168) {
-    ai = -1;
-    di = 16 + p - 162;
-  } else if (p < 186) {
-    ai = 21 + (p - 168) / 3;
-    di = 22 + (p - 168) % 3;
-  } else {
-    ai = -1;
-    di = 22 + p - 186;
+// Parameter reduction. The gradient of the weights and bias of layer l is the sum over samples of the
+// outer product (activation row) x (pre-activation adjoint row). The 189 parameters form 31 "rows": one
+// per input of a layer plus one for its bias (L1: 5 + 1 rows of 10 outputs, L2: 10 + 1 of 6, L3: 6 + 1
+// of 6, L4: 6 + 1 of 3). Thread t takes row t / kGroups for the samples s = t % kGroups (mod kGroups):
+// one activation load, then J loads and J FMAs per sample, partial sums of a chunk in the closure
+// precision and the running sums in FP64 registers for the whole trajectory.
+constexpr int kGroups = 8;
+constexpr int kRowTasks = 31;
+
+struct RowTask {
+  int ai;  // activation index in the row (-1: bias, activation 1)
+  int d0;  // first pre-activation adjoint index
+  int J;   // outputs
+  int p0;  // first packed parameter index
+};
+
+__device__ __forceinline__ RowTask row_task(int r) {
+  if (r < 5) return {r, 0, 10, r * 10};
+  if (r == 5) return {-1, 0, 10, 50};
+  if (r < 16) return {5 + (r - 6), 10, 6, 60 + (r - 6) * 6};
+  if (r == 16) return {-1, 10, 6, 120};
+  if (r < 23) return {15 + (r - 17), 16, 6, 126 + (r - 17) * 6};
+  if (r == 23) return {-1, 16, 6, 162};
+  if (r < 30) return {21 + (r - 24), 22, 3, 168 + (r - 24) * 3};
+  return {-1, 22, 3, 186};
+}
+
+// Running sums in shared memory, acc[j * kTrainThreads + thread] (keeps them out of the registers that the
+// closure adjoint needs).
+struct GradAcc {
+  double* v;
+};
+
+// Adds the rows of one chunk (ns samples) into this thread's running sums.
+template <typename Tr>
+__device__ __forceinline__ void accumulate_rows(const Tr* __restrict__ rows, int ns, GradAcc& acc) {
+  const int r = threadIdx.x / kGroups, g = threadIdx.x % kGroups;
+  if (r >= kRowTasks) return;
+  const RowTask t = row_task(r);
+  Tr part[10];
+#pragma unroll
+  for (int j = 0; j < 10; ++j) part[j] = Tr(0);
+  for (int s = g; s < ns; s += kGroups) {
+    const Tr* row = rows + (size_t)s * kRow;
+    const Tr a = t.ai < 0 ? Tr(1) : row[t.ai];
+    const Tr* d = row + kRowA + t.d0;
+#pragma unroll
+    for (int j = 0; j < 10; ++j)
+      if (j < t.J) part[j] = fma_t(a, d[j], part[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < 10; ++j)
+    if (j < t.J) acc.v[j * kTrainThreads + threadIdx.x] += (double)part[j];
+}
+
+// Sums the kGroups partial rows of every parameter in a fixed order into out[189].
+template <typename Tr>
+__device__ __forceinline__ void finish_rows(const GradAcc& acc, double* scratch, double* __restrict__ out) {
+  const int r = threadIdx.x / kGroups, g = threadIdx.x % kGroups;
+  __syncthreads();
+  if (r < kRowTasks) {
+    const RowTask t = row_task(r);
+#pragma unroll
+    for (int j = 0; j < 10; ++j)
+      if (j < t.J) scratch[g * kP5 + t.p0 + j] = acc.v[j * kTrainThreads + threadIdx.x];
+  }
+  __syncthreads();
+  if (threadIdx.x < kP5) {
+    double s = 0.0;
+    for (int q = 0; q < kGroups; ++q) s += scratch[q * kP5 + threadIdx.x];
+    out[threadIdx.x] = s;
   }
 }
 
 // out = J_rhs(w)^T v for the CTA's trajectory, with the parameter term v . d rhs / d theta added to acc
-// (thread p < 189 holds parameter p). G: 5 n doubles of scratch; rows: kTrainThreads rows of kRow.
+// (accumulate_rows). G: 5 n doubles of scratch; rows: kTrainThreads rows of kRow.
 template <int M>
 __device__ __forceinline__ void vjp_rhs(const double* __restrict__ w, const double* __restrict__ v,
                                         double* __restrict__ out, double* __restrict__ G, unsigned short* qu,
                                         const AdvTraj& T, typename TrainReal<M>::T* __restrict__ rows,
-                                        const typename ClosureParams<M>::type& P, double& acc, int pa, int pd) {
+                                        const typename ClosureParams<M>::type& P, GradAcc& acc) {
   using Tr = typename TrainReal<M>::T;
   const int n = T.n;
   const int lr = T.a > 0.0 ? 1 : 2;
@@ -650,16 +694,7 @@ __device__ __forceinline__ void vjp_rhs(const double* __restrict__ w, const doub
       for (int k = 0; k < 5; ++k) G[k * n + i] = qb[k];
     }
     __syncthreads();
-    const int ns = 2 * min(kTrainThreads / 2, count - base);
-    if (threadIdx.x < kP5) {
-      const Tr* dcol = rows + kRowA + pd;
-      if (pa < 0) {
-        for (int r = 0; r < ns; ++r) acc += (double)dcol[(size_t)r * kRow];
-      } else {
-        const Tr* acol = rows + pa;
-        for (int r = 0; r < ns; ++r) acc += (double)acol[(size_t)r * kRow] * (double)dcol[(size_t)r * kRow];
-      }
-    }
+    accumulate_rows<Tr>(rows, 2 * min(kTrainThreads / 2, count - base), acc);
     __syncthreads();
   }
   // gather: out_j = sum_k G[k][j + 2 - k]
@@ -679,13 +714,13 @@ __device__ __forceinline__ void vjp_rhs(const double* __restrict__ w, const doub
 template <int M>
 constexpr size_t train_bwd_smem(int n) {
   return (size_t)12 * n * sizeof(double) + ((size_t)2 * n + 15) / 16 * 16 +
-         (size_t)kTrainThreads * kRow * sizeof(typename TrainReal<M>::T);
+         (size_t)kTrainThreads * kRow * sizeof(typename TrainReal<M>::T) + (size_t)10 * kTrainThreads * sizeof(double);
 }
 
 constexpr size_t train_fwd_smem(int n) { return (size_t)3 * n * sizeof(double) + ((size_t)2 * n + 15) / 16 * 16; }
 
 template <int M>
-__global__ void __launch_bounds__(kTrainThreads, 1)
+__global__ void __launch_bounds__(kTrainThreads, M == M_SR32 ? 2 : 1)
     k_train_bwd(const double* __restrict__ ck, const unsigned* __restrict__ signs, const double* __restrict__ vel, int n,
                 double dx, double dt, int steps, int every, double gscale, double* __restrict__ seg,
                 double* __restrict__ grad_part, double* __restrict__ grad_u0,
@@ -708,9 +743,9 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
   T.n = n;
   T.a = vel[b];
   T.dx = dx;
-  int pa = -1, pd = 0;
-  if (threadIdx.x < kP5) param_slot(threadIdx.x, pa, pd);
-  double acc = 0.0;
+  GradAcc acc{reinterpret_cast<double*>(reinterpret_cast<char*>(rows) + (size_t)kTrainThreads * kRow * sizeof(Tr))};
+#pragma unroll
+  for (int j = 0; j < 10; ++j) acc.v[j * kTrainThreads + threadIdx.x] = 0.0;
   for (int i = threadIdx.x; i < n; i += kTrainThreads) Lam[i] = 0.0;
   const int K = (steps + every - 1) / every;
   const int words = (n + 31) >> 5;
@@ -738,7 +773,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
         V[i] = (2.0 / 3.0) * dt * lam;
       }
       __syncthreads();
-      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc, pa, pd);  // u3 = u/3 + 2/3 (u2 + dt L(u2))
+      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);  // u3 = u/3 + 2/3 (u2 + dt L(u2))
       for (int i = threadIdx.x; i < n; i += kTrainThreads) {
         const double l2 = (2.0 / 3.0) * Lam[i] + R[i];
         L2[i] = l2;
@@ -747,7 +782,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
         V[i] = 0.25 * dt * l2;
       }
       __syncthreads();
-      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc, pa, pd);  // u2 = 3/4 u + 1/4 (u1 + dt L(u1))
+      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);  // u2 = 3/4 u + 1/4 (u1 + dt L(u1))
       for (int i = threadIdx.x; i < n; i += kTrainThreads) {
         const double l1 = 0.25 * L2[i] + R[i];
         LU[i] += 0.75 * L2[i];
@@ -756,14 +791,14 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
         V[i] = dt * l1;
       }
       __syncthreads();
-      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc, pa, pd);  // u1 = u + dt L(u)
+      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);  // u1 = u + dt L(u)
       for (int i = threadIdx.x; i < n; i += kTrainThreads) Lam[i] = LU[i] + L2[i] + R[i];
       __syncthreads();
     }
   }
   if (grad_u0)
     for (int i = threadIdx.x; i < n; i += kTrainThreads) grad_u0[(size_t)b * n + i] = Lam[i];
-  if (threadIdx.x < kP5) grad_part[(size_t)b * kP5 + threadIdx.x] = acc;
+  finish_rows<Tr>(acc, reinterpret_cast<double*>(rows), grad_part + (size_t)b * kP5);
 }
 
 // Fixed-order sums over trajectories: grad_out[p] = sum_b grad_part[b][p]; loss_out = lscale * sum_b loss_part[b].
