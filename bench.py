@@ -349,11 +349,33 @@ def main():
         if rank == 0 and world == 1:
             line["cpu_baseline"] = cpu_sample(start.cpu().numpy(), args.method, {"n": n, "mlp": mlp},
                                               args.cpu_seconds)
+        if rank == 0:
+            line["matched_l1"] = matched_l1_block(args.method, mlp, dev)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def matched_l1_block(method, mlp, dev):
+    """The metric's "at matched L1 error", on a smooth and a discontinuous problem: the periodic isentropic
+    vortex (the reference's exp 05 setup, [-10,10]^2, t = 2, CFL 0.4) at N = 100..800 against the exact
+    solution, and the seeded quadrant problem at N = 100..400 against a 2000^2 WENO5-JS solution; for each
+    SR point the JS resolution with the same L1 (log-log interpolation) and both device times to it."""
+    from weno_sr_publishing_b200 import accuracy as AC
+    ns = (100, 200, 400, 800)
+    sr = [AC.vortex_run(n, method, mlp, dev) for n in ns]
+    js = [AC.vortex_run(n, "js", None, dev) for n in ns]
+    pts = lambda rs: [{"n": r.n, "l1": r.l1, "ms": r.device_ms, "steps": r.steps} for r in rs]  # noqa: E731
+    vortex = {"problem": "isentropic vortex [-10,10]^2 periodic, t=2, CFL 0.4, L1(rho) vs exact cell averages",
+              "sr": pts(sr), "js": pts(js), "matched": AC.matched_l1(sr[:-1], js)}
+    study, ref_ms = AC.quadrant_study(method, mlp, dev)
+    quadrant = {"problem": "seeded quadrant Riemann problem (seed 0), t=0.25, CFL 0.4, L1(rho) vs the 2000^2 "
+                           "WENO5-JS solution block-averaged", "reference_ms": ref_ms,
+                "sr": pts(study[method]), "js": pts(study["js"]),
+                "matched": AC.matched_l1(study[method], study["js"])}
+    return {"vortex": vortex, "quadrant": quadrant}
 
 
 DIST_CYCLE = (2, 8, 64, 128, 256, 512, 1024)

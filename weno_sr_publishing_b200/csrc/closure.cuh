@@ -36,6 +36,10 @@ struct Mlp5d {
 };
 struct Mlp5f {
   float p[kParams5];
+  float2 d[kParams5];  // each parameter twice: the packed (direct, reflected) operand of mlp_pair_x2
+  __host__ __device__ void duplicate() {
+    for (int k = 0; k < kParams5; ++k) d[k] = make_float2(p[k], p[k]);
+  }
 };
 struct NoParams {};
 
@@ -361,6 +365,76 @@ __device__ __forceinline__ double gamma_s(const double q[5]) {
 #define WSR_FEATURES_F32 1
 #endif
 
+// FP32 MLP of the direct and reflected inputs together with Blackwell's packed FP32 arithmetic
+// (fma/mul/add .f32x2: two independent single-precision operations per instruction, each rounded as its
+// scalar form). The two orientations share every weight, so each weight is read once as a duplicated pair
+// from the parameter block; the transcendental units stay scalar. Same values as mlp_pair<float, false>.
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(unsigned long long v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ unsigned long long wpair(const float2& w) {
+  return *reinterpret_cast<const unsigned long long*>(&w);
+}
+__device__ __forceinline__ unsigned long long swish2(unsigned long long z) {
+  float a, b;
+  upk2(z, a, b);
+  return pk2(swish<float>(a), swish<float>(b));
+}
+
+template <int NI, int NO>
+__device__ __forceinline__ void dense_x2(const float2* __restrict__ D, int w, int bias, const unsigned long long* x,
+                                         unsigned long long* y, bool act) {
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    unsigned long long z = wpair(D[bias + o]);
+#pragma unroll
+    for (int k = 0; k < NI; ++k) z = fma2(x[k], wpair(D[w + k * NO + o]), z);
+    y[o] = act ? swish2(z) : z;
+  }
+}
+
+__device__ __forceinline__ void mlp_pair_x2(const float2* __restrict__ D, const float xa[5], const float xb[5],
+                                            float ra[3], float rb[3]) {
+  unsigned long long x[5], h1[10], h2[6], h3[6], z4[3];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) x[k] = pk2(xa[k], xb[k]);
+  dense_x2<5, 10>(D, kW1, kB1, x, h1, true);
+  dense_x2<10, 6>(D, kW2, kB2, h1, h2, true);
+  dense_x2<6, 6>(D, kW3, kB3, h2, h3, true);
+  dense_x2<6, 3>(D, kW4, kB4, h3, z4, false);
+  float ba[3], bb[3];
+#pragma unroll
+  for (int o = 0; o < 3; ++o) {
+    float za, zb;
+    upk2(z4[o], za, zb);
+    ba[o] = 6.0f * tanh_t(div6(za));
+    bb[o] = 6.0f * tanh_t(div6(zb));
+  }
+  float ma = ba[0] > ba[1] ? ba[0] : ba[1];
+  ma = ma > ba[2] ? ma : ba[2];
+  float mb = bb[0] > bb[1] ? bb[0] : bb[1];
+  mb = mb > bb[2] ? mb : bb[2];
+  const float ea0 = exp_t(ba[0] - ma), ea1 = exp_t(ba[1] - ma), ea2 = exp_t(ba[2] - ma);
+  const float eb0 = exp_t(bb[0] - mb), eb1 = exp_t(bb[1] - mb), eb2 = exp_t(bb[2] - mb);
+  const float ia = rcp_t(ea0 + ea1 + ea2), ib = rcp_t(eb0 + eb1 + eb2);
+  ra[0] = ea0 * ia;
+  ra[1] = ea1 * ia;
+  ra[2] = ea2 * ia;
+  rb[0] = eb0 * ib;
+  rb[1] = eb1 * ib;
+  rb[2] = eb2 * ib;
+}
+
 // Queue element types: MLP inputs in the closure precision.
 template <int M>
 struct QIn {
@@ -389,7 +463,10 @@ __device__ __forceinline__ void closure_from_features(const typename QIn<M>::T* 
     float xa[5] = {x[0], x[1], x[2], x[3], x[4]};
     float xb[5] = {x[2], x[1], x[0], x[3], x[4]};
     float ra[3], rb[3];
-    mlp_pair<float, B>(reinterpret_cast<const float*>(&P), xa, xb, ra, rb);
+    if constexpr (B)
+      mlp_pair<float, true>(reinterpret_cast<const float*>(&P), xa, xb, ra, rb);
+    else
+      mlp_pair_x2(P.d, xa, xb, ra, rb);
     r0 = 0.5 * ((double)ra[0] + (double)rb[2]);
     r1 = 0.5 * ((double)ra[1] + (double)rb[1]);
     r2 = 0.5 * ((double)ra[2] + (double)rb[0]);

@@ -277,6 +277,8 @@ int wsr_closure_upload(wsr_ctx* ctx, int kind, const double* packed, int n) {
     ctx->p32.p[k] = static_cast<float>(packed[k]);
     ctx->pbf16.p[k] = __bfloat162float(__float2bfloat16_rn(static_cast<float>(packed[k])));
   }
+  ctx->p32.duplicate();
+  ctx->pbf16.duplicate();
   ctx->have_closure = true;
   return WSR_OK;
 }
@@ -827,12 +829,14 @@ extern "C" int wsr_euler2d_stage_noalloc(const double* u_stage, const double* u0
     case WSR_METHOD_SR_F32: {
       Mlp5f P;
       for (int k = 0; k < kParams5; ++k) P.p[k] = static_cast<float>(closure_params[k]);
+      P.duplicate();
       return noalloc_launch<M_SR32>(P, a, w, st);
     }
     default: {
       Mlp5f P;
       for (int k = 0; k < kParams5; ++k)
         P.p[k] = __bfloat162float(__float2bfloat16_rn(static_cast<float>(closure_params[k])));
+      P.duplicate();
       return noalloc_launch<M_SRBF16>(P, a, w, st);
     }
   }
