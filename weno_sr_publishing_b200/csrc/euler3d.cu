@@ -426,40 +426,30 @@ __global__ void __launch_bounds__(kT3) k3_normal(const double* __restrict__ q, d
   const int3 e = step_of<DIR>();
   Tally tally;
   V5 ch[5];
-  V5 left, right;
-  {
-    V5 s[5];
 #pragma unroll
-    for (int p = 0; p < 5; ++p) s[p] = ld5(q, d.cell(k + p * e.z, j + p * e.y, i + p * e.x));
-    const Eig<DIR> E(roe(s[1], s[2]));
-#pragma unroll
-    for (int p = 0; p < 5; ++p) ch[p] = E.left(s[p]);
-    V5 cv;
+  for (int p = 0; p < 5; ++p) ch[p] = ld5(q, d.cell(k + p * e.z, j + p * e.y, i + p * e.x));
+  Eig<DIR> E(roe(ch[1], ch[2]));
+  const size_t o = d.cell(k, j, i);
+  // side 0: the lr = 2 value (low face); side 1: the lr = 1 value (high face) of the stencil round-tripped
+  // through side 0's eigenvectors. One loop, so the closure is inlined once.
 #pragma unroll 1
-    for (int c = 0; c < 5; ++c) {
-      const double st[5] = {ch[0].v[c], ch[1].v[c], ch[2].v[c], ch[3].v[c], ch[4].v[c]};
-      cv.v[c] = recon<M>(st, 1, P, opts, tally);
-    }
-    left = E.right(cv);
-    // the lr = 1 side works on the stencil round-tripped through these eigenvectors
+  for (int side = 0; side < 2; ++side) {
+    if (side == 1) {
 #pragma unroll
-    for (int p = 0; p < 5; ++p) ch[p] = E.right(ch[p]);
-  }
-  {
-    const Eig<DIR> E(roe(ch[2], ch[3]));
+      for (int p = 0; p < 5; ++p) ch[p] = E.right(ch[p]);
+      E = Eig<DIR>(roe(ch[2], ch[3]));
+    }
 #pragma unroll
     for (int p = 0; p < 5; ++p) ch[p] = E.left(ch[p]);
     V5 cv;
 #pragma unroll 1
     for (int c = 0; c < 5; ++c) {
       const double st[5] = {ch[0].v[c], ch[1].v[c], ch[2].v[c], ch[3].v[c], ch[4].v[c]};
-      cv.v[c] = recon<M>(st, 0, P, opts, tally);
+      cv.v[c] = recon<M>(st, side == 0 ? 1 : 0, P, opts, tally);
     }
-    right = E.right(cv);
+    st5(side == 0 ? nl : nr, o, E.right(cv));
   }
-  const size_t o = d.cell(k, j, i);
-  st5(nl, o, left);
-  st5(nr, o, right);
+
   if (counters && (opts & OPT_COUNT)) {
     if (tally.mlp) atomicAdd(&counters[0], (unsigned long long)tally.mlp);
     if (tally.plateau) atomicAdd(&counters[1], (unsigned long long)tally.plateau);
@@ -479,20 +469,16 @@ __global__ void __launch_bounds__(kT3) k3_trans(const double* __restrict__ nl, c
   const int3 e = step_of<TA>();
   Tally tally;
   const size_t o = d.cell(k, j, i);
+  // items (side, Gauss point, component) in one loop, so the closure is inlined once
 #pragma unroll 1
-  for (int side = 0; side < 2; ++side) {
+  for (int item = 0; item < 20; ++item) {
+    const int side = item / 10, gp = (item / 5) & 1, c = item % 5;
     const double* src = side == 0 ? nl : nr;
-    V5 g1, g2;
-#pragma unroll 1
-    for (int c = 0; c < 5; ++c) {
-      double st[5];
+    double st[5];
 #pragma unroll
-      for (int p = 0; p < 5; ++p) st[p] = src[d.cell(k + (p + 1) * e.z, j + (p + 1) * e.y, i + (p + 1) * e.x) * 5 + c];
-      g1.v[c] = recon<M>(st, 2, P, opts, tally);
-      g2.v[c] = recon<M>(st, 3, P, opts, tally);
-    }
-    st5(side == 0 ? a_l1 : a_r1, o, g1);
-    st5(side == 0 ? a_l2 : a_r2, o, g2);
+    for (int p = 0; p < 5; ++p) st[p] = src[d.cell(k + (p + 1) * e.z, j + (p + 1) * e.y, i + (p + 1) * e.x) * 5 + c];
+    double* dst = side == 0 ? (gp == 0 ? a_l1 : a_l2) : (gp == 0 ? a_r1 : a_r2);
+    dst[o * 5 + c] = recon<M>(st, 2 + gp, P, opts, tally);
   }
   if (counters && (opts & OPT_COUNT)) {
     if (tally.mlp) atomicAdd(&counters[2], (unsigned long long)tally.mlp);
@@ -520,17 +506,21 @@ __global__ void __launch_bounds__(kT3) k3_flux(const double* __restrict__ a_l1, 
     const double* srcl = first == 1 ? a_l1 : a_l2;
     const double* srcr = first == 1 ? a_r1 : a_r2;
     V5 pl, pr;
+    // items (side, component) in one loop, so the closure is inlined once
 #pragma unroll 1
-    for (int c = 0; c < 5; ++c) {
-      double sl[5], sr[5];
+    for (int item = 0; item < 10; ++item) {
+      const int side = item / 5, c = item % 5;
+      double st[5];
 #pragma unroll
       for (int p = 0; p < 5; ++p) {
         const int kk = k + (p + 1) * eb.z, jj = j + (p + 1) * eb.y, ii = i + (p + 1) * eb.x;
-        sl[p] = srcl[d.cell(kk + e.z, jj + e.y, ii + e.x) * 5 + c];
-        sr[p] = srcr[d.cell(kk, jj, ii) * 5 + c];
+        st[p] = side == 0 ? srcl[d.cell(kk + e.z, jj + e.y, ii + e.x) * 5 + c] : srcr[d.cell(kk, jj, ii) * 5 + c];
       }
-      pl.v[c] = recon<M>(sl, second == 1 ? 2 : 3, P, opts, tally);
-      pr.v[c] = recon<M>(sr, second == 1 ? 2 : 3, P, opts, tally);
+      const double v = recon<M>(st, second == 1 ? 2 : 3, P, opts, tally);
+      if (side == 0)
+        pl.v[c] = v;
+      else
+        pr.v[c] = v;
     }
     V5 f;
     if constexpr (FLUX == 1)

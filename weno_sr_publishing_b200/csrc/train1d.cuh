@@ -764,34 +764,33 @@ __global__ void __launch_bounds__(kTrainThreads, M == M_SR32 ? 2 : 1)
     for (int k = k1 - 1; k >= k0; --k) {
       const double* st = sg + (size_t)(k - k0) * 3 * n;
       const unsigned* sw = signs + ((size_t)b * steps + k) * words * 2;
-      for (int i = threadIdx.x; i < n; i += kTrainThreads) {
-        const unsigned pos = sw[(i >> 5) * 2], neg = sw[(i >> 5) * 2 + 1], bit = 1u << (i & 31);
-        const double code = (pos & bit) ? 1.0 : ((neg & bit) ? -1.0 : 0.0);
-        const double lam = Lam[i] + gscale * code;
-        Lam[i] = lam;
-        S[i] = st[2 * n + i];
-        V[i] = (2.0 / 3.0) * dt * lam;
+      // The three stages in reverse, each with one VJP (a single call site keeps the kernel's code small):
+      //   r = 2: u3 = u/3 + 2/3 (u2 + dt L(u2));  r = 1: u2 = 3/4 u + 1/4 (u1 + dt L(u1));  r = 0: u1 = u + dt L(u)
+#pragma unroll 1
+      for (int r = 2; r >= 0; --r) {
+        for (int i = threadIdx.x; i < n; i += kTrainThreads) {
+          if (r == 2) {
+            const unsigned pos = sw[(i >> 5) * 2], neg = sw[(i >> 5) * 2 + 1], bit = 1u << (i & 31);
+            const double code = (pos & bit) ? 1.0 : ((neg & bit) ? -1.0 : 0.0);
+            const double lam = Lam[i] + gscale * code;
+            Lam[i] = lam;
+            V[i] = (2.0 / 3.0) * dt * lam;
+          } else if (r == 1) {
+            const double l2 = (2.0 / 3.0) * Lam[i] + R[i];
+            L2[i] = l2;
+            LU[i] = Lam[i] / 3.0;
+            V[i] = 0.25 * dt * l2;
+          } else {
+            const double l1 = 0.25 * L2[i] + R[i];
+            LU[i] += 0.75 * L2[i];
+            L2[i] = l1;
+            V[i] = dt * l1;
+          }
+          S[i] = st[r * n + i];
+        }
+        __syncthreads();
+        vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);
       }
-      __syncthreads();
-      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);  // u3 = u/3 + 2/3 (u2 + dt L(u2))
-      for (int i = threadIdx.x; i < n; i += kTrainThreads) {
-        const double l2 = (2.0 / 3.0) * Lam[i] + R[i];
-        L2[i] = l2;
-        LU[i] = Lam[i] / 3.0;
-        S[i] = st[n + i];
-        V[i] = 0.25 * dt * l2;
-      }
-      __syncthreads();
-      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);  // u2 = 3/4 u + 1/4 (u1 + dt L(u1))
-      for (int i = threadIdx.x; i < n; i += kTrainThreads) {
-        const double l1 = 0.25 * L2[i] + R[i];
-        LU[i] += 0.75 * L2[i];
-        L2[i] = l1;
-        S[i] = st[i];
-        V[i] = dt * l1;
-      }
-      __syncthreads();
-      vjp_rhs<M>(S, V, R, G, qu, T, rows, P, acc);  // u1 = u + dt L(u)
       for (int i = threadIdx.x; i < n; i += kTrainThreads) Lam[i] = LU[i] + L2[i] + R[i];
       __syncthreads();
     }
