@@ -479,6 +479,8 @@ def bench_1d(args, world, rank, local):
                "method": method, "loss": "mean L1 to exact cell averages at every completed step",
                "l2_policy": "inputs larger than L2 for the long distances (checkpoints + stage scratch)"}
     cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    if args.workload == "train1d" and world > 1:
+        cfg["parallelism"] = f"data parallel x{world}: each rank its own 1024 trajectories, gradient all-reduce"
     if args.impl == "reference":
         if rank != 0:
             return
@@ -619,7 +621,9 @@ def bench_1d(args, world, rank, local):
                 e0.record(stream)
                 r.forward()
                 e1.record(stream)
-                r.backward()
+                g, _ = r.backward()
+                if world > 1:
+                    dist.all_reduce(g)  # data parallelism: the 189 gradient values summed over ranks
                 e2.record(stream)
                 torch.cuda.synchronize()
                 fwd_ms += e0.elapsed_time(e1)

@@ -304,6 +304,43 @@ class TrainConfig:
                 "seed": self.seed, "loss": "mean_l1_exact_cell_averages_every_step", "velocities": (1.0, -1.0)}
 
 
+def _world():
+    """(world size, rank) of the default process group, or (1, 0) without one."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_world_size(), dist.get_rank()
+    return 1, 0
+
+
+def allreduce_gradients(model: torch.nn.Module) -> None:
+    """Data parallelism over trajectories: average the parameter gradients over the process group (one
+    all-reduce of the 189 packed values; each rank's loss is the mean over its own trajectories, so the
+    average is the gradient of the global mean)."""
+    world, _ = _world()
+    if world == 1:
+        return
+    import torch.distributed as dist
+    params = [p for p in model.parameters() if p.grad is not None]
+    flat = torch.cat([p.grad.reshape(-1).to(torch.float64) for p in params])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM)
+    flat /= world
+    o = 0
+    for p in params:
+        k = p.grad.numel()
+        p.grad.copy_(flat[o:o + k].reshape(p.grad.shape).to(p.grad.dtype))
+        o += k
+
+
+def _allreduce_mean(value: float, device) -> float:
+    world, _ = _world()
+    if world == 1:
+        return value
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item()) / world
+
+
 def _save_model(path: Path, model: ClosureMLP, step: int, cfg: TrainConfig) -> None:
     meta = {"raw_step": step, "recipe": "l1_exact_cell_averages_every_step", "precision": cfg.precision,
             "primary_cfl": cfg.cfl, "propagation_distances_cells": list(cfg.distances),
@@ -317,15 +354,24 @@ def train(cfg: TrainConfig, resume: Path | None = None, max_steps: int | None = 
     """Train a WENO5 closure from the reference's initialisation; returns a summary dict.
 
     Writes checkpoints/model_step_XXXXXX.npz every checkpoint_interval steps, state/latest.pt every
-    state_interval steps (and at the end), and history.csv."""
+    state_interval steps (and at the end), and history.csv.
+
+    Under torch.distributed (one process per GPU) the batch of each step is split over the ranks: every rank
+    draws its own cfg.batch / world trajectories from its own seeded stream, and the gradients are averaged
+    with one all-reduce before the identical optimiser steps; rank 0 writes the files."""
+    world, rank = _world()
+    if cfg.batch % (2 * world):
+        raise ValueError(f"batch {cfg.batch} must split into an even number of trajectories per rank ({world} ranks)")
+    local_batch = cfg.batch // world
     out = Path(cfg.out_dir)
-    out.mkdir(parents=True, exist_ok=True)
+    if rank == 0:
+        out.mkdir(parents=True, exist_ok=True)
     dtype = torch.float32 if cfg.precision == "f32" else torch.float64
     dev = torch.device(cfg.device)
     model = ClosureMLP(seed=cfg.seed, dtype=dtype).to(dev)
     opt = torch.optim.Adam(model.parameters(), lr=cfg.lr)
     sched = make_scheduler(opt, cfg.lr, cfg.lr_final, cfg.steps)
-    rng = np.random.default_rng(cfg.seed)
+    rng = np.random.default_rng(cfg.seed if world == 1 else [cfg.seed, rank])
     start, skipped = 1, 0
     if resume is not None:
         state = torch.load(resume, map_location=dev, weights_only=False)
@@ -334,35 +380,42 @@ def train(cfg: TrainConfig, resume: Path | None = None, max_steps: int | None = 
         model.load_state_dict(state["model_state_dict"])
         opt.load_state_dict(state["optimizer_state_dict"])
         sched.load_state_dict(state["scheduler_state_dict"])
-        rng.bit_generator.state = state["profile_rng_state"]
+        rng.bit_generator.state = state["profile_rng_state"] if world == 1 else state["profile_rng_states"][rank]
         start, skipped = int(state["step"]) + 1, int(state.get("skipped", 0))
-    else:
+    elif rank == 0:
         _save_model(out / "checkpoints" / "model_step_000000.npz", model, 0, cfg)
     hist = out / "history.csv"
     fields = ["step", "loss", "distance_cells", "horizon", "batch", "lr", "grad", "skipped"]
-    if start == 1 or not hist.exists():
+    if rank == 0 and (start == 1 or not hist.exists()):
         with hist.open("w", newline="") as f:
             csv.DictWriter(f, fieldnames=fields).writeheader()
     end = cfg.steps if max_steps is None else min(cfg.steps, start - 1 + max_steps)
     last = {}
 
     def save_state(step):
-        _atomic_torch_save({"step": step, "skipped": skipped, "model_state_dict": model.state_dict(),
-                            "optimizer_state_dict": opt.state_dict(), "scheduler_state_dict": sched.state_dict(),
-                            "profile_rng_state": rng.bit_generator.state, "training_signature": cfg.signature()},
-                           out / "state" / "latest.pt")
+        rng_states = [rng.bit_generator.state]
+        if world > 1:
+            import torch.distributed as dist
+            rng_states = [None] * world
+            dist.all_gather_object(rng_states, rng.bit_generator.state)
+        if rank == 0:
+            _atomic_torch_save({"step": step, "skipped": skipped, "model_state_dict": model.state_dict(),
+                                "optimizer_state_dict": opt.state_dict(), "scheduler_state_dict": sched.state_dict(),
+                                "profile_rng_state": rng_states[0], "profile_rng_states": rng_states,
+                                "training_signature": cfg.signature()}, out / "state" / "latest.pt")
 
     for step in range(start, end + 1):
         dist = float(cfg.distances[distance_index_for_step(step, len(cfg.distances), cfg.seed)])
-        batch = TrajectoryBatch.sample(rng, cfg.batch, cfg.grid, dist, cfg.cfl, dev, cfg.ckpt_every)
+        batch = TrajectoryBatch.sample(rng, local_batch, cfg.grid, dist, cfg.cfl, dev, cfg.ckpt_every)
         loss = trajectory_loss(model, batch)
         opt.zero_grad(set_to_none=True)
-        lval = float(loss.detach())
+        lval = _allreduce_mean(float(loss.detach()), dev)
         if not math.isfinite(lval):
             skipped += 1
             sched.step()
             continue
         loss.backward()
+        allreduce_gradients(model)
         grad = float(torch.nn.utils.clip_grad_norm_(model.parameters(), cfg.grad_clip))
         if not math.isfinite(grad) or grad > cfg.grad_skip:
             skipped += 1
@@ -370,16 +423,17 @@ def train(cfg: TrainConfig, resume: Path | None = None, max_steps: int | None = 
         else:
             opt.step()
         sched.step()
-        last = {"step": step, "loss": lval, "distance_cells": dist, "horizon": batch.steps, "batch": batch.B,
+        last = {"step": step, "loss": lval, "distance_cells": dist, "horizon": batch.steps, "batch": batch.B * world,
                 "lr": sched.get_last_lr()[0], "grad": grad, "skipped": skipped}
-        if step == 1 or step % cfg.log_interval == 0:
+        if rank == 0 and (step == 1 or step % cfg.log_interval == 0):
             with hist.open("a", newline="") as f:
                 csv.DictWriter(f, fieldnames=fields).writerow(last)
-        if step % cfg.checkpoint_interval == 0:
+        if rank == 0 and step % cfg.checkpoint_interval == 0:
             _save_model(out / "checkpoints" / f"model_step_{step:06d}.npz", model, step, cfg)
         if step % cfg.state_interval == 0:
             save_state(step)
     save_state(end)
-    _save_model(out / "checkpoints" / f"model_step_{end:06d}.npz", model, end, cfg)
-    (out / "summary.json").write_text(json.dumps({**last, "completed": end}, indent=1))
+    if rank == 0:
+        _save_model(out / "checkpoints" / f"model_step_{end:06d}.npz", model, end, cfg)
+        (out / "summary.json").write_text(json.dumps({**last, "completed": end}, indent=1))
     return {"model": model, "last": last, "skipped": skipped, "completed": end}
