@@ -41,6 +41,7 @@ extern "C" {
 #define WSR_METHOD_SR_F64 1   /* WENO5-SR, FP64 MLP (REFSYM) */
 #define WSR_METHOD_SR_F32 2   /* WENO5-SR, FP32 MLP, FP64 elsewhere (MIXED) */
 #define WSR_METHOD_SR_BF16 3  /* WENO5-SR, BF16 inputs/parameters/activations, FP32 accumulation */
+#define WSR_METHOD_Z 4        /* WENO5-Z (Borges p = 2, eps = h^2 per direction); 2D functions only */
 
 /* boundaries */
 #define WSR_BC_TRANSMISSIVE 0

@@ -35,7 +35,7 @@
 
 #define GC 3
 
-enum { OR_METHOD_JS = 0, OR_METHOD_SR64 = 1, OR_METHOD_SR32 = 2, OR_METHOD_SRBF16 = 3 };
+enum { OR_METHOD_JS = 0, OR_METHOD_SR64 = 1, OR_METHOD_SR32 = 2, OR_METHOD_SRBF16 = 3, OR_METHOD_Z = 4 };
 enum { OR_BC_TRANSMISSIVE = 0, OR_BC_PERIODIC = 1 };
 enum { OR_FLUX_HLLC = 0, OR_FLUX_FORCE = 1 };
 
@@ -248,6 +248,24 @@ static void js_weights(const double q[5], int head, double w[3]) {
     w[0] = a0 / s; w[1] = a1 / s; w[2] = a2 / s;
 }
 
+/* WENO-Z, Borges et al. p = 2, eps = h^2 of the reconstruction direction
+ * (weno_z_borges_p2_results/weno5_helpers_z.py:545-574, 853-879). */
+static void z_weights(const double q[5], int head, double eps, double w[3]) {
+    double d[3];
+    optimal_weights(head, d);
+    double t2 = q[2] - 2.0 * q[3] + q[4], u2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
+    double t1 = q[1] - 2.0 * q[2] + q[3], u1 = q[1] - q[3];
+    double t0 = q[0] - 2.0 * q[1] + q[2], u0 = q[0] - 4.0 * q[1] + 3.0 * q[2];
+    double b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * u2 * u2;
+    double b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * u1 * u1;
+    double b0 = (13.0 / 12.0) * t0 * t0 + 0.25 * u0 * u0;
+    double tau = fabs(b0 - b2);
+    double r0 = tau / (b0 + eps), r1 = tau / (b1 + eps), r2 = tau / (b2 + eps);
+    double a0 = d[0] * (1.0 + r0 * r0), a1 = d[1] * (1.0 + r1 * r1), a2 = d[2] * (1.0 + r2 * r2);
+    double s = a0 + a1 + a2;
+    w[0] = a0 / s; w[1] = a1 / s; w[2] = a2 / s;
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* Closure: features (DEPLOY:76-120), plateau (DEPLOY:123-131), MLP (DEPLOY:154-205;            */
 /* F32CORE:152-203), reflection-averaged weights (DEPLOY:208-279; F32CORE:206-283)             */
@@ -440,6 +458,15 @@ double or_reconstruct(const double q[5], int head, int method, const double *P64
     return w[0] * s[0] + w[1] * s[1] + w[2] * s[2];
 }
 
+/* The reconstruction with the grid spacing h of its direction (used by WENO-Z only). */
+double or_reconstruct_h(const double q[5], int head, int method, const double *P64, const float *P32, double h) {
+    if (method != OR_METHOD_Z) return or_reconstruct(q, head, method, P64, P32);
+    double w[3], s[3];
+    z_weights(q, head, h * h, w);
+    head_candidates(q, head, s);
+    return w[0] * s[0] + w[1] * s[1] + w[2] * s[2];
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* Stage (REFSYM:298-435 / MIXED:121-168 / HLLC5:294-358)                                      */
 /* ------------------------------------------------------------------------------------------ */
@@ -490,7 +517,7 @@ static void normal_recon(const vec4 q[5], int dir, const or_cfg *c, vec4 *face_l
         vec4 cf;
         for (int f = 0; f < 4; ++f) {
             double s[5] = {ch[0].v[f], ch[1].v[f], ch[2].v[f], ch[3].v[f], ch[4].v[f]};
-            cf.v[f] = or_reconstruct(s, head, c->method, c->P64, c->P32);
+            cf.v[f] = or_reconstruct_h(s, head, c->method, c->P64, c->P32, dir == 1 ? c->dx : c->dy);
         }
         vec4 out = char_to_con(cf, roe, dir, c->gamma);
         if (side == 0) *face_l = out; else *face_r = out;
@@ -545,8 +572,8 @@ static void stage(const double *u_stage, const double *u0, double *u_out, double
                         sr[k] = b->xl[((size_t)(j + 1 + k) * nxt + (i + 1)) * 4 + comp];
                         sl[k] = b->xr[((size_t)(j + 1 + k) * nxt + i) * 4 + comp];
                     }
-                    ur.v[comp] = or_reconstruct(sr, head, c->method, c->P64, c->P32);
-                    ul.v[comp] = or_reconstruct(sl, head, c->method, c->P64, c->P32);
+                    ur.v[comp] = or_reconstruct_h(sr, head, c->method, c->P64, c->P32, c->dy);
+                    ul.v[comp] = or_reconstruct_h(sl, head, c->method, c->P64, c->P32, c->dy);
                 }
                 vec4 f = riemann(ul, ur, 1, dt_dx, c);
                 for (int k = 0; k < 4; ++k) f.v[k] *= dt_dx;
@@ -567,8 +594,8 @@ static void stage(const double *u_stage, const double *u0, double *u_out, double
                         sr[k] = b->yl[((size_t)(j + 1) * nxt + (i + 1 + k)) * 4 + comp];
                         sl[k] = b->yr[((size_t)j * nxt + (i + 1 + k)) * 4 + comp];
                     }
-                    ur.v[comp] = or_reconstruct(sr, head, c->method, c->P64, c->P32);
-                    ul.v[comp] = or_reconstruct(sl, head, c->method, c->P64, c->P32);
+                    ur.v[comp] = or_reconstruct_h(sr, head, c->method, c->P64, c->P32, c->dx);
+                    ul.v[comp] = or_reconstruct_h(sl, head, c->method, c->P64, c->P32, c->dx);
                 }
                 vec4 f = riemann(ul, ur, 2, dt_dy, c);
                 for (int k = 0; k < 4; ++k) f.v[k] *= dt_dy;
@@ -727,6 +754,11 @@ void or_force_flux_flat(const double *ul, const double *ur, int dir, double c, d
 void or_closure_weights_batch(const double *q, int n, int head, int method, const double *P64, const float *P32,
                               double *w) {
     for (int k = 0; k < n; ++k) or_closure_weights(q + 5 * k, head, method, P64, P32, w + 3 * k);
+}
+
+void or_reconstruct_h_batch(const double *q, int n, int head, int method, const double *P64, const float *P32,
+                            double h, double *out) {
+    for (int k = 0; k < n; ++k) out[k] = or_reconstruct_h(q + 5 * k, head, method, P64, P32, h);
 }
 
 void or_reconstruct_batch(const double *q, int n, int head, int method, const double *P64, const float *P32,

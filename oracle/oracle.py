@@ -12,7 +12,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 
-METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3}
+METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3, "z": 4}
 BC = {"transmissive": 0, "periodic": 1}
 FLUX = {"hllc": 0, "force": 1}
 N_PARAMS5 = 189
@@ -45,6 +45,7 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_force_flux_flat.argtypes = [_dp, _dp, C.c_int, C.c_double, C.c_double, _dp]
         lib.or_closure_weights_batch.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _fp, _dp]
         lib.or_reconstruct_batch.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _fp, _dp]
+        lib.or_reconstruct_h_batch.argtypes = [_dp, C.c_int, C.c_int, C.c_int, _dp, _fp, C.c_double, _dp]
         lib.or_mlp_ratios_batch.argtypes = [_dp, C.c_int, C.c_int, _dp, _fp, _dp]
         lib.or_num_threads.restype = C.c_int
         _vp = C.c_void_p
@@ -85,6 +86,15 @@ def reconstruct(q: np.ndarray, head: int, method: str, params=None) -> np.ndarra
     out = np.zeros(q.shape[0])
     p64, p32 = _params(params)
     _lib().or_reconstruct_batch(q, q.shape[0], head, METHOD[method], p64, p32, out)
+    return out
+
+
+def reconstruct_h(q: np.ndarray, head: int, method: str, h: float, params=None) -> np.ndarray:
+    """reconstruct() with the grid spacing of the stencil's direction (WENO-Z's eps = h^2)."""
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 5)
+    out = np.zeros(q.shape[0])
+    p64, p32 = _params(params)
+    _lib().or_reconstruct_h_batch(q, q.shape[0], head, METHOD[method], p64, p32, float(h), out)
     return out
 
 

@@ -14,7 +14,9 @@ What it does:
 * runs ``scripts/verify_release.py::verify_reflection`` (which asserts the reference's own pinned
   MLP outputs) and stores the same fixed-feature outputs.
 
-Outputs: tests/golden/closure2d.npz, hllc2d.npz, euler2d_<case>.npz, mlp_golden.npz.
+* runs the WENO5-Z helpers and minimal solver (weno_z_borges_p2_results) the same way (``--only z``).
+
+Outputs: tests/golden/closure2d.npz, hllc2d.npz, euler2d_<case>.npz, mlp_golden.npz, euler2d_z.npz.
 """
 from __future__ import annotations
 
@@ -204,6 +206,38 @@ def gen_euler2d(wh, adapters, out_dir: Path) -> None:
         np.savez_compressed(out_dir / f"euler2d_{name}.npz", **rec)
 
 
+Z_CASES = [
+    ("rough_trans", 11, 9, "transmissive", "random", 0.1),
+    ("smooth_periodic", 12, 10, "periodic", "smooth", 0.05),
+]
+
+
+def gen_z(zh, zmin, out_dir: Path) -> None:
+    """WENO5-Z (weno_z_borges_p2_results): reconstructions at two spacings, and the minimal solver's
+    run_to_time / first stage on non-square grids (dx != dy, so the per-direction eps is exercised)."""
+    rng = np.random.default_rng(20260803)
+    q = make_stencils(rng, 96)
+    rec = {"q": q, "h": np.array([0.05, 1.0e-3])}
+    for hi, h in enumerate((0.05, 1.0e-3)):
+        for lr in (1, 2):
+            rec[f"v_lr{lr}_h{hi}"] = np.array([zh.weno5_lr_value(*map(float, s), lr, h) for s in q])
+            rec[f"v_g{lr}_h{hi}"] = np.array([zh.weno5_gauss_lr_value(*map(float, s), lr, h) for s in q])
+    for name, nx, ny, bc, kind, t_end in Z_CASES:
+        init = random_cell_state(np.random.default_rng(7), nx, ny) if kind == "random" else smooth_state(nx, ny)
+        params = zh.Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4, t_end=t_end)
+        t0 = time.time()
+        final, dts, steps, t = zmin.run_to_time(init, params, t_end, "cpu", bc)
+        arrays = {"u0": warp_shim.array(init, dtype=warp_shim.float64),
+                  "u1": warp_shim.zeros(params.padded_shape, dtype=warp_shim.float64)}
+        zmin._launch_stage(arrays["u0"], arrays["u0"], arrays["u1"], zmin._stage(params, "cpu"), params, dts[0], 1,
+                           "cpu", bc)
+        rec.update({f"{name}_initial": init, f"{name}_final": np.asarray(final), f"{name}_dts": np.asarray(dts),
+                    f"{name}_steps": steps, f"{name}_t": t, f"{name}_stage1": np.asarray(arrays["u1"]),
+                    f"{name}_nx": nx, f"{name}_ny": ny, f"{name}_t_end": t_end, f"{name}_bc": bc})
+        print(f"euler2d z {name}: steps={steps} t={t:.6g} ({time.time() - t0:.1f}s)", flush=True)
+    np.savez_compressed(out_dir / "euler2d_z.npz", **rec)
+
+
 def gen_mlp_golden(reference: Path) -> dict:
     sys.path.insert(0, str(reference / "scripts"))
     vr = importlib.import_module("verify_release")
@@ -262,6 +296,11 @@ def main() -> None:
     if "mlp" in only:
         np.savez_compressed(HERE / "mlp_golden.npz", **gen_mlp_golden(args.reference))
         print("mlp_golden.npz written", flush=True)
+    if "z" in only:
+        zh = importlib.import_module("weno_z_borges_p2_results.weno5_helpers_z")
+        zmin = importlib.import_module("weno_z_borges_p2_results.weno5_hllc_z_min")
+        gen_z(zh, zmin, HERE)
+        print("euler2d_z.npz written", flush=True)
 
 
 if __name__ == "__main__":

@@ -11,7 +11,7 @@ from oracle import oracle as O
 from weno_sr_publishing_b200 import euler2d as E
 from weno_sr_publishing_b200 import problems
 from weno_sr_publishing_b200.params import Params
-from weno_sr_publishing_b200.solvers import weno5_hllc, weno5_hllc_mixed, weno5_hllc_refsym
+from weno_sr_publishing_b200.solvers import weno5_hllc, weno5_hllc_mixed, weno5_hllc_refsym, weno5_hllc_z_min
 
 pytestmark = pytest.mark.gpu
 
@@ -20,10 +20,10 @@ MODELS = Path(__file__).resolve().parents[1] / "weno_sr_publishing_b200" / "mode
 NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")
 P64 = {k: v for k, v in np.load(MODELS / "weno5_sr_fp64_step012250.npz").items() if k in NAMES}
 P32 = {k: v for k, v in np.load(MODELS / "weno5_sr_fp32_step016500.npz").items() if k in NAMES}
-PARAMS = {"js": None, "sr_f64": P64, "sr_f32": P32, "sr_bf16": P32}
+PARAMS = {"js": None, "z": None, "sr_f64": P64, "sr_f32": P32, "sr_bf16": P32}
 # Relative max-norm tolerances of one stage against the oracle (FMA contraction and CUDA's libm account
 # for the FP64 differences; the FP32/BF16 closures differ in expf/tanhf rounding).
-STAGE_TOL = {"js": 1e-13, "sr_f64": 1e-12, "sr_f32": 2e-6, "sr_bf16": 5e-3}
+STAGE_TOL = {"js": 1e-13, "z": 1e-12, "sr_f64": 1e-12, "sr_f32": 2e-6, "sr_bf16": 5e-3}
 CASES = ["rough_trans", "quadrant_trans", "smooth_periodic"]
 DEV = "cuda:0"
 
@@ -41,7 +41,7 @@ def _t(a):
 
 
 @pytest.mark.parametrize("case", CASES)
-@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32", "sr_bf16"])
+@pytest.mark.parametrize("method", ["js", "z", "sr_f64", "sr_f32", "sr_bf16"])
 @pytest.mark.parametrize("rk", [1, 2, 3])
 def test_stage_matches_oracle(case, method, rk):
     e = np.load(G / f"euler2d_{case}.npz")
@@ -84,7 +84,26 @@ def test_run_to_time_matches_reference_fixture(case, method, adapter, tol):
     np.testing.assert_array_equal(ghost, ref_ghost)
 
 
-@pytest.mark.parametrize("method,tol", [("js", 1e-11), ("sr_f64", 1e-11), ("sr_f32", 1e-5)])
+@pytest.mark.parametrize("case", ["rough_trans", "smooth_periodic"])
+def test_z_run_to_time_matches_reference_fixture(case):
+    """WENO5-Z through the weno5_hllc_z_min adapter against the reference's minimal Z solver (dx != dy)."""
+    path = G / "euler2d_z.npz"
+    if not path.exists():
+        pytest.skip("euler2d_z.npz not generated")
+    z = np.load(path)
+    nx, ny, bc, t_end = int(z[f"{case}_nx"]), int(z[f"{case}_ny"]), str(z[f"{case}_bc"]), float(z[f"{case}_t_end"])
+    p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4, t_end=t_end)
+    final, dts, steps, t = weno5_hllc_z_min.run_to_time(z[f"{case}_initial"], p, t_end, DEV, bc)
+    assert steps == int(z[f"{case}_steps"]) and abs(t - float(z[f"{case}_t"])) <= 1e-14
+    np.testing.assert_allclose(dts, z[f"{case}_dts"], rtol=1e-12, atol=0)
+    assert _rel(_interior(final, nx, ny), _interior(z[f"{case}_final"], nx, ny)) <= 1e-12
+    arrays = weno5_hllc_z_min.allocate_forward(z[f"{case}_initial"], p, DEV)
+    weno5_hllc_z_min.launch_stage(arrays["u0"], arrays["u0"], arrays["u1"], arrays["s1"], p, dts[0], 1, DEV, bc)
+    got = arrays["u1"].cpu().numpy()
+    assert _rel(_interior(got, nx, ny), _interior(z[f"{case}_stage1"], nx, ny)) <= 1e-12
+
+
+@pytest.mark.parametrize("method,tol", [("js", 1e-11), ("z", 1e-11), ("sr_f64", 1e-11), ("sr_f32", 1e-5)])
 def test_quadrant_64x48_ten_steps_vs_oracle(method, tol):
     nx, ny = 64, 48
     init = problems.make_quadrant_state(nx, ny, problems.seeded_quadrant_states(3), 4)
@@ -99,7 +118,7 @@ def test_quadrant_64x48_ten_steps_vs_oracle(method, tol):
     np.testing.assert_allclose(res.dts, rdts, rtol=100 * tol)
 
 
-@pytest.mark.parametrize("method", ["js", "sr_f32"])
+@pytest.mark.parametrize("method", ["js", "z", "sr_f32"])
 def test_uniform_flow_is_preserved(method):
     nx, ny = 40, 33
     p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4)
@@ -111,7 +130,7 @@ def test_uniform_flow_is_preserved(method):
     assert _rel(got, _interior(u, nx, ny)) <= 1e-14
 
 
-@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32"])
+@pytest.mark.parametrize("method", ["js", "z", "sr_f64", "sr_f32"])
 def test_periodic_mass_conservation_256(method):
     nx = ny = 256
     p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4)
@@ -125,7 +144,7 @@ def test_periodic_mass_conservation_256(method):
     assert np.all(np.abs(m1 - m0) <= 1e-11 * np.abs(m0).max())
 
 
-@pytest.mark.parametrize("method", ["js", "sr_f64"])
+@pytest.mark.parametrize("method", ["js", "z", "sr_f64"])
 def test_xy_transpose_symmetry(method):
     nx = ny = 36
     p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4)

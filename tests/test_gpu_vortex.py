@@ -18,21 +18,29 @@ DEV = "cuda:0"
 # L1(rho) published in experiments/05_isentropic_vortex/tables/vortex_convergence.md
 PUBLISHED = {
     "js": {25: 2.09503105e-03, 50: 2.58534962e-04, 100: 1.70516911e-05, 200: 7.56466862e-07},
+    "z": {25: 1.20358031e-03, 50: 1.39351536e-04, 100: 8.44142862e-06, 200: 3.27070728e-07},
     "sr_f64": {25: 1.01691423e-03, 50: 8.40101626e-05, 100: 6.77814229e-06, 200: 2.70107746e-07},
     "sr_f32": {25: 1.01682875e-03, 50: 7.74117518e-05, 100: 6.11798199e-06, 200: 3.77746381e-07},
 }
-PARAMS = {"js": None, "sr_f64": P64, "sr_f32": P32}
+# L2(rho) column of the same table
+PUBLISHED_L2 = {
+    "js": {25: 9.74121493e-03, 50: 1.30721696e-03, 100: 9.50807226e-05, 200: 4.12767694e-06},
+    "z": {25: 4.93908021e-03, 50: 7.59669784e-04, 100: 4.21348293e-05, 200: 1.68818669e-06},
+    "sr_f64": {25: 4.64146546e-03, 50: 3.99561134e-04, 100: 2.87451263e-05, 200: 1.29509918e-06},
+    "sr_f32": {25: 4.71476896e-03, 50: 3.64743278e-04, 100: 2.52162435e-05, 200: 1.89868002e-06},
+}
+PARAMS = {"js": None, "z": None, "sr_f64": P64, "sr_f32": P32}
 
 
-@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32"])
+@pytest.mark.parametrize("method", ["js", "z", "sr_f64", "sr_f32"])
 @pytest.mark.parametrize("n", [25, 50, 100, 200])
 def test_vortex_l1_matches_published_table(method, n):
     r = A.vortex_run(n, method, PARAMS[method], DEV)
-    ref = PUBLISHED[method][n]
     # the table has 9 significant digits; the FP32 closure differs from the reference's GPU run in the last
     # float bits of exp/tanh
     tol = 1e-8 if method != "sr_f32" else 1e-5
-    assert abs(r.l1 / ref - 1.0) <= tol, (r.l1, ref)
+    for got, ref in ((r.l1, PUBLISHED[method][n]), (r.l2, PUBLISHED_L2[method][n])):
+        assert abs(got / ref - 1.0) <= tol, (got, ref)
 
 
 def test_matched_l1_interpolation():

@@ -138,3 +138,38 @@ def test_euler2d_first_stage(case):
         ref = e[f"{method}_stage1"]
         err = np.abs(out - ref).max() / np.abs(ref).max()
         assert err <= tol, (method, err)
+
+
+# WENO5-Z (weno_z_borges_p2_results): the oracle follows the reference's expression order, so it is
+# bitwise equal to the reference on every reconstruction and every run.
+def _z_fixture():
+    path = G / "euler2d_z.npz"
+    if not path.exists():
+        pytest.skip("euler2d_z.npz not generated")
+    return np.load(path)
+
+
+@pytest.mark.parametrize("hi", [0, 1])
+@pytest.mark.parametrize("key,head", [("lr1", 0), ("lr2", 1), ("g1", 2), ("g2", 3)])
+def test_z_reconstruction_bitwise(key, head, hi):
+    z = _z_fixture()
+    np.testing.assert_array_equal(O.reconstruct_h(z["q"], head, "z", float(z["h"][hi])), z[f"v_{key}_h{hi}"])
+
+
+def test_z_weights_differ_from_js():
+    """Sanity: the Z fixture is not the JS reconstruction in disguise."""
+    z = _z_fixture()
+    assert np.abs(O.reconstruct(z["q"], 0, "js") - z["v_lr1_h0"]).max() > 1e-6
+
+
+@pytest.mark.parametrize("case", ["rough_trans", "smooth_periodic"])
+def test_z_run_and_stage_bitwise(case):
+    z = _z_fixture()
+    nx, ny, bc = int(z[f"{case}_nx"]), int(z[f"{case}_ny"]), str(z[f"{case}_bc"])
+    init = z[f"{case}_initial"]
+    fin, dts, steps, t = O.euler2d_run(init, nx, ny, 1.0 / nx, 1.0 / ny, 0.4, float(z[f"{case}_t_end"]), "z", bc)
+    assert steps == int(z[f"{case}_steps"]) and t == float(z[f"{case}_t"])
+    np.testing.assert_array_equal(dts, z[f"{case}_dts"])
+    np.testing.assert_array_equal(fin, z[f"{case}_final"])
+    out = O.euler2d_stage(init, init, np.zeros_like(init), nx, ny, 1.0 / nx, 1.0 / ny, float(dts[0]), 1, "z", bc)
+    np.testing.assert_array_equal(out[3:-3, 3:-3], z[f"{case}_stage1"][3:-3, 3:-3])

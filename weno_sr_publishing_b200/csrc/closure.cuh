@@ -25,7 +25,11 @@
 
 namespace wsr {
 
-enum Method { M_JS = 0, M_SR64 = 1, M_SR32 = 2, M_SRBF16 = 3 };
+enum Method { M_JS = 0, M_SR64 = 1, M_SR32 = 2, M_SRBF16 = 3, M_Z = 4 };
+
+// Methods whose weights come from the MLP closure (and so run the compacted plateau/queue split).
+template <int M>
+__host__ __device__ constexpr bool has_mlp() { return M == M_SR64 || M == M_SR32 || M == M_SRBF16; }
 
 // Packed parameters, layout w1[5][10] b1[10] w2[10][6] b2[6] w3[6][6] b3[6] w4[6][3] b4[3].
 constexpr int kW1 = 0, kB1 = 50, kW2 = 60, kB2 = 120, kW3 = 126, kB3 = 162, kW4 = 168, kB4 = 186;
@@ -42,6 +46,10 @@ struct Mlp5f {
   }
 };
 struct NoParams {};
+// WENO-Z smoothness epsilon h^2 per grid direction (x: dx^2, y: dy^2).
+struct ZEps {
+  double ex, ey;
+};
 
 template <int M>
 struct ClosureParams {
@@ -58,6 +66,10 @@ struct ClosureParams<M_SR32> {
 template <>
 struct ClosureParams<M_SRBF16> {
   using type = Mlp5f;  // pre-rounded to bfloat16 on upload
+};
+template <>
+struct ClosureParams<M_Z> {
+  using type = ZEps;
 };
 
 // Options bitmask. OPT_COUNT makes the reconstruction kernels count closure evaluations (SR stencils
@@ -567,6 +579,46 @@ __device__ __forceinline__ double js_value(const double s[5], int head) {
   js_head_weights(js_stencil(s), linear_weights(head), w);
   candidates(s, head, c);
   return combine(w, c);
+}
+
+// WENO-Z (Borges, Carmona, Costa & Don 2008, p = 2) with eps = h^2 along the reconstruction direction
+// (weno_z_borges_p2_results/weno5_helpers_z.py:545-574, 853-879): tau5 = |beta0 - beta2|,
+// alpha_k = d_k (1 + (tau5 / (beta_k + eps))^2), w = alpha / sum. The head-independent factors
+// g_k = 1 + ratio_k^2 are formed once per stencil and serve both Gauss heads.
+__device__ __forceinline__ StencilW z_stencil(const double q[5], double eps) {
+  double t2 = q[2] - 2.0 * q[3] + q[4], u2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
+  double t1 = q[1] - 2.0 * q[2] + q[3], u1 = q[1] - q[3];
+  double t0 = q[0] - 2.0 * q[1] + q[2], u0 = q[0] - 4.0 * q[1] + 3.0 * q[2];
+  double b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * u2 * u2;
+  double b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * u1 * u1;
+  double b0 = (13.0 / 12.0) * t0 * t0 + 0.25 * u0 * u0;
+  const double tau = fabs(b0 - b2);
+  const double r0 = tau * rcp64(b0 + eps), r1 = tau * rcp64(b1 + eps), r2 = tau * rcp64(b2 + eps);
+  StencilW s;
+  s.a0 = 1.0 + r0 * r0;
+  s.a1 = 1.0 + r1 * r1;
+  s.a2 = 1.0 + r2 * r2;
+  s.linear = false;
+  return s;
+}
+
+__device__ __forceinline__ void z_head_weights(const StencilW& s, const Lin3& d, double w[3]) {
+  double a0 = d.d0 * s.a0, a1 = d.d1 * s.a1, a2 = d.d2 * s.a2;
+  double inv = rcp64(a0 + a1 + a2);
+  w[0] = a0 * inv;
+  w[1] = a1 * inv;
+  w[2] = a2 * inv;
+}
+
+__device__ __forceinline__ double z_value_w(const StencilW& z, const double s[5], int head) {
+  double w[3], c[3];
+  z_head_weights(z, linear_weights(head), w);
+  candidates(s, head, c);
+  return combine(w, c);
+}
+
+__device__ __forceinline__ double z_value(const double s[5], int head, double eps) {
+  return z_value_w(z_stencil(s, eps), s, head);
 }
 
 }  // namespace wsr

@@ -180,16 +180,18 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
       for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][t];
       if constexpr (M == M_JS) {
         s_val[n][t] = js_value(s, side);
+      } else if constexpr (M == M_Z) {
+        s_val[n][t] = z_value(s, side, DIR == 1 ? P.ex : P.ey);  // eps = h^2 of the normal direction
       } else {
         need = !is_plateau(sensors5(s));
         if (!need) s_val[n][t] = linear_value(s, side);
         ++(need ? tally.mlp : tally.plateau);
       }
     }
-    if constexpr (M != M_JS) queue_push(need, n * kBlock + t, s_q, &s_count);
+    if constexpr (has_mlp<M>()) queue_push(need, n * kBlock + t, s_q, &s_count);
   }
   // Phase B
-  if constexpr (M != M_JS) {
+  if constexpr (has_mlp<M>()) {
     __syncthreads();
     const int count = s_count;
 #pragma unroll 1
@@ -210,7 +212,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
     for (int side = 0; side < 2; ++side) {
       double cf[4] = {s_val[side][t], s_val[2 + side][t], s_val[4 + side][t], s_val[6 + side][t]};
       d4 face = char_to_con<DIR>(cf, J);
-      if constexpr (M != M_JS) {
+      if constexpr (has_mlp<M>()) {
         if ((opts & OPT_JS_FALLBACK) && !admissible(face, gas.g)) {
           // positivity fallback: redo this face value with JS weights
           double jf[4];
@@ -307,6 +309,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       js_head_weights(js, linear_weights(3), w);
       candidates(s, 3, c);
       s_g[1][n][t] = combine(w, c);
+    } else if constexpr (M == M_Z) {
+      const StencilW z = z_stencil(s, DIR == 1 ? P.ey : P.ex);  // eps = h^2 of the transverse direction
+      s_g[0][n][t] = z_value_w(z, s, 2);
+      s_g[1][n][t] = z_value_w(z, s, 3);
     } else {
       need = !is_plateau(sensors5(s));
       if (!need) {
@@ -315,10 +321,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       }
       ++(need ? tally.mlp : tally.plateau);
     }
-    if constexpr (M != M_JS) queue_push(need, n * kBlock + t, s_q, &s_count);
+    if constexpr (has_mlp<M>()) queue_push(need, n * kBlock + t, s_q, &s_count);
   }
   // Phase B: one closure evaluation per queued stencil serves both Gauss points.
-  if constexpr (M != M_JS) {
+  if constexpr (has_mlp<M>()) {
     __syncthreads();
     const int count = s_count;
 #pragma unroll 1

@@ -70,10 +70,10 @@ int check_2d(wsr_ctx* ctx, int nx, int ny, int method, int bc, int flux, void* w
   if (nx < 3 || ny < 3) return fail(ctx, WSR_ERR_ARG, "nx and ny must be >= 3 (got %d, %d)", nx, ny);
   if ((long long)(nx + 6) * (ny + 6) > (1ll << 31) / 4)
     return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
-  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
   if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC) return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
   if (flux != WSR_FLUX_HLLC && flux != WSR_FLUX_FORCE) return fail(ctx, WSR_ERR_ARG, "bad flux %d", flux);
-  if (method != WSR_METHOD_JS && !ctx->have_closure)
+  if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && !ctx->have_closure)
     return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before wsr_closure_upload");
   if (!ws) return fail(ctx, WSR_ERR_ARG, "workspace is NULL");
   if (reinterpret_cast<uintptr_t>(ws) % kAlign) return fail(ctx, WSR_ERR_ARG, "workspace must be 256-byte aligned");
@@ -121,9 +121,18 @@ struct StageArgs {
 };
 
 // One stage = 5 launches. dt/dx and dt/dy are read from ws.ctl on the device.
+// Kernel parameters of a method: the uploaded closure, or for WENO-Z the per-direction eps = h^2.
+template <int M>
+typename ClosureParams<M>::type stage_params(const wsr_ctx* ctx, const StageArgs& a) {
+  if constexpr (M == M_Z)
+    return ZEps{a.dx * a.dx, a.dy * a.dy};
+  else
+    return params_of<M>(ctx);
+}
+
 template <int M>
 int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
-  const auto& P = params_of<M>(ctx);
+  const auto P = stage_params<M>(ctx, a);
   const dim3 blk(128);  // the reconstruction kernels compact closure work per warp of a 128-thread block
   {
     ProfScope ps(ctx, st, 0);
@@ -170,6 +179,8 @@ int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, 
       return launch_stage<M_SR64>(ctx, a, w, st);
     case WSR_METHOD_SR_F32:
       return launch_stage<M_SR32>(ctx, a, w, st);
+    case WSR_METHOD_Z:
+      return launch_stage<M_Z>(ctx, a, w, st);
     default:
       return launch_stage<M_SRBF16>(ctx, a, w, st);
   }

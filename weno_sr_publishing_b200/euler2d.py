@@ -58,7 +58,9 @@ def _check_state(u: torch.Tensor, p: Params) -> None:
 
 def prepare_closure(method: str, mlp_params, dev: int) -> N.Context:
     ctx = N.context(dev)
-    if method != "js":
+    if method not in N.METHOD:
+        raise ValueError(f"unknown method {method!r}")
+    if method in N.SR_METHODS:
         if mlp_params is None:
             raise ValueError(f"method {method!r} needs mlp_params")
         ctx.upload_closure(N.pack_params(mlp_params))
