@@ -46,6 +46,8 @@ extern "C" {
 /* boundaries */
 #define WSR_BC_TRANSMISSIVE 0
 #define WSR_BC_PERIODIC 1
+#define WSR_BC_DOUBLE_MACH 2 /* Mach-10 double-Mach reflection on [0, nx dx] x [0, ny dy] (time dependent;
+                                 weno5_hllc_refsym.py:26-124); 2D stage and run functions only */
 
 /* interface fluxes */
 #define WSR_FLUX_HLLC 0
@@ -78,6 +80,13 @@ size_t wsr_euler2d_workspace_bytes(int nx, int ny);
 int wsr_euler2d_stage(wsr_ctx *ctx, const double *u_stage, const double *u0, double *u_out, int nx, int ny,
                       double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux,
                       int opts, void *workspace, size_t workspace_bytes, void *stream);
+
+/* wsr_euler2d_stage with the boundary evaluated at boundary_time (the reference's launch_stage
+ * boundary_time argument, weno5_hllc_refsym.py:298-311); only the double-Mach boundary depends on it.
+ * wsr_euler2d_run uses t, t + dt and t + dt/2 for the three stages of a step. */
+int wsr_euler2d_stage_at(wsr_ctx *ctx, const double *u_stage, const double *u0, double *u_out, int nx, int ny,
+                         double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux,
+                         int opts, double boundary_time, void *workspace, size_t workspace_bytes, void *stream);
 
 /* max over the interior of max(|u|+c, |v|+c), rho and p floored at 1e-15. Synchronises `stream`
  * and writes the host value. */

@@ -36,7 +36,7 @@
 #define GC 3
 
 enum { OR_METHOD_JS = 0, OR_METHOD_SR64 = 1, OR_METHOD_SR32 = 2, OR_METHOD_SRBF16 = 3, OR_METHOD_Z = 4 };
-enum { OR_BC_TRANSMISSIVE = 0, OR_BC_PERIODIC = 1 };
+enum { OR_BC_TRANSMISSIVE = 0, OR_BC_PERIODIC = 1, OR_BC_DOUBLE_MACH = 2 };
 enum { OR_FLUX_HLLC = 0, OR_FLUX_FORCE = 1 };
 
 typedef struct { double v[4]; } vec4;
@@ -476,6 +476,7 @@ typedef struct {
     double dx, dy, gamma;
     const double *P64;
     const float *P32;
+    double bt; /* boundary time of the stage (double-Mach only) */
 } or_cfg;
 
 static inline vec4 load4(const double *a, int nxt, int j, int i) {
@@ -487,6 +488,47 @@ static inline void store4(double *a, int nxt, int j, int i, vec4 q) {
     memcpy(a + ((size_t)j * nxt + i) * 4, q.v, sizeof(q.v));
 }
 
+/* Double-Mach reflection (REFSYM:26-124): a Mach-10 shock through (1/6, 0) at 60 degrees to the wall.
+ * The exact pre/post-shock state fills the top ghost rows (at the shock position of time t), the left ghost
+ * columns and the bottom ghost rows left of x = 1/6; the bottom ghost rows right of it reflect the interior
+ * (v negated); the right ghost columns copy the last interior column. */
+static vec4 double_mach_state(double x, double y, double t, double g) {
+    double r3 = sqrt(3.0);
+    double shock_x = 1.0 / 6.0 + y / r3 + 20.0 * t / r3;
+    double rho, u, v, p;
+    if (x < shock_x) { rho = 8.0; u = 8.25 * r3 * 0.5; v = -8.25 * 0.5; p = 116.5; }
+    else { rho = 1.4; u = 0.0; v = 0.0; p = 1.0; }
+    vec4 q = {{rho, rho * u, rho * v, 0.5 * rho * (u * u + v * v) + p / (g - 1.0)}};
+    return q;
+}
+
+static void apply_double_mach(double *a, const or_cfg *c) {
+    int nx = c->nx, ny = c->ny, nxt = nx + 2 * GC, nyt = ny + 2 * GC;
+    for (int j = 0; j < nyt; ++j) {
+        for (int i = 0; i < nxt; ++i) {
+            int in_x = i >= GC && i < nx + GC, in_y = j >= GC && j < ny + GC;
+            if (in_x && in_y) continue;
+            double x = ((double)(i - GC) + 0.5) * c->dx, y = ((double)(j - GC) + 0.5) * c->dy;
+            if (j >= ny + GC) {
+                store4(a, nxt, j, i, double_mach_state(x, y, c->bt, c->gamma));
+            } else if (j < GC) {
+                if (x < 1.0 / 6.0) {
+                    store4(a, nxt, j, i, double_mach_state(x, 0.0, c->bt, c->gamma));
+                } else {
+                    int si = i < GC ? GC : (i >= nx + GC ? nx + GC - 1 : i);
+                    vec4 q = load4(a, nxt, 2 * GC - 1 - j, si);
+                    q.v[2] = -q.v[2];
+                    store4(a, nxt, j, i, q);
+                }
+            } else if (i < GC) {
+                store4(a, nxt, j, i, double_mach_state(x, y, c->bt, c->gamma));
+            } else {
+                store4(a, nxt, j, i, load4(a, nxt, j, nx + GC - 1));
+            }
+        }
+    }
+}
+
 /* copy_transmissive_boundary_kernel / copy_periodic_boundary_kernel (DEPLOY:371-408) */
 static void apply_bc(const double *src, double *dst, const or_cfg *c) {
     int nxt = c->nx + 2 * GC, nyt = c->ny + 2 * GC;
@@ -494,7 +536,7 @@ static void apply_bc(const double *src, double *dst, const or_cfg *c) {
     for (int j = 0; j < nyt; ++j) {
         for (int i = 0; i < nxt; ++i) {
             int si = i, sj = j;
-            if (c->bc == OR_BC_TRANSMISSIVE) {
+            if (c->bc != OR_BC_PERIODIC) {
                 if (i < GC) si = GC; else if (i >= c->nx + GC) si = c->nx + GC - 1;
                 if (j < GC) sj = GC; else if (j >= c->ny + GC) sj = c->ny + GC - 1;
             } else {
@@ -504,6 +546,7 @@ static void apply_bc(const double *src, double *dst, const or_cfg *c) {
             store4(dst, nxt, j, i, load4(src, nxt, sj, si));
         }
     }
+    if (c->bc == OR_BC_DOUBLE_MACH) apply_double_mach(dst, c);
 }
 
 /* Characteristic normal reconstruction of the cell centred on stencil q[2]: left face (lr=2,
@@ -660,16 +703,23 @@ static void free_stage(or_stage_buf *b) {
     free(b->fx1); free(b->fx2); free(b->fy1); free(b->fy2);
 }
 
-/* One SSPRK3 stage: u_out(interior) from u_stage and u0. Returns 0 on success. */
-int or_euler2d_stage(const double *u_stage, const double *u0, double *u_out, int nx, int ny, double dx,
-                     double dy, double gamma, double dt, int rk, int method, int bc, int flux,
-                     const double *P64, const float *P32) {
-    or_cfg c = {nx, ny, method, bc, flux, dx, dy, gamma, P64, P32};
+/* One SSPRK3 stage: u_out(interior) from u_stage and u0, with the boundary evaluated at boundary_time
+ * (the double-Mach boundary depends on it). Returns 0 on success. */
+int or_euler2d_stage_at(const double *u_stage, const double *u0, double *u_out, int nx, int ny, double dx,
+                        double dy, double gamma, double dt, int rk, int method, int bc, int flux,
+                        const double *P64, const float *P32, double boundary_time) {
+    or_cfg c = {nx, ny, method, bc, flux, dx, dy, gamma, P64, P32, boundary_time};
     or_stage_buf b;
     if (alloc_stage(&b, padded_len(nx, ny))) { free_stage(&b); return -1; }
     stage(u_stage, u0, u_out, dt, rk, &c, &b);
     free_stage(&b);
     return 0;
+}
+
+int or_euler2d_stage(const double *u_stage, const double *u0, double *u_out, int nx, int ny, double dx,
+                     double dy, double gamma, double dt, int rk, int method, int bc, int flux,
+                     const double *P64, const float *P32) {
+    return or_euler2d_stage_at(u_stage, u0, u_out, nx, ny, dx, dy, gamma, dt, rk, method, bc, flux, P64, P32, 0.0);
 }
 
 /* run_to_time (REFSYM:462-544, MIXED:185-212, HLLC5:386-410). State buffers follow the reference:
@@ -698,8 +748,12 @@ int or_euler2d_run(const double *initial, double *out, int nx, int ny, double dx
         double dt = ms < 1.0e-15 ? 1.0e10 : cfl * hmin / ms;
         if (fixed_steps <= 0 && t_end - t < dt) dt = t_end - t;
         if (!isfinite(dt) || dt <= 0.0) break;
+        /* boundary times of the three stages: t, t + dt, t + dt/2 (REFSYM:479-527) */
+        c.bt = t;
         stage(u[0], u[0], u[1], dt, 1, &c, &b);
+        c.bt = t + dt;
         stage(u[1], u[0], u[2], dt, 2, &c, &b);
+        c.bt = t + 0.5 * dt;
         stage(u[2], u[0], u[3], dt, 3, &c, &b);
         double *tmp = u[0]; u[0] = u[3]; u[3] = tmp;
         t += dt;

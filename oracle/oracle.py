@@ -13,7 +13,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 
 METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3, "z": 4}
-BC = {"transmissive": 0, "periodic": 1}
+BC = {"transmissive": 0, "periodic": 1, "double-mach": 2}
 FLUX = {"hllc": 0, "force": 1}
 N_PARAMS5 = 189
 PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")
@@ -39,6 +39,8 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_euler2d_stage.restype = C.c_int
         lib.or_euler2d_stage.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _fp]
+        lib.or_euler2d_stage_at.restype = C.c_int
+        lib.or_euler2d_stage_at.argtypes = lib.or_euler2d_stage.argtypes + [C.c_double]
         lib.or_euler2d_max_speed.restype = C.c_double
         lib.or_euler2d_max_speed.argtypes = [_dp, C.c_int, C.c_int, C.c_double]
         lib.or_hllc_flux_flat.argtypes = [_dp, _dp, C.c_int, C.c_double, _dp]
@@ -125,13 +127,13 @@ def max_speed(u: np.ndarray, nx: int, ny: int, gamma: float = 1.4) -> float:
 
 
 def euler2d_stage(u_stage, u0, u_out, nx, ny, dx, dy, dt, rk, method, bc="transmissive", flux="hllc",
-                  params=None, gamma=1.4) -> np.ndarray:
+                  params=None, gamma=1.4, boundary_time=0.0) -> np.ndarray:
     """One SSPRK3 stage; returns a copy of u_out with its interior overwritten."""
     out = np.array(u_out, dtype=np.float64, copy=True)
     p64, p32 = _params(params)
-    rc = _lib().or_euler2d_stage(np.ascontiguousarray(u_stage, dtype=np.float64),
-                                 np.ascontiguousarray(u0, dtype=np.float64), out, nx, ny, dx, dy, gamma, dt, rk,
-                                 METHOD[method], BC[bc], FLUX[flux], p64, p32)
+    rc = _lib().or_euler2d_stage_at(np.ascontiguousarray(u_stage, dtype=np.float64),
+                                    np.ascontiguousarray(u0, dtype=np.float64), out, nx, ny, dx, dy, gamma, dt, rk,
+                                    METHOD[method], BC[bc], FLUX[flux], p64, p32, float(boundary_time))
     if rc != 0:
         raise MemoryError("oracle stage allocation failed")
     return out

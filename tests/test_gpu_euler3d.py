@@ -139,3 +139,18 @@ def test_invalid_arguments_raise():
     q = torch.zeros((11, 11, 11, 5), dtype=torch.float64, device=DEV)
     with pytest.raises(ValueError):
         E3.run(q, 5, 5, 5, 0.1, 0.1, 0.1, 0.4, "sr_f64", steps=1)  # SR without parameters
+
+
+def test_step_file_of_device_state(tmp_path):
+    """The device state written as a step file (uint32 nz ny nx, f64 time, f64 primitive) reads back as the
+    primitive interior of the oracle's state."""
+    from weno_sr_publishing_b200 import binary_io as B  # noqa: PLC0415
+    nx, ny, nz = 12, 9, 7
+    q0 = _random_state(nx, ny, nz, 11)
+    ref, dts = O.euler3d_run(q0, nx, ny, nz, 0.1, 0.1, 0.1, 0.4, 2, "js", "hllc")
+    q = torch.as_tensor(q0, device=DEV).contiguous()
+    res = E3.run(q, nx, ny, nz, 0.1, 0.1, 0.1, 0.4, "js", "hllc", steps=2)
+    B.write_state(tmp_path / "step.bin", res.t, q, nx, ny, nz)
+    t, prim = B.read_step(tmp_path / "step.bin")
+    assert t == res.t and prim.shape == (nz, ny, nx, 5)
+    np.testing.assert_array_equal(prim, B.primitive_interior(ref, nx, ny, nz))

@@ -173,3 +173,64 @@ def test_z_run_and_stage_bitwise(case):
     np.testing.assert_array_equal(fin, z[f"{case}_final"])
     out = O.euler2d_stage(init, init, np.zeros_like(init), nx, ny, 1.0 / nx, 1.0 / ny, float(dts[0]), 1, "z", bc)
     np.testing.assert_array_equal(out[3:-3, 3:-3], z[f"{case}_stage1"][3:-3, 3:-3])
+
+
+# Double-Mach boundary (time dependent): the oracle against the reference's own runs with
+# boundary="double-mach" on a 32 x 8 grid of [0, 4] x [0, 1] (tests/golden/make_golden_double_mach.py).
+@pytest.mark.parametrize("method,tol", [("z", 0.0), ("sr_f64", 1e-13), ("sr_f32", 2e-6)])
+def test_double_mach_run_matches_reference(method, tol):
+    path = G / "double_mach.npz"
+    if not path.exists():
+        pytest.skip("double_mach.npz not generated")
+    d = np.load(path)
+    nx, ny = int(d["nx"]), int(d["ny"])
+    params = {"z": None, "sr_f64": P64, "sr_f32": P32}[method]
+    fin, dts, steps, t = O.euler2d_run(d["initial"], nx, ny, 4.0 / nx, 1.0 / ny, 0.4, float(d["t_end"]), method,
+                                       "double-mach", params=params)
+    assert steps == int(d[f"{method}_steps"]) and abs(t - float(d[f"{method}_t"])) < 1e-15
+    np.testing.assert_allclose(dts, d[f"{method}_dts"], rtol=max(tol, 1e-16), atol=0)
+    ref = d[f"{method}_final"][3:-3, 3:-3]
+    err = np.abs(fin[3:-3, 3:-3] - ref).max() / np.abs(ref).max()
+    assert err <= tol, err
+
+
+def test_double_mach_initial_state_matches_reference():
+    from weno_sr_publishing_b200 import problems  # noqa: PLC0415
+    path = G / "double_mach.npz"
+    if not path.exists():
+        pytest.skip("double_mach.npz not generated")
+    d = np.load(path)
+    s = problems.double_mach_state(int(d["nx"]), int(d["ny"]))
+    assert np.abs(s - d["initial"]).max() <= 1e-14 * np.abs(d["initial"]).max()
+
+
+def test_double_mach_wall_face_is_ill_conditioned():
+    """The reference's double-Mach run on the coarse fixture grid is sensitive at the 1e-7 level: a one-ulp
+    change of the first dt flips the sign of the HLLC contact speed (about 1e-17) on wall faces whose
+    reconstructed states have negative energy, and with it the sign of their energy flux. This bounds how
+    closely any other arithmetic (FMA contraction, a different reciprocal) can follow the reference."""
+    path = G / "double_mach.npz"
+    if not path.exists():
+        pytest.skip("double_mach.npz not generated")
+    d = np.load(path)
+    nx, ny = int(d["nx"]), int(d["ny"])
+    dx, dy = 4.0 / nx, 1.0 / ny
+
+    def run(dts):
+        u0, t = d["initial"], 0.0
+        for dt in dts:
+            u1 = O.euler2d_stage(u0, u0, np.zeros_like(u0), nx, ny, dx, dy, dt, 1, "z", "double-mach",
+                                 boundary_time=t)
+            u2 = O.euler2d_stage(u1, u0, np.zeros_like(u0), nx, ny, dx, dy, dt, 2, "z", "double-mach",
+                                 boundary_time=t + dt)
+            u0 = O.euler2d_stage(u2, u0, np.zeros_like(u0), nx, ny, dx, dy, dt, 3, "z", "double-mach",
+                                 boundary_time=t + 0.5 * dt)
+            t += dt
+        return u0[3:-3, 3:-3]
+
+    dts = [float(v) for v in d["z_dts"]]
+    a = run(dts)
+    np.testing.assert_array_equal(a, d["z_final"][3:-3, 3:-3])
+    b = run([float(np.nextafter(dts[0], 1.0))] + dts[1:])
+    rel = np.abs(a - b).max() / np.abs(a).max()
+    assert 1e-7 < rel < 2e-6, rel

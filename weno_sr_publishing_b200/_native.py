@@ -18,7 +18,7 @@ WSR_OK, WSR_ERR_ARG, WSR_ERR_CUDA, WSR_ERR_NO_CLOSURE = 0, 1, 2, 3
 METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3, "z": 4}
 # methods whose weights come from an uploaded MLP closure
 SR_METHODS = ("sr_f64", "sr_f32", "sr_bf16")
-BC = {"transmissive": 0, "periodic": 1}
+BC = {"transmissive": 0, "periodic": 1, "double-mach": 2}
 FLUX = {"hllc": 0, "force": 1}
 FLUX3 = {"evilin": 0, "hllc": 1}
 OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT = 1, 2, 4
@@ -52,6 +52,7 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_workspace_bytes.argtypes = [i, i]
             L.wsr_euler2d_workspace_bytes.restype = sz
             L.wsr_euler2d_stage.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, vp, sz, vp]
+            L.wsr_euler2d_stage_at.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, d, vp, sz, vp]
             L.wsr_euler2d_max_speed.argtypes = [vp, vp, i, i, d, C.POINTER(d), vp, sz, vp]
             L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
                                           C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
@@ -81,7 +82,7 @@ def lib() -> C.CDLL:
 
 def exported_symbols() -> list[str]:
     return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
-            "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_max_speed", "wsr_euler2d_run",
+            "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_stage_at", "wsr_euler2d_max_speed", "wsr_euler2d_run",
             "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops",
             "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
             "wsr_train1d_backward", "wsr_euler3d_workspace_bytes", "wsr_euler3d_stage", "wsr_euler3d_max_speed",

@@ -25,7 +25,15 @@ namespace wsr {
 
 constexpr int kGhost = 3;
 
-enum Bc { BC_TRANSMISSIVE = 0, BC_PERIODIC = 1 };
+enum Bc { BC_TRANSMISSIVE = 0, BC_PERIODIC = 1, BC_DOUBLE_MACH = 2 };
+
+// Boundary of one stage. The double-Mach boundary is time dependent: it is evaluated at
+// ctl->t + t_off * ctl->dt (the SSPRK3 stages use t, t + dt and t + dt/2, REFSYM:462-527), on the cell
+// centres ((i - 3 + 1/2) dx, (j - 3 + 1/2) dy) of the padded grid.
+struct StageBc {
+  int kind;
+  double dx, dy, t_off;
+};
 enum Flux { FLUX_HLLC = 0, FLUX_FORCE = 1 };
 
 // Device-resident time-step control block (one per run).
@@ -65,6 +73,44 @@ __device__ __forceinline__ void store_cell(double* __restrict__ u, size_t idx, c
   double2* p = reinterpret_cast<double2*>(u + idx * 4);
   p[0] = make_double2(q.v[0], q.v[1]);
   p[1] = make_double2(q.v[2], q.v[3]);
+}
+
+// Double-Mach reflection (REFSYM:26-124): a Mach-10 shock through (1/6, 0) at 60 degrees to the wall.
+// Exact pre/post-shock state at (x, y) and time t, with round-to-nearest operations in the reference's order.
+__device__ __noinline__ d4 double_mach_state(double x, double y, double t, double g) {
+  const double r3 = __dsqrt_rn(3.0);
+  const double shock_x = __dadd_rn(__dadd_rn(1.0 / 6.0, __ddiv_rn(y, r3)), __ddiv_rn(__dmul_rn(20.0, t), r3));
+  double rho = 1.4, u = 0.0, v = 0.0, p = 1.0;
+  if (x < shock_x) {
+    rho = 8.0;
+    u = __dmul_rn(__dmul_rn(8.25, r3), 0.5);
+    v = -4.125;
+    p = 116.5;
+  }
+  const double e = __dadd_rn(__dmul_rn(__dmul_rn(0.5, rho), __dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v))),
+                             __ddiv_rn(p, __dsub_rn(g, 1.0)));
+  return d4{{rho, __dmul_rn(rho, u), __dmul_rn(rho, v), e}};
+}
+
+// Value of the ghost cell at padded (pj, pi) under the double-Mach boundary: the exact state on the top rows
+// (all columns), the left columns and the bottom rows left of x = 1/6 (there at y = 0); a reflection of the
+// interior (v negated, column clamped to the interior) on the bottom rows right of it; a copy of the last
+// interior column on the right.
+__device__ __noinline__ d4 double_mach_ghost(const double* __restrict__ u, int nx, int ny, int pj, int pi,
+                                             const StageBc& bc, double t, double g) {
+  const int nxt = nx + 2 * kGhost;
+  const double x = __dmul_rn((double)(pi - kGhost) + 0.5, bc.dx);
+  const double y = __dmul_rn((double)(pj - kGhost) + 0.5, bc.dy);
+  if (pj >= ny + kGhost) return double_mach_state(x, y, t, g);
+  if (pj < kGhost) {
+    if (x < 1.0 / 6.0) return double_mach_state(x, 0.0, t, g);
+    const int si = pi < kGhost ? kGhost : (pi >= nx + kGhost ? nx + kGhost - 1 : pi);
+    d4 q = load_cell(u, nxt, 2 * kGhost - 1 - pj, si);
+    q.v[2] = -q.v[2];
+    return q;
+  }
+  if (pi < kGhost) return double_mach_state(x, y, t, g);
+  return load_cell(u, nxt, pj, nx + kGhost - 1);
 }
 
 __device__ __forceinline__ bool admissible(const d4& q, double g) {  // rho > 0 and p > 0
@@ -130,7 +176,7 @@ __device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q,
 // -------------------------------------------------------------------------------------------
 template <int M, int DIR>
 __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
-                                                      double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
+                                                      double* __restrict__ out_r, int nx, int ny, StageBc bc, Gas gas,
                                                       const StepCtl* __restrict__ ctl, int opts,
                                                       int* __restrict__ fallbacks,
                                                       unsigned long long* __restrict__ counters,
@@ -152,11 +198,14 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
   {
     // cells are loaded one at a time for the projection (L1 hits after the first touch), which keeps
     // the six-cell stencil out of the register budget
+    const double bt = bc.kind == BC_DOUBLE_MACH ? ctl->t + bc.t_off * ctl->dt : 0.0;
     auto cell = [&](int k) {
       if (!active) return d4{{1.0, 0.0, 0.0, 2.5}};  // inert filler for threads past the edge
       const int pj = DIR == 1 ? r : r + k;
       const int pi = DIR == 1 ? c + k : c;
-      return load_cell(u, nxt, map_index(pj, ny, bc), map_index(pi, nx, bc));
+      if (bc.kind == BC_DOUBLE_MACH && (pj < kGhost || pj >= ny + kGhost || pi < kGhost || pi >= nx + kGhost))
+        return double_mach_ghost(u, nx, ny, pj, pi, bc, bt, gas.g);
+      return load_cell(u, nxt, map_index(pj, ny, bc.kind), map_index(pi, nx, bc.kind));
     };
     J = roe_jacobian(cell(2), cell(3), gas);
     const CharL L = char_left<DIR>(J, gas);

@@ -71,7 +71,8 @@ int check_2d(wsr_ctx* ctx, int nx, int ny, int method, int bc, int flux, void* w
   if ((long long)(nx + 6) * (ny + 6) > (1ll << 31) / 4)
     return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
   if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
-  if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC) return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
+  if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC && bc != WSR_BC_DOUBLE_MACH)
+    return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
   if (flux != WSR_FLUX_HLLC && flux != WSR_FLUX_FORCE) return fail(ctx, WSR_ERR_ARG, "bad flux %d", flux);
   if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && !ctx->have_closure)
     return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before wsr_closure_upload");
@@ -118,9 +119,12 @@ struct StageArgs {
   double* u_out;
   int nx, ny, bc, flux, opts, rk;
   double dx, dy, g;
+  double t_off;  // boundary time of the stage = ctl->t + t_off * ctl->dt
 };
 
 // One stage = 5 launches. dt/dx and dt/dy are read from ws.ctl on the device.
+inline StageBc stage_bc(const StageArgs& a) { return StageBc{a.bc, a.dx, a.dy, a.t_off}; }
+
 // Kernel parameters of a method: the uploaded closure, or for WENO-Z the per-direction eps = h^2.
 template <int M>
 typename ClosureParams<M>::type stage_params(const wsr_ctx* ctx, const StageArgs& a) {
@@ -137,14 +141,14 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t s
   {
     ProfScope ps(ctx, st, 0);
     dim3 grd((a.nx + 1 + 127) / 128, a.ny + 5);
-    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks,
+    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks,
                                         w.counters + 0, P);
   }
   WSR_LAUNCHED(ctx, "k_normal<x>");
   {
     ProfScope ps(ctx, st, 1);
     dim3 grd((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4);
-    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks,
+    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks,
                                         w.counters + 2, P);
   }
   WSR_LAUNCHED(ctx, "k_normal<y>");
@@ -299,9 +303,9 @@ size_t wsr_euler2d_workspace_bytes(int nx, int ny) {
   return ws_bytes(nx, ny);
 }
 
-int wsr_euler2d_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, double* u_out, int nx, int ny,
-                      double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux, int opts,
-                      void* workspace, size_t workspace_bytes, void* stream) {
+int wsr_euler2d_stage_at(wsr_ctx* ctx, const double* u_stage, const double* u0, double* u_out, int nx, int ny,
+                         double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux, int opts,
+                         double boundary_time, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
   if (rc) return rc;
   if (!u_stage || !u0 || !u_out) return fail(ctx, WSR_ERR_ARG, "null state pointer");
@@ -312,10 +316,17 @@ int wsr_euler2d_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, dou
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
   Ws2d w = carve(workspace, nx, ny);
-  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, boundary_time, 1.0e300, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
   WSR_LAUNCHED(ctx, "k_init_ctl");
-  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma};
+  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma, 0.0};
   return dispatch_stage(ctx, method, a, w, st);
+}
+
+int wsr_euler2d_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, double* u_out, int nx, int ny,
+                      double dx, double dy, double gamma, double dt, int rk, int method, int bc, int flux, int opts,
+                      void* workspace, size_t workspace_bytes, void* stream) {
+  return wsr_euler2d_stage_at(ctx, u_stage, u0, u_out, nx, ny, dx, dy, gamma, dt, rk, method, bc, flux, opts, 0.0,
+                              workspace, workspace_bytes, stream);
 }
 
 int wsr_euler2d_max_speed(wsr_ctx* ctx, const double* u, int nx, int ny, double gamma, double* out_host,
@@ -384,9 +395,9 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
         k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
       }
       WSR_LAUNCHED(ctx, "k_step_begin");
-      StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma};
-      StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma};
-      StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma};
+      StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma, 0.0};
+      StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma, 1.0};
+      StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma, 0.5};
       if ((rc = dispatch_stage(ctx, method, a1, w, st))) return rc;
       if ((rc = dispatch_stage(ctx, method, a2, w, st))) return rc;
       if ((rc = dispatch_stage(ctx, method, a3, w, st))) return rc;
@@ -794,9 +805,9 @@ template <int M>
 int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
   const dim3 blk(128);
   k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny + 5), blk, 0, st>>>(
-      a.u_stage, w.xl, w.xr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
+      a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
   k_normal<M, 2><<<dim3((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4), blk, 0, st>>>(
-      a.u_stage, w.yl, w.yr, a.nx, a.ny, a.bc, make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
+      a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
   k_flux<M, 1><<<dim3((a.nx + 1 + 31) / 32, (a.ny + 3) / 4), blk, 0, st>>>(
       w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P);
   k_flux<M, 2><<<dim3((a.nx + 127) / 128, a.ny + 1), blk, 0, st>>>(
@@ -828,7 +839,7 @@ extern "C" int wsr_euler2d_stage_noalloc(const double* u_stage, const double* u0
   Ws2d w = carve(scratch, nx, ny);
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
   if (cudaGetLastError() != cudaSuccess) return WSR_ERR_CUDA;
-  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma};
+  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma, 0.0};
   switch (method) {
     case WSR_METHOD_JS:
       return noalloc_launch<M_JS>(NoParams{}, a, w, st);

@@ -69,8 +69,9 @@ def prepare_closure(method: str, mlp_params, dev: int) -> N.Context:
 
 def stage(u_stage: torch.Tensor, u0: torch.Tensor, u_out: torch.Tensor, params: Params, dt: float, rk: int,
           method: str, boundary: str, mlp_params=None, flux: str = "hllc", opts: int = 0,
-          ws: Workspace | None = None) -> None:
-    """One SSPRK3 stage into the interior of u_out (launch_stage of the reference adapters)."""
+          ws: Workspace | None = None, boundary_time: float = 0.0) -> None:
+    """One SSPRK3 stage into the interior of u_out (launch_stage of the reference adapters); the
+    double-Mach boundary is evaluated at boundary_time."""
     for t in (u_stage, u0, u_out):
         _check_state(t, params)
     if boundary not in N.BC:
@@ -78,10 +79,11 @@ def stage(u_stage: torch.Tensor, u0: torch.Tensor, u_out: torch.Tensor, params: 
     dev = u_stage.device.index
     ctx = prepare_closure(method, mlp_params, dev)
     ws = ws or workspace(params.nx, params.ny, u_stage.device)
-    ctx.check(N.lib().wsr_euler2d_stage(
+    ctx.check(N.lib().wsr_euler2d_stage_at(
         ctx.handle, C.c_void_p(u_stage.data_ptr()), C.c_void_p(u0.data_ptr()), C.c_void_p(u_out.data_ptr()),
         params.nx, params.ny, params.dx, params.dy, params.gamma, float(dt), int(rk), N.METHOD[method],
-        N.BC[boundary], N.FLUX[flux], int(opts), C.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(dev)))
+        N.BC[boundary], N.FLUX[flux], int(opts), float(boundary_time), C.c_void_p(ws.ptr), ws.nbytes,
+        _stream_ptr(dev)))
 
 
 def max_speed(u: torch.Tensor, params: Params, ws: Workspace | None = None) -> float:

@@ -101,6 +101,34 @@ def isentropic_vortex(nx: int, ny: int, t: float = 0.0, quadrature: int = 5, gam
     return state
 
 
+def double_mach_primitive(x, y, t: float = 0.0):
+    """Double-Mach reflection: a Mach-10 shock through (1/6, 0) at 60 degrees to the wall, moving right;
+    post-shock (8, 8.25 cos 30, -8.25 sin 30, 116.5) left of it, (1.4, 0, 0, 1) right of it
+    (run_double_mach_compare.py:50-56)."""
+    r3 = np.sqrt(3.0)
+    left = np.asarray(x) < 1.0 / 6.0 + np.asarray(y) / r3 + 20.0 * t / r3
+    return (np.where(left, 8.0, 1.4), np.where(left, 8.25 * r3 * 0.5, 0.0), np.where(left, -8.25 * 0.5, 0.0),
+            np.where(left, 116.5, 1.0))
+
+
+def double_mach_state(nx: int, ny: int, quadrature: int = 15, gamma: float = 1.4, x_length: float = 4.0,
+                      y_length: float = 1.0, ghost: int = GHOST) -> np.ndarray:
+    """Padded initial state of the double-Mach problem on [0, 4] x [0, 1]: Gauss-Legendre cell averages
+    (quadrature^2 points) of every padded cell (run_double_mach_compare.py:69-88)."""
+    xi, wi = np.polynomial.legendre.leggauss(quadrature)
+    dx, dy = x_length / nx, y_length / ny
+    jj, ii = np.indices((ny + 2 * ghost, nx + 2 * ghost))
+    xc = (ii - ghost + 0.5) * dx
+    yc = (jj - ghost + 0.5) * dy
+    state = np.zeros((ny + 2 * ghost, nx + 2 * ghost, 4))
+    for sx, wx in zip(xi, wi):
+        x = xc + 0.5 * dx * float(sx)
+        for sy, wy in zip(xi, wi):
+            rho, u, v, p = double_mach_primitive(x, yc + 0.5 * dy * float(sy))
+            state += 0.25 * float(wx) * float(wy) * conserved_from_primitive(rho, u, v, p, gamma)
+    return state
+
+
 # ------------------------------------------------------------------------------------------------
 # 3D shock-bubble interaction
 # ------------------------------------------------------------------------------------------------

@@ -14,12 +14,10 @@ import torch
 from .. import euler2d as E
 from ..params import Params, interior_stats
 
-SUPPORTED_BOUNDARIES = ("transmissive", "periodic")
+SUPPORTED_BOUNDARIES = ("transmissive", "periodic", "double-mach")
 
 
 def _check_boundary(boundary: str) -> None:
-    if boundary == "double-mach":
-        raise NotImplementedError("the double-Mach boundary is not provided by this build")
     if boundary not in SUPPORTED_BOUNDARIES:
         raise ValueError(f"unsupported boundary {boundary!r}")
 
@@ -41,21 +39,20 @@ def allocate_forward(u0, params: Params, device: str) -> dict:
 
 
 def launch_stage(method: str, u_stage, u0, u_out, stage: dict, params: Params, dt: float, rk: int, device: str,
-                 mlp_params, boundary: str, eno_cutoff: bool = False, js_fallback: bool = False) -> None:
+                 mlp_params, boundary: str, eno_cutoff: bool = False, js_fallback: bool = False,
+                 boundary_time: float = 0.0) -> None:
     _check_boundary(boundary)
     opts = (E.N.OPT_ENO_CUTOFF if eno_cutoff else 0) | (E.N.OPT_JS_FALLBACK if js_fallback else 0)
     E.stage(u_stage, u0, u_out, params, dt, rk, method, boundary, mlp_params=mlp_params, opts=opts,
-            ws=stage["workspace"])
+            ws=stage["workspace"], boundary_time=boundary_time)
 
 
 def advance_step(method: str, arrays: dict, params: Params, dt: float, device: str, mlp_params,
-                 boundary: str) -> None:
-    launch_stage(method, arrays["u0"], arrays["u0"], arrays["u1"], arrays["s1"], params, dt, 1, device, mlp_params,
-                 boundary)
-    launch_stage(method, arrays["u1"], arrays["u0"], arrays["u2"], arrays["s2"], params, dt, 2, device, mlp_params,
-                 boundary)
-    launch_stage(method, arrays["u2"], arrays["u0"], arrays["u3"], arrays["s3"], params, dt, 3, device, mlp_params,
-                 boundary)
+                 boundary: str, t: float = 0.0) -> None:
+    """One SSPRK3 step from time t (the boundary times of the stages are t, t + dt and t + dt/2)."""
+    for rk, src, dst, bt in ((1, "u0", "u1", t), (2, "u1", "u2", t + dt), (3, "u2", "u3", t + 0.5 * dt)):
+        launch_stage(method, arrays[src], arrays["u0"], arrays[dst], arrays[f"s{rk}"], params, dt, rk, device,
+                     mlp_params, boundary, boundary_time=bt)
     arrays["u0"], arrays["u3"] = arrays["u3"], arrays["u0"]
 
 

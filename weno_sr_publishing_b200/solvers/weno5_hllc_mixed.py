@@ -12,8 +12,8 @@ def allocate_forward(u0, params, device):
 
 
 def launch_stage(u_stage, u0, u_out, stage, params, dt, rk, device, mlp_params, boundary, boundary_time=0.0):
-    del boundary_time
-    A.launch_stage(METHOD, u_stage, u0, u_out, stage, params, dt, rk, device, mlp_params, boundary)
+    A.launch_stage(METHOD, u_stage, u0, u_out, stage, params, dt, rk, device, mlp_params, boundary,
+                   boundary_time=boundary_time)
 
 
 def advance_step(arrays, params, dt, device, mlp_params, boundary):

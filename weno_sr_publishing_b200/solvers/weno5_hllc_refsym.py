@@ -13,8 +13,8 @@ def allocate_forward(initial, params, device):
 
 def launch_stage(u_stage, u0, u_out, stage, params, dt, rk, device, mlp_params, boundary, boundary_time=0.0,
                  eno_cutoff=False):
-    del boundary_time  # only the double-Mach boundary is time dependent
-    A.launch_stage(METHOD, u_stage, u0, u_out, stage, params, dt, rk, device, mlp_params, boundary, eno_cutoff)
+    A.launch_stage(METHOD, u_stage, u0, u_out, stage, params, dt, rk, device, mlp_params, boundary, eno_cutoff,
+                   boundary_time=boundary_time)
 
 
 def advance_step(arrays, params, dt, device, mlp_params, boundary):
