@@ -167,7 +167,9 @@ __device__ __forceinline__ void sr_head_weights(const StencilW& s, const Lin3& d
     return;
   }
   double a0 = d.d0 * (s.a0 * s.a0), a1 = d.d1 * (s.a1 * s.a1), a2 = d.d2 * (s.a2 * s.a2);
-  double inv = 1.0 / fmax(a0 + a1 + a2, 1.0e-300);  // 1e-300 is below the range of rcp64
+  // The reference divides by max(sum, 1e-300). Here a_k = 1/(3 r_k + 1e-12) >= 1/(3 + 1e-12) for ratios in
+  // [0, 1], so the sum lies in [1e-2, 1e24] and the guard never binds: one Newton-refined reciprocal.
+  double inv = rcp64(a0 + a1 + a2);
   w[0] = a0 * inv;
   w[1] = a1 * inv;
   w[2] = a2 * inv;
@@ -397,10 +399,42 @@ __device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigne
 __device__ __forceinline__ unsigned long long wpair(const float2& w) {
   return *reinterpret_cast<const unsigned long long*>(&w);
 }
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// swish of two lanes: z / (1 + e^-z) with e^-z = 2^(-z log2 e) and the reciprocal from the transcendental
+// unit (scalar), the scaling, the 1 + e and the final product as packed pairs.
 __device__ __forceinline__ unsigned long long swish2(unsigned long long z) {
+#if WSR_SWISH_MODE == 1
+  const float nl2e = -1.44269502f;  // -log2(e) rounded to float
+  float ta, tb;
+  upk2(mul2(z, pk2(nl2e, nl2e)), ta, tb);
+  float sa, sb;
+  upk2(add2(pk2(ex2_approx(ta), ex2_approx(tb)), pk2(1.0f, 1.0f)), sa, sb);
+  return mul2(z, pk2(rcp_approx(sa), rcp_approx(sb)));
+#else
   float a, b;
   upk2(z, a, b);
   return pk2(swish<float>(a), swish<float>(b));
+#endif
 }
 
 template <int NI, int NO>
@@ -512,7 +546,7 @@ __device__ __forceinline__ void sr_betas(const double s[5], const typename Closu
     // feature are formed in FP32 (the MLP consumes FP32 inputs; dmax >= 1e-13 here, so every value is
     // a normal float).
     const double d20 = s[0] - 2.0 * s[1] + s[2], d21 = s[1] - 2.0 * s[2] + s[3], d22 = s[2] - 2.0 * s[3] + s[4];
-    const float inv = __frcp_rn((float)se.dmax);
+    const float inv = rcp_nr((float)se.dmax);
     const float e = 1.0e-15f;
     float x[5];
     x[0] = (float)se.d0 * inv;
@@ -522,7 +556,7 @@ __device__ __forceinline__ void sr_betas(const double s[5], const typename Closu
     const float g1 = __fdividef(fabsf((float)d21), (float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
     const float g2 = __fdividef(fabsf((float)d22), (float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
     x[3] = fminf(1.0f, fmaxf(fmaxf(g0, g1), g2));
-    const float rel = (float)se.dmax * __frcp_rn((float)se.qscale);
+    const float rel = (float)se.dmax * rcp_nr((float)se.qscale);
     x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (__log10f(rel) + 4.0f) * 0.25f)));
     if constexpr (M == M_SRBF16) {
 #pragma unroll
@@ -552,7 +586,7 @@ __device__ __forceinline__ double sr_value(const double s[5], int head, double a
                                            Tally& tally) {
   double w[3], c[3];
   const Lin3 d = linear_weights(head);
-  if (!(isfinite(a0) && isfinite(a1) && isfinite(a2)) && (opts & OPT_JS_FALLBACK)) {
+  if ((opts & OPT_JS_FALLBACK) && !(isfinite(a0) && isfinite(a1) && isfinite(a2))) {
     js_head_weights(js_stencil(s), d, w);
     ++tally.fallbacks;
   } else {
