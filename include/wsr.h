@@ -72,6 +72,23 @@ const char *wsr_last_error(const wsr_ctx *ctx);
  * values rounded to their precision. */
 int wsr_closure_upload(wsr_ctx *ctx, int kind, const double *packed, int n);
 
+/* ---- 2D Euler WENO7-JS with Shu's fourth-order TVD Runge-Kutta (weno7_point_rk4_shu/point_rk4.py) ----
+ * State: padded [ny+8][nx+8][4] FP64 conserved (ghost width 4); characteristic WENO7 normal reconstruction,
+ * conservative two-point Gauss WENO7 transverse reconstruction, HLLC; boundary WSR_BC_TRANSMISSIVE or
+ * WSR_BC_PERIODIC (ghost cells are derived, never read from u). */
+size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny);
+/* One right-hand side into rhs (interior [ny][nx][4]): L(u) (reverse = 0) or the downwind operator L~(u)
+ * whose interface fluxes take the Gauss states in swapped order (reverse = 1); compute_rhs of
+ * point_rk4.py:435-511. */
+int wsr_euler2d_w7_rhs(wsr_ctx *ctx, const double *u, double *rhs, int nx, int ny, double dx, double dy,
+                       double gamma, int bc, int reverse, void *workspace, size_t workspace_bytes, void *stream);
+/* Time loop of run_from_initial (point_rk4.py:568-600) on u in place from time t_start: dt = cfl min(dx, dy)
+ * / max speed, the loop runs while t < t_end, a step that would pass t_end is shortened to reach it; at most
+ * max_steps steps. dts_host (capacity max_steps) receives each step's dt. */
+int wsr_euler2d_w7_run(wsr_ctx *ctx, double *u, int nx, int ny, double dx, double dy, double gamma, double cfl,
+                       double t_start, double t_end, int bc, int max_steps, double *dts_host, int *steps_out,
+                       double *t_out, void *workspace, size_t workspace_bytes, void *stream);
+
 /* Bytes of device workspace the 2D functions need for an nx x ny interior. */
 size_t wsr_euler2d_workspace_bytes(int nx, int ny);
 

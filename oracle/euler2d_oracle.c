@@ -832,3 +832,242 @@ void or_mlp_ratios_batch(const double *x, int n, int prec, const double *P64, co
         }
     }
 }
+
+/* ------------------------------------------------------------------------------------------ */
+/* 2D Euler WENO7-JS with Shu's fourth-order TVD RK (weno7_point_rk4_shu/point_rk4.py:150-616,       */
+/* weno7_external_clean/warp_weno7_ader4_helpers_classical_only.py:557-855, 2147-2202).              */
+/* Padded arrays [ny+8][nx+8][4], ghost width 4, filled in place before each right-hand side.        */
+/* ------------------------------------------------------------------------------------------ */
+#define G7 4
+
+static void w7_beta(const double *q, double *b) { /* classical_only.py:558-563 */
+    double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
+    b[3] = 2107.0*q3*q3 - 9402.0*q4*q3 + 7042.0*q3*q5 - 1854.0*q3*q6 - 17246.0*q4*q5 - 3882.0*q5*q6 + 11003.0*q4*q4 + 7043.0*q5*q5 + 547.0*q6*q6 + 4642.0*q4*q6;
+    b[2] = 267.0*q5*q5 - 1642.0*q5*q4 + 1602.0*q5*q3 - 494.0*q5*q2 - 2522.0*q3*q2 + 3443.0*q3*q3 + 547.0*q2*q2 - 5966.0*q4*q3 + 2843.0*q4*q4 + 1922.0*q4*q2;
+    b[1] = 267.0*q1*q1 - 494.0*q4*q1 - 1642.0*q2*q1 + 1602.0*q3*q1 - 5966.0*q3*q2 + 3443.0*q3*q3 - 2522.0*q4*q3 + 2843.0*q2*q2 + 547.0*q4*q4 + 1922.0*q4*q2;
+    b[0] = 2107.0*q3*q3 + 7042.0*q3*q1 - 1854.0*q3*q0 - 9402.0*q3*q2 - 17246.0*q2*q1 + 4642.0*q2*q0 + 547.0*q0*q0 - 3882.0*q1*q0 + 11003.0*q2*q2 + 7043.0*q1*q1;
+}
+
+static double w7_face_cand(int loc, double a, double b, double c, double d) { /* stencil_weno7, dorder 0 */
+    if (loc == 5) return 25.0/12.0*a - 23.0/12.0*b + 13.0/12.0*c - 1.0/4.0*d;
+    if (loc == 4) return 1.0/4.0*a + 13.0/12.0*b - 5.0/12.0*c + 1.0/12.0*d;
+    if (loc == 3) return -1.0/12.0*a + 7.0/12.0*b + 7.0/12.0*c - 1.0/12.0*d;
+    if (loc == 2) return 1.0/12.0*a - 5.0/12.0*b + 13.0/12.0*c + 1.0/4.0*d;
+    return -1.0/4.0*a + 13.0/12.0*b - 23.0/12.0*c + 25.0/12.0*d;
+}
+
+static double w7_gauss_cand(int loc, double a, double b, double c, double d) { /* stencil_weno7_2gauss */
+    double s = sqrt(3.0);
+    switch (loc) {
+    case 1: return (-11.0*s/216.0)*a + (17.0*s/72.0)*b - (35.0*s/72.0)*c + ((65.0*s + 216.0)/216.0)*d;
+    case 2: return (7.0*s/216.0)*a - (13.0*s/72.0)*b + ((7.0*s + 72.0)/72.0)*c + (11.0*s/216.0)*d;
+    case 3: return (-11.0*s/216.0)*a + ((72.0 - 7.0*s)/72.0)*b + (13.0*s/72.0)*c - (7.0*s/216.0)*d;
+    case 4: return ((216.0 - 65.0*s)/216.0)*a + (35.0*s/72.0)*b - (17.0*s/72.0)*c + (11.0*s/216.0)*d;
+    case 5: return (11.0*s/216.0)*a - (17.0*s/72.0)*b + (35.0*s/72.0)*c + ((216.0 - 65.0*s)/216.0)*d;
+    case 6: return (-7.0*s/216.0)*a + (13.0*s/72.0)*b + ((72.0 - 7.0*s)/72.0)*c - (11.0*s/216.0)*d;
+    case 7: return (11.0*s/216.0)*a + ((7.0*s + 72.0)/72.0)*b - (13.0*s/72.0)*c + (7.0*s/216.0)*d;
+    default: return ((65.0*s + 216.0)/216.0)*a - (35.0*s/72.0)*b + (17.0*s/72.0)*c - (11.0*s/216.0)*d;
+    }
+}
+
+static double w7_js_combine(const double *q, const double *s, const double *d) { /* weno7_lr_scalar */
+    double b[4];
+    w7_beta(q, b);
+    double r0 = 1.0 / (1.0e-6 + b[0]), r1 = 1.0 / (1.0e-6 + b[1]), r2 = 1.0 / (1.0e-6 + b[2]), r3 = 1.0 / (1.0e-6 + b[3]);
+    double a0 = d[0] * r0 * r0, a1 = d[1] * r1 * r1, a2 = d[2] * r2 * r2, a3 = d[3] * r3 * r3;
+    double asum = a0 + a1 + a2 + a3;
+    return (a0 * s[0] + a1 * s[1] + a2 * s[2] + a3 * s[3]) / asum;
+}
+
+double or_w7_face(const double *q, int lr) {
+    double s[4];
+    int o = lr == 1 ? 1 : 2;
+    for (int k = 0; k < 4; ++k) s[k] = w7_face_cand(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+    double d1[4] = {1.0/35.0, 12.0/35.0, 18.0/35.0, 4.0/35.0}, d2[4] = {4.0/35.0, 18.0/35.0, 12.0/35.0, 1.0/35.0};
+    return w7_js_combine(q, s, lr == 1 ? d1 : d2);
+}
+
+double or_w7_gauss(const double *q, int lr) { /* weno7_gauss_lr_scalar */
+    double r3 = sqrt(3.0), s[4], d[4];
+    int o = lr == 1 ? 1 : 5;
+    for (int k = 0; k < 4; ++k) s[k] = w7_gauss_cand(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+    if (lr == 1) {
+        d[0] = 59.0/880.0 - 5.0*r3/16632.0; d[1] = 381.0/880.0 - 587.0*r3/194040.0;
+        d[2] = 587.0*r3/194040.0 + 381.0/880.0; d[3] = 5.0*r3/16632.0 + 59.0/880.0;
+    } else {
+        d[0] = 5.0*r3/16632.0 + 59.0/880.0; d[1] = 587.0*r3/194040.0 + 381.0/880.0;
+        d[2] = 381.0/880.0 - 587.0*r3/194040.0; d[3] = 59.0/880.0 - 5.0*r3/16632.0;
+    }
+    return w7_js_combine(q, s, d);
+}
+
+/* weno7_lr_vec_characteristic: Roe(q3, q4) for lr = 1, Roe(q2, q3) for lr = 2 */
+static vec4 w7_char_face(const vec4 *q, int lr, int dir, double g) {
+    vec4 roe = lr == 2 ? roe_average_state(q[2], q[3], g) : roe_average_state(q[3], q[4], g);
+    vec4 c[7], cf;
+    for (int k = 0; k < 7; ++k) c[k] = con_to_char(q[k], roe, dir, g);
+    for (int f = 0; f < 4; ++f) {
+        double s[7];
+        for (int k = 0; k < 7; ++k) s[k] = c[k].v[f];
+        cf.v[f] = or_w7_face(s, lr);
+    }
+    return char_to_con(cf, roe, dir, g);
+}
+
+static void w7_fill_bc(double *u, int nx, int ny, int bc) { /* apply_(periodic_)boundary_kernel */
+    int nxt = nx + 2 * G7, nyt = ny + 2 * G7;
+    for (int j = 0; j < nyt; ++j)
+        for (int i = 0; i < nxt; ++i) {
+            int si = i, sj = j;
+            if (bc == OR_BC_PERIODIC) {
+                if (i < G7) si = i + nx; else if (i >= nx + G7) si = i - nx;
+                if (j < G7) sj = j + ny; else if (j >= ny + G7) sj = j - ny;
+            } else {
+                if (i < G7) si = G7; else if (i >= nx + G7) si = nx + G7 - 1;
+                if (j < G7) sj = G7; else if (j >= ny + G7) sj = ny + G7 - 1;
+            }
+            if (si != i || sj != j) store4(u, nxt, j, i, load4(u, nxt, sj, si));
+        }
+}
+
+/* compute_rhs (point_rk4.py:435-511): rhs interior [ny][nx][4]. src's ghost cells are filled in place.
+ * Returns 0, or -1 on allocation failure. */
+int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, double g, int bc, int reverse) {
+    int nxt = nx + 2 * G7, nyt = ny + 2 * G7;
+    size_t np = (size_t)nxt * nyt * 4;
+    double *xl = calloc(np, 8), *xr = calloc(np, 8), *yl = calloc(np, 8), *yr = calloc(np, 8);
+    double *f1 = calloc(np, 8), *f2 = calloc(np, 8), *h1 = calloc(np, 8), *h2 = calloc(np, 8);
+    int rc = 0;
+    if (!xl || !xr || !yl || !yr || !f1 || !f2 || !h1 || !h2) { rc = -1; goto done; }
+    w7_fill_bc(src, nx, ny, bc);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < ny + 8; ++j)
+        for (int i = 0; i < nx + 2; ++i) {
+            vec4 q[7];
+            for (int k = 0; k < 7; ++k) q[k] = load4(src, nxt, j, i + k);
+            store4(xl, nxt, j, i, w7_char_face(q, 2, 1, g));
+            store4(xr, nxt, j, i, w7_char_face(q, 1, 1, g));
+        }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx + 1; ++i)
+            for (int loca = 1; loca <= 2; ++loca) {
+                vec4 sl, sr;
+                for (int comp = 0; comp < 4; ++comp) {
+                    double a[7], b[7];
+                    for (int k = 0; k < 7; ++k) {
+                        a[k] = xr[((size_t)(j + 1 + k) * nxt + i) * 4 + comp];
+                        b[k] = xl[((size_t)(j + 1 + k) * nxt + i + 1) * 4 + comp];
+                    }
+                    sl.v[comp] = or_w7_gauss(a, loca);
+                    sr.v[comp] = or_w7_gauss(b, loca);
+                }
+                vec4 f = reverse ? or_hllc_flux(sr, sl, 1, g) : or_hllc_flux(sl, sr, 1, g);
+                store4(loca == 1 ? f1 : f2, nxt, j, i, f);
+            }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < ny + 2; ++j)
+        for (int i = 0; i < nx + 8; ++i) {
+            vec4 q[7];
+            for (int k = 0; k < 7; ++k) q[k] = load4(src, nxt, j + k, i);
+            store4(yl, nxt, j, i, w7_char_face(q, 2, 2, g));
+            store4(yr, nxt, j, i, w7_char_face(q, 1, 2, g));
+        }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < ny + 1; ++j)
+        for (int i = 0; i < nx; ++i)
+            for (int loca = 1; loca <= 2; ++loca) {
+                vec4 sl, sr;
+                for (int comp = 0; comp < 4; ++comp) {
+                    double a[7], b[7];
+                    for (int k = 0; k < 7; ++k) {
+                        a[k] = yr[((size_t)j * nxt + i + 1 + k) * 4 + comp];
+                        b[k] = yl[((size_t)(j + 1) * nxt + i + 1 + k) * 4 + comp];
+                    }
+                    sl.v[comp] = or_w7_gauss(a, loca);
+                    sr.v[comp] = or_w7_gauss(b, loca);
+                }
+                vec4 f = reverse ? or_hllc_flux(sr, sl, 2, g) : or_hllc_flux(sl, sr, 2, g);
+                store4(loca == 1 ? h1 : h2, nxt, j, i, f);
+            }
+    {
+        double inv_dx = 1.0 / dx, inv_dy = 1.0 / dy;
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i)
+                for (int comp = 0; comp < 4; ++comp) {
+#define A7(a, jy, ix) (a)[((size_t)(jy) * nxt + (ix)) * 4 + comp]
+                    double fxl = A7(f1, j, i) + A7(f2, j, i), fxr = A7(f1, j, i + 1) + A7(f2, j, i + 1);
+                    double fyb = A7(h1, j, i) + A7(h2, j, i), fyt = A7(h1, j + 1, i) + A7(h2, j + 1, i);
+#undef A7
+                    rhs[((size_t)j * nx + i) * 4 + comp] = -0.5 * (fxr - fxl) * inv_dx - 0.5 * (fyt - fyb) * inv_dy;
+                }
+    }
+done:
+    free(xl); free(xr); free(yl); free(yr); free(f1); free(f2); free(h1); free(h2);
+    return rc;
+}
+
+static double w7_max_speed(const double *u, int nx, int ny, double g) {
+    double m = 0.0;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const double *q = u + ((size_t)(j + G7) * (nx + 2 * G7) + i + G7) * 4;
+            double rho = fmax(q[0], 1.0e-15), vx = q[1] / rho, vy = q[2] / rho;
+            double p = fmax((g - 1.0) * (q[3] - 0.5 * rho * (vx * vx + vy * vy)), 1.0e-15);
+            double a = sqrt(g * p / rho), s = fmax(fabs(vx) + a, fabs(vy) + a);
+            if (s > m) m = s;
+        }
+    return m;
+}
+
+/* run_from_initial (point_rk4.py:568-600) with launch_shu_rk4_step (514-538): u is advanced in place.
+ * Returns the step count (dts receives up to max_dts values) or -1 on allocation failure. */
+int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double cfl, double t_end, int bc,
+              int max_steps, double *dts, int max_dts, double *t_out) {
+    size_t np = (size_t)(nx + 2 * G7) * (ny + 2 * G7) * 4, ni = (size_t)nx * ny * 4;
+    double *u1 = calloc(np, 8), *u2 = calloc(np, 8), *u3 = calloc(np, 8);
+    double *r0 = calloc(ni, 8), *rt0 = calloc(ni, 8), *r1 = calloc(ni, 8), *rt1 = calloc(ni, 8),
+           *r2 = calloc(ni, 8), *r3 = calloc(ni, 8);
+    int nxt = nx + 2 * G7, step = 0;
+    double t = 0.0;
+    if (!u1 || !u2 || !u3 || !r0 || !rt0 || !r1 || !rt1 || !r2 || !r3) { step = -1; goto done; }
+    while (t < t_end && step < max_steps) {
+        double ms = w7_max_speed(u, nx, ny, g);
+        double dt = ms < 1.0e-15 ? 1.0e10 : cfl * fmin(dx, dy) / ms;
+        if (t + dt > t_end) dt = t_end - t;
+        if (dt <= 0.0) break;
+#define IN7(a, j, i, c) (a)[((size_t)((j) + G7) * nxt + (i) + G7) * 4 + (c)]
+#define RI7(a, j, i, c) (a)[((size_t)(j) * nx + (i)) * 4 + (c)]
+        if (or_w7_rhs(u, r0, nx, ny, dx, dy, g, bc, 0)) { step = -1; goto done; }
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
+            IN7(u1, j, i, c) = IN7(u, j, i, c) + 0.5 * dt * RI7(r0, j, i, c);
+        if (or_w7_rhs(u, rt0, nx, ny, dx, dy, g, bc, 1) || or_w7_rhs(u1, r1, nx, ny, dx, dy, g, bc, 0)) {
+            step = -1; goto done;
+        }
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
+            IN7(u2, j, i, c) = 649.0/1600.0 * IN7(u, j, i, c) - 10890423.0/25193600.0 * dt * RI7(rt0, j, i, c)
+                               + 951.0/1600.0 * IN7(u1, j, i, c) + 5000.0/7873.0 * dt * RI7(r1, j, i, c);
+        if (or_w7_rhs(u1, rt1, nx, ny, dx, dy, g, bc, 1) || or_w7_rhs(u2, r2, nx, ny, dx, dy, g, bc, 0)) {
+            step = -1; goto done;
+        }
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
+            IN7(u3, j, i, c) = 53989.0/2500000.0 * IN7(u, j, i, c) - 102261.0/5000000.0 * dt * RI7(rt0, j, i, c)
+                               + 4806213.0/20000000.0 * IN7(u1, j, i, c) - 5121.0/20000.0 * dt * RI7(rt1, j, i, c)
+                               + 23619.0/32000.0 * IN7(u2, j, i, c) + 7873.0/10000.0 * dt * RI7(r2, j, i, c);
+        if (or_w7_rhs(u3, r3, nx, ny, dx, dy, g, bc, 0)) { step = -1; goto done; }
+        for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
+            IN7(u, j, i, c) = 1.0/5.0 * IN7(u, j, i, c) + 1.0/10.0 * dt * RI7(r0, j, i, c)
+                              + 6127.0/30000.0 * IN7(u1, j, i, c) + 1.0/6.0 * dt * RI7(r1, j, i, c)
+                              + 7873.0/30000.0 * IN7(u2, j, i, c) + 1.0/3.0 * IN7(u3, j, i, c)
+                              + 1.0/6.0 * dt * RI7(r3, j, i, c);
+#undef IN7
+#undef RI7
+        t += dt;
+        if (dts && step < max_dts) dts[step] = dt;
+        ++step;
+    }
+    if (t_out) *t_out = t;
+done:
+    free(u1); free(u2); free(u3); free(r0); free(rt0); free(r1); free(rt1); free(r2); free(r3);
+    return step;
+}

@@ -58,6 +58,15 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_euler3d_max_speed.restype = C.c_double
         lib.or_euler3d_max_speed.argtypes = [_dp, C.c_int, C.c_int, C.c_int]
         lib.or_hllc5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
+        lib.or_w7_face.restype = C.c_double
+        lib.or_w7_face.argtypes = [_dp, C.c_int]
+        lib.or_w7_gauss.restype = C.c_double
+        lib.or_w7_gauss.argtypes = [_dp, C.c_int]
+        lib.or_w7_rhs.restype = C.c_int
+        lib.or_w7_rhs.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
+        lib.or_w7_run.restype = C.c_int
+        lib.or_w7_run.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                  C.c_int, C.c_int, _dp, C.c_int, C.POINTER(C.c_double)]
         lib.or_evilin5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, _dp]
         _LIBS[name] = lib
     return _LIBS[name]
@@ -196,3 +205,40 @@ def evilin5(ul, ur, direction: int, dt_dx: float) -> np.ndarray:
     out = np.empty_like(ul)
     _lib().or_evilin5_batch(ul, ur, ul.shape[0], direction, dt_dx, out)
     return out
+
+
+# ------------------------------------------------------------------------------------------------
+# 2D Euler WENO7-JS with Shu RK4 (padded [ny+8][nx+8][4], ghost width 4)
+# ------------------------------------------------------------------------------------------------
+BC7 = {"transmissive": 0, "outflow": 0, "periodic": 1}
+
+
+def w7_face(q, lr: int) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    return np.array([_lib().or_w7_face(np.ascontiguousarray(r), lr) for r in q])
+
+
+def w7_gauss(q, lr: int) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    return np.array([_lib().or_w7_gauss(np.ascontiguousarray(r), lr) for r in q])
+
+
+def w7_rhs(u, nx, ny, dx, dy, bc="periodic", reverse=False, gamma=1.4) -> np.ndarray:
+    """L(u) (or L~(u)) on the interior [ny][nx][4]."""
+    src = np.array(u, dtype=np.float64, copy=True, order="C")
+    out = np.zeros((ny, nx, 4))
+    if _lib().or_w7_rhs(src, out, nx, ny, dx, dy, gamma, BC7[bc], int(bool(reverse))):
+        raise MemoryError("oracle allocation failed")
+    return out
+
+
+def w7_run(u, nx, ny, dx, dy, cfl, t_end, bc="periodic", max_steps=1_000_000, gamma=1.4, fast=False):
+    """run_from_initial of the WENO7 point RK4 path. Returns (final padded state, dts, steps, t)."""
+    out = np.array(u, dtype=np.float64, copy=True, order="C")
+    dts = np.zeros(min(max_steps, 1 << 20))
+    t = C.c_double(0.0)
+    steps = _lib(fast).or_w7_run(out, nx, ny, dx, dy, gamma, cfl, t_end, BC7[bc], max_steps, dts, dts.size,
+                                 C.byref(t))
+    if steps < 0:
+        raise MemoryError("oracle allocation failed")
+    return out, list(dts[:steps]), steps, t.value

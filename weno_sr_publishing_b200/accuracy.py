@@ -58,6 +58,29 @@ def vortex_run(n: int, method: str, mlp_params=None, device="cuda", quadrature: 
                         e0.elapsed_time(e1))
 
 
+def vortex7_run(n: int, device="cuda", quadrature: int = 15) -> VortexResult:
+    """WENO7-JS with Shu RK4 on the same vortex problem (the WENO7 rows of the reference's convergence table:
+    weno7_point_rk4_shu/point_rk4.py, HLLC, characteristic, [-10, 10]^2, CFL 0.4, t = 2)."""
+    from . import euler2d_w7 as E7  # noqa: PLC0415
+
+    p = E7.Params(nx=n, ny=n, cfl=CFL, t_end=T_END)
+    init = problems.vortex_point_rk4(n, n, 0.0, quadrature)
+    exact = problems.vortex_point_rk4(n, n, T_END, quadrature)
+    dev = torch.device(device)
+    u = torch.as_tensor(init, device=dev).contiguous()
+    ws = E7.workspace(n, n, dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    res = E7.run(u, p, "periodic", ws=ws)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    err = u.cpu().numpy()[4:-4, 4:-4, 0] - exact[4:-4, 4:-4, 0]
+    return VortexResult(n, "w7_js", float(np.mean(np.abs(err))), float(np.sqrt(np.mean(err * err))), res.steps,
+                        e0.elapsed_time(e1))
+
+
 def loglog_n_for_error(points: list[VortexResult], target: float) -> float:
     """Resolution N at which the method's L1 equals `target`, interpolating log L1 linearly in log N between
     the two bracketing points (extrapolating from the nearest pair outside the range)."""

@@ -1,0 +1,327 @@
+// 2D Euler WENO7-JS with Shu's fourth-order TVD Runge-Kutta (L and the downwind operator L~), sm_100a.
+//
+// Reference: weno7_point_rk4_shu/point_rk4.py:150-538 with the classical WENO7 helpers of
+// weno7_external_clean/warp_weno7_ader4_helpers_classical_only.py:557-855 (betas, face and two-point Gauss
+// candidate stencils, optimal weights, characteristic face reconstruction). Layout: padded row-major
+// u[ny+8][nx+8][4] FP64 conserved, ghost width 4; ghost cells are not materialised (stencil loads map a padded
+// index to its source cell, as apply_boundary_kernel / apply_periodic_boundary_kernel write them).
+//
+// One right-hand side L(u) (or L~(u), whose interface fluxes take the two Gauss states in swapped order):
+//   k7_normal<DIR=1>, <DIR=2>  one thread per face: Roe average of the two cells next to it, the 8 cells
+//                              around it projected once, lr=1 of the left cell and lr=2 of the right cell
+//   k7_flux<DIR=1>, <DIR=2>    one thread per face: 8 transverse WENO7 stencils on the face values, both
+//                              Gauss points from one set of betas, HLLC at each point, f1 + f2
+//   k7_rhs                     -1/2 (f_{i+1} - f_i)/dx - 1/2 (g_{j+1} - g_j)/dy on the interior
+// Six right-hand sides and four combinations make one Shu RK4 step (point_rk4.py:514-538).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "euler2d.cuh"
+
+namespace wsr {
+namespace w7 {
+
+constexpr int kG = 4;  // ghost width
+constexpr int kBlock7 = 128;
+
+__device__ __forceinline__ int map7(int p, int n, int bc) {
+  if (bc == BC_TRANSMISSIVE) return p < kG ? kG : (p >= n + kG ? n + kG - 1 : p);
+  return p < kG ? p + n : (p >= n + kG ? p - n : p);
+}
+
+// Smoothness indicators of the four 4-point substencils (warp_weno7_ader4_helpers_classical_only.py:558-563),
+// each polynomial in the reference's term order.
+__device__ __forceinline__ void w7_beta(const double q[7], double b[4]) {
+  const double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
+  b[3] = 2107.0 * q3 * q3 - 9402.0 * q4 * q3 + 7042.0 * q3 * q5 - 1854.0 * q3 * q6 - 17246.0 * q4 * q5 -
+         3882.0 * q5 * q6 + 11003.0 * q4 * q4 + 7043.0 * q5 * q5 + 547.0 * q6 * q6 + 4642.0 * q4 * q6;
+  b[2] = 267.0 * q5 * q5 - 1642.0 * q5 * q4 + 1602.0 * q5 * q3 - 494.0 * q5 * q2 - 2522.0 * q3 * q2 +
+         3443.0 * q3 * q3 + 547.0 * q2 * q2 - 5966.0 * q4 * q3 + 2843.0 * q4 * q4 + 1922.0 * q4 * q2;
+  b[1] = 267.0 * q1 * q1 - 494.0 * q4 * q1 - 1642.0 * q2 * q1 + 1602.0 * q3 * q1 - 5966.0 * q3 * q2 +
+         3443.0 * q3 * q3 - 2522.0 * q4 * q3 + 2843.0 * q2 * q2 + 547.0 * q4 * q4 + 1922.0 * q4 * q2;
+  b[0] = 2107.0 * q3 * q3 + 7042.0 * q3 * q1 - 1854.0 * q3 * q0 - 9402.0 * q3 * q2 - 17246.0 * q2 * q1 +
+         4642.0 * q2 * q0 + 547.0 * q0 * q0 - 3882.0 * q1 * q0 + 11003.0 * q2 * q2 + 7043.0 * q1 * q1;
+}
+
+// Face candidates (stencil_weno7, dorder 0): location 1..5, four points each.
+__device__ __forceinline__ double w7_face(int loc, double a, double b, double c, double d) {
+  switch (loc) {
+    case 5:
+      return 25.0 / 12.0 * a - 23.0 / 12.0 * b + 13.0 / 12.0 * c - 1.0 / 4.0 * d;
+    case 4:
+      return 1.0 / 4.0 * a + 13.0 / 12.0 * b - 5.0 / 12.0 * c + 1.0 / 12.0 * d;
+    case 3:
+      return -1.0 / 12.0 * a + 7.0 / 12.0 * b + 7.0 / 12.0 * c - 1.0 / 12.0 * d;
+    case 2:
+      return 1.0 / 12.0 * a - 5.0 / 12.0 * b + 13.0 / 12.0 * c + 1.0 / 4.0 * d;
+    default:
+      return -1.0 / 4.0 * a + 13.0 / 12.0 * b - 23.0 / 12.0 * c + 25.0 / 12.0 * d;
+  }
+}
+
+// Two-point Gauss candidates (stencil_weno7_2gauss, dorder 0): locations 1..4 for the first Gauss point,
+// 5..8 for the second, with s = sqrt(3) correctly rounded.
+constexpr double kS3 = 1.7320508075688772;
+__device__ __forceinline__ double w7_gauss(int loc, double a, double b, double c, double d) {
+  constexpr double s = kS3;
+  switch (loc) {
+    case 1:
+      return (-11.0 * s / 216.0) * a + (17.0 * s / 72.0) * b - (35.0 * s / 72.0) * c + ((65.0 * s + 216.0) / 216.0) * d;
+    case 2:
+      return (7.0 * s / 216.0) * a - (13.0 * s / 72.0) * b + ((7.0 * s + 72.0) / 72.0) * c + (11.0 * s / 216.0) * d;
+    case 3:
+      return (-11.0 * s / 216.0) * a + ((72.0 - 7.0 * s) / 72.0) * b + (13.0 * s / 72.0) * c - (7.0 * s / 216.0) * d;
+    case 4:
+      return ((216.0 - 65.0 * s) / 216.0) * a + (35.0 * s / 72.0) * b - (17.0 * s / 72.0) * c + (11.0 * s / 216.0) * d;
+    case 5:
+      return (11.0 * s / 216.0) * a - (17.0 * s / 72.0) * b + (35.0 * s / 72.0) * c + ((216.0 - 65.0 * s) / 216.0) * d;
+    case 6:
+      return (-7.0 * s / 216.0) * a + (13.0 * s / 72.0) * b + ((72.0 - 7.0 * s) / 72.0) * c - (11.0 * s / 216.0) * d;
+    case 7:
+      return (11.0 * s / 216.0) * a + ((7.0 * s + 72.0) / 72.0) * b - (13.0 * s / 72.0) * c + (7.0 * s / 216.0) * d;
+    default:
+      return ((65.0 * s + 216.0) / 216.0) * a - (35.0 * s / 72.0) * b + (17.0 * s / 72.0) * c - (11.0 * s / 216.0) * d;
+  }
+}
+
+// JS combination (weno7_lr_scalar): a_k = d_k / (1e-6 + beta_k)^2, value = sum a_k s_k / sum a_k.
+__device__ __forceinline__ double w7_combine(const double r[4], const double d[4], const double s[4]) {
+  const double a0 = d[0] * r[0] * r[0], a1 = d[1] * r[1] * r[1], a2 = d[2] * r[2] * r[2], a3 = d[3] * r[3] * r[3];
+  return (a0 * s[0] + a1 * s[1] + a2 * s[2] + a3 * s[3]) * rcp64(a0 + a1 + a2 + a3);
+}
+
+__device__ __forceinline__ void w7_rcp_betas(const double q[7], double r[4]) {
+  double b[4];
+  w7_beta(q, b);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r[k] = rcp64(1.0e-6 + b[k]);
+}
+
+// Face value: lr = 1 (right face of the centre cell q[3]) or lr = 2 (left face).
+__device__ __forceinline__ double w7_js_face(const double q[7], int lr) {
+  double r[4], s[4];
+  w7_rcp_betas(q, r);
+  const int o = lr == 1 ? 1 : 2;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_face(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  const double d1[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
+  const double d2[4] = {4.0 / 35.0, 18.0 / 35.0, 12.0 / 35.0, 1.0 / 35.0};
+  return w7_combine(r, lr == 1 ? d1 : d2, s);
+}
+
+// Both Gauss-point values of one transverse stencil from one set of betas (weno7_gauss_lr_scalar, lr 1, 2).
+__device__ __forceinline__ void w7_js_gauss(const double q[7], double& g1, double& g2) {
+  double r[4], s[4];
+  w7_rcp_betas(q, r);
+  constexpr double s3 = kS3;
+  const double e0 = 59.0 / 880.0, e1 = 5.0 * s3 / 16632.0, f0 = 381.0 / 880.0, f1 = 587.0 * s3 / 194040.0;
+  const double da[4] = {e0 - e1, f0 - f1, f1 + f0, e1 + e0};
+  const double db[4] = {e1 + e0, f1 + f0, f0 - f1, e0 - e1};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_gauss(1 + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  g1 = w7_combine(r, da, s);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_gauss(5 + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  g2 = w7_combine(r, db, s);
+}
+
+// Normal reconstruction, one thread per face.
+// DIR=1: face (r, c), r in [1, ny+7), c in [0, nx]: padded row r, cells c..c+7; face between cells c+3 and
+//        c+4. Writes out_r[r][c] (lr=1 of cell c+3) and out_l[r][c+1] (lr=2 of cell c+4); arrays [ny+8][nx+2].
+// DIR=2: face (r, c), r in [0, ny], c in [1, nx+7): padded column c, cells r..r+7; writes out_r[r][c] and
+//        out_l[r+1][c]; arrays [ny+2][nx+8].
+template <int DIR>
+__global__ void __launch_bounds__(kBlock7, 4) k7_normal(const double* __restrict__ u, double* __restrict__ out_l,
+                                                       double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
+                                                       const StepCtl* __restrict__ ctl) {
+  __shared__ double s_ch[4][8][kBlock7];
+  if (ctl->done) return;
+  const int t = threadIdx.x;
+  const int c = DIR == 1 ? blockIdx.x * kBlock7 + t : blockIdx.x * 32 + (t & 31);
+  const int r = DIR == 1 ? blockIdx.y : blockIdx.y * 4 + (t >> 5);
+  const int nxt = nx + 2 * kG;
+  const bool active = DIR == 1 ? (r >= 1 && r < ny + 7 && c <= nx) : (r <= ny && c >= 1 && c < nx + 7);
+  if (!active) return;  // no block-wide synchronisation below: each thread uses its own shared slots
+  auto cell = [&](int k) {
+    const int pj = DIR == 1 ? r : r + k;
+    const int pi = DIR == 1 ? c + k : c;
+    return load_cell(u, nxt, map7(pj, ny, bc), map7(pi, nx, bc));
+  };
+  const RoeJ J = roe_jacobian(cell(3), cell(4), gas);
+  {
+    const CharL L = char_left<DIR>(J, gas);
+#pragma unroll 1
+    for (int k = 0; k < 8; ++k) {
+      const d4 qk = cell(k);
+#pragma unroll
+      for (int f = 0; f < 4; ++f) s_ch[f][k][t] = project<DIR>(L, f, qk);
+    }
+  }
+#pragma unroll 1
+  for (int side = 0; side < 2; ++side) {
+    double cf[4];
+#pragma unroll 1
+    for (int f = 0; f < 4; ++f) {
+      double q[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][t];
+      cf[f] = w7_js_face(q, side == 0 ? 1 : 2);
+    }
+    const d4 face = char_to_con<DIR>(cf, J);
+    const size_t idx = DIR == 1 ? (size_t)r * (nx + 2) + c + side : (size_t)(r + side) * (nx + 8) + c;
+    store_cell(side == 0 ? out_r : out_l, idx, face);
+  }
+}
+
+// Transverse reconstruction and flux, one thread per face.
+// x faces (j, i), j in [0, ny), i in [0, nx]: u_L from xr[j+1..j+7][i], u_R from xl[j+1..j+7][i+1].
+// y faces (j, i), j in [0, ny], i in [0, nx): u_L from yr[j][i+1..i+7], u_R from yl[j+1][i+1..i+7].
+// Output f[j][i] = F(g1) + F(g2) (unscaled); with `reverse` the Riemann problem takes (u_R, u_L).
+template <int DIR>
+__global__ void __launch_bounds__(kBlock7, 4) k7_flux(const double* __restrict__ fl, const double* __restrict__ fr,
+                                                     double* __restrict__ fout, int nx, int ny, Gas gas, int reverse,
+                                                     const StepCtl* __restrict__ ctl) {
+  if (ctl->done) return;
+  const int t = threadIdx.x;
+  const int i = DIR == 1 ? blockIdx.x * 32 + (t & 31) : blockIdx.x * kBlock7 + t;
+  const int j = DIR == 1 ? blockIdx.y * 4 + (t >> 5) : blockIdx.y;
+  const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
+  if (i >= nfx || j >= nfy) return;
+  d4 l1, l2, r1, r2;
+#pragma unroll 1
+  for (int n = 0; n < 8; ++n) {
+    const int comp = n >> 1, side = n & 1;  // side 0: u_L from fr, side 1: u_R from fl
+    double q[7];
+    const double* src = side == 0 ? fr : fl;
+    if (DIR == 1) {
+      const int ncols = nx + 2, col = side == 0 ? i : i + 1;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) q[k] = __ldg(src + ((size_t)(j + 1 + k) * ncols + col) * 4 + comp);
+    } else {
+      const int ncols = nx + 8, row = side == 0 ? j : j + 1;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) q[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
+    }
+    double g1, g2;
+    w7_js_gauss(q, g1, g2);
+    if (side == 0) {
+      l1.v[comp] = g1;
+      l2.v[comp] = g2;
+    } else {
+      r1.v[comp] = g1;
+      r2.v[comp] = g2;
+    }
+  }
+  const d4 f1 = reverse ? hllc_flux<DIR>(r1, l1, gas) : hllc_flux<DIR>(l1, r1, gas);
+  const d4 f2 = reverse ? hllc_flux<DIR>(r2, l2, gas) : hllc_flux<DIR>(l2, r2, gas);
+  d4 o;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] + f2.v[k];
+  store_cell(fout, (size_t)j * nfx + i, o);
+}
+
+// rhs[j][i] = -1/2 (f[j][i+1] - f[j][i]) / dx - 1/2 (g[j+1][i] - g[j][i]) / dy (point_rk4.py:290-312).
+__global__ void __launch_bounds__(256) k7_rhs(const double* __restrict__ fx, const double* __restrict__ fy,
+                                              double* __restrict__ rhs, int nx, int ny, double inv_dx, double inv_dy,
+                                              const StepCtl* __restrict__ ctl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (ctl->done || i >= nx) return;
+  const d4 fxl = load_cell(fx, nx + 1, j, i), fxr = load_cell(fx, nx + 1, j, i + 1);
+  const d4 fyb = load_cell(fy, nx, j, i), fyt = load_cell(fy, nx, j + 1, i);
+  d4 o;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) o.v[k] = -0.5 * (fxr.v[k] - fxl.v[k]) * inv_dx - 0.5 * (fyt.v[k] - fyb.v[k]) * inv_dy;
+  store_cell(rhs, (size_t)j * nx + i, o);
+}
+
+// Shu RK4 combinations on the interior (point_rk4.py:315-403), in the reference's coefficient and operand
+// order; rhs arrays are interior-only [ny][nx][4], states padded.
+struct ShuArgs {
+  const double* u;
+  const double* u1;
+  const double* u2;
+  const double* u3;
+  const double* rhs0;
+  const double* rhs_t0;
+  const double* rhs1;
+  const double* rhs_t1;
+  const double* rhs2;
+  const double* rhs3;
+  double* out;
+};
+
+template <int S>
+__global__ void __launch_bounds__(256) k7_shu(ShuArgs a, int nx, int ny, const StepCtl* __restrict__ ctl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (ctl->done || i >= nx) return;
+  const double dt = ctl->dt;
+  const int nxt = nx + 2 * kG;
+  const size_t p = (size_t)(j + kG) * nxt + (i + kG);
+  const d4 u0 = load_cell(a.u, nxt, j + kG, i + kG);
+  d4 o;
+  if constexpr (S == 1) {
+    const d4 r0 = load_cell(a.rhs0, nx, j, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o.v[k] = u0.v[k] + 0.5 * dt * r0.v[k];
+  } else if constexpr (S == 2) {
+    const d4 rt0 = load_cell(a.rhs_t0, nx, j, i), v1 = load_cell(a.u1, nxt, j + kG, i + kG);
+    const d4 r1 = load_cell(a.rhs1, nx, j, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      o.v[k] = 649.0 / 1600.0 * u0.v[k] - 10890423.0 / 25193600.0 * dt * rt0.v[k] + 951.0 / 1600.0 * v1.v[k] +
+               5000.0 / 7873.0 * dt * r1.v[k];
+  } else if constexpr (S == 3) {
+    const d4 rt0 = load_cell(a.rhs_t0, nx, j, i), v1 = load_cell(a.u1, nxt, j + kG, i + kG);
+    const d4 rt1 = load_cell(a.rhs_t1, nx, j, i), v2 = load_cell(a.u2, nxt, j + kG, i + kG);
+    const d4 r2 = load_cell(a.rhs2, nx, j, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      o.v[k] = 53989.0 / 2500000.0 * u0.v[k] - 102261.0 / 5000000.0 * dt * rt0.v[k] +
+               4806213.0 / 20000000.0 * v1.v[k] - 5121.0 / 20000.0 * dt * rt1.v[k] + 23619.0 / 32000.0 * v2.v[k] +
+               7873.0 / 10000.0 * dt * r2.v[k];
+  } else {
+    const d4 r0 = load_cell(a.rhs0, nx, j, i), v1 = load_cell(a.u1, nxt, j + kG, i + kG);
+    const d4 r1 = load_cell(a.rhs1, nx, j, i), v2 = load_cell(a.u2, nxt, j + kG, i + kG);
+    const d4 v3 = load_cell(a.u3, nxt, j + kG, i + kG), r3 = load_cell(a.rhs3, nx, j, i);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      o.v[k] = 1.0 / 5.0 * u0.v[k] + 1.0 / 10.0 * dt * r0.v[k] + 6127.0 / 30000.0 * v1.v[k] +
+               1.0 / 6.0 * dt * r1.v[k] + 7873.0 / 30000.0 * v2.v[k] + 1.0 / 3.0 * v3.v[k] + 1.0 / 6.0 * dt * r3.v[k];
+  }
+  store_cell(a.out, p, o);
+}
+
+// Max wave speed of the interior (compute_max_speed_kernel, classical_only.py:2147-2159).
+__global__ void __launch_bounds__(256) k7_max_speed(const double* __restrict__ u, int nx, int ny, double g,
+                                                    StepCtl* __restrict__ ctl) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (ctl->done) return;
+  unsigned long long sb = 0;
+  if (i < nx) sb = speed_bits(load_cell(u, nx + 2 * kG, j + kG, i + kG), g);
+  block_max_to(sb, &ctl->max_speed_bits);
+}
+
+// dt of the next step (point_rk4.py:136-147, 568-590): cfl min(dx, dy) / max speed (1e10 below 1e-15),
+// the loop runs while t < t_end and a step that would pass t_end is shortened to reach it. Resets the
+// max-speed slot for the next step. `ring` records each step's dt (slot steps mod ring_len).
+__global__ void k7_step_begin(StepCtl* ctl, double* ring, int ring_len) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (ctl->done) return;
+  if (!(ctl->t < ctl->t_end) || ctl->steps >= ctl->max_steps) {
+    ctl->done = 1;
+    return;
+  }
+  const double ms = __longlong_as_double((long long)ctl->max_speed_bits);
+  double dt = ms < 1.0e-15 ? 1.0e10 : ctl->cfl * ctl->hmin / ms;
+  if (ctl->t + dt > ctl->t_end) dt = ctl->t_end - ctl->t;
+  if (!(dt > 0.0)) {
+    ctl->done = 1;
+    return;
+  }
+  ctl->dt = dt;
+  ctl->max_speed_bits = 0ull;
+  ring[ctl->steps % ring_len] = dt;
+}
+
+}  // namespace w7
+}  // namespace wsr

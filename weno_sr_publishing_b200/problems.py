@@ -101,6 +101,35 @@ def isentropic_vortex(nx: int, ny: int, t: float = 0.0, quadrature: int = 5, gam
     return state
 
 
+def vortex_point_rk4(nx: int, ny: int, t: float = 0.0, quadrature: int = 15, gamma: float = 1.4,
+                     x_min: float = -10.0, x_max: float = 10.0, y_min: float = -10.0, y_max: float = 10.0,
+                     ghost: int = 4) -> np.ndarray:
+    """Cell averages (quadrature^2 Gauss-Legendre points) of the periodic isentropic vortex of the WENO7
+    point-value path (weno7_point_rk4_shu/point_rk4.py:77-117): strength 5, mean flow (1, 1), period 20,
+    centre displaced by (t, t) with the nearest periodic image, on the padded [ny+2g][nx+2g] grid."""
+    xi, wi = np.polynomial.legendre.leggauss(quadrature)
+    dx, dy = (x_max - x_min) / nx, (y_max - y_min) / ny
+    jj, ii = np.indices((ny + 2 * ghost, nx + 2 * ghost))
+    xc = x_min + (ii - ghost + 0.5) * dx
+    yc = y_min + (jj - ghost + 0.5) * dy
+    length, beta = 20.0, 5.0
+    out = np.zeros((ny + 2 * ghost, nx + 2 * ghost, 4))
+    for sx, wx in zip(xi, wi):
+        x = xc + 0.5 * dx * float(sx)
+        for sy, wy in zip(xi, wi):
+            y = yc + 0.5 * dy * float(sy)
+            ddx = x - t - length * np.round((x - t) / length)
+            ddy = y - t - length * np.round((y - t) / length)
+            r2 = ddx * ddx + ddy * ddy
+            d_t = -((gamma - 1.0) * beta * beta) / (8.0 * gamma * np.pi * np.pi) * np.exp(1.0 - r2)
+            rho = 1.0 + (np.power(1.0 + d_t, 1.0 / (gamma - 1.0)) - 1.0)
+            p = 1.0 + (np.power(1.0 + d_t, gamma / (gamma - 1.0)) - 1.0)
+            f = beta / (2.0 * np.pi) * np.exp(0.5 * (1.0 - r2))
+            u, v = 1.0 - f * ddy, 1.0 + f * ddx
+            out += 0.25 * float(wx) * float(wy) * conserved_from_primitive(rho, u, v, p, gamma)
+    return out
+
+
 def double_mach_primitive(x, y, t: float = 0.0):
     """Double-Mach reflection: a Mach-10 shock through (1/6, 0) at 60 degrees to the wall, moving right;
     post-shock (8, 8.25 cos 30, -8.25 sin 30, 116.5) left of it, (1.4, 0, 0, 1) right of it

@@ -27,6 +27,7 @@ import numpy as np
 import torch
 
 from . import euler2d as E
+from . import euler2d_w7 as E7
 from .params import Params
 
 Primitive = tuple[float, float, float]
@@ -199,10 +200,10 @@ def tube_params(tube: ShockTube, gamma: float = 1.4) -> Params:
                   t_end=tube.t_end, gamma=gamma)
 
 
-def tube_initial_state(tube: ShockTube, gamma: float = 1.4) -> np.ndarray:
-    """Padded [ny+6][nx+6][4] state: exact cell averages of the initial step (a cell cut by x0 gets the
+def tube_initial_state(tube: ShockTube, gamma: float = 1.4, ghost: int = 3) -> np.ndarray:
+    """Padded [ny+2g][nx+2g][4] state: exact cell averages of the initial step (a cell cut by x0 gets the
     length-weighted mix, run_shock_tube_benchmark.py:56-77), the same on every row."""
-    g = 3
+    g = ghost
     dx = (tube.x_max - tube.x_min) / tube.nx
     xl = tube.x_min + (np.arange(tube.nx + 2 * g) - g) * dx
     left_len = np.clip(np.minimum(xl + dx, tube.x0) - xl, 0.0, dx)
@@ -240,10 +241,31 @@ def _run_padded(init: np.ndarray, p: Params, t_end: float, method: str, mlp_para
     return final[3:3 + p.ny, 3:3 + p.nx], res, e0.elapsed_time(e1)
 
 
+def _run_w7(tube: ShockTube, gamma: float, device) -> tuple:
+    """WENO7-JS with Shu RK4 on the tube, ghost width 4 (the WENO7 runs of run_sod.py:86-99 and
+    run_shock_tube_benchmark.py:127-177)."""
+    dx = (tube.x_max - tube.x_min) / tube.nx
+    p = E7.Params(nx=tube.nx, ny=tube.ny, x_min=tube.x_min, x_max=tube.x_max, y_min=0.0, y_max=tube.ny * dx,
+                  gamma=gamma, cfl=tube.cfl, t_end=tube.t_end)
+    dev = torch.device(device)
+    u = torch.as_tensor(tube_initial_state(tube, gamma, ghost=4), device=dev).contiguous()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = E7.run(u, p, "transmissive")
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return u.cpu().numpy()[4:4 + tube.ny, 4:4 + tube.nx], res, e0.elapsed_time(e1)
+
+
 def shock_tube_run(tube: ShockTube, method: str, mlp_params=None, device="cuda", gamma: float = 1.4) -> dict:
-    """Run the tube on the GPU to t_end and compare the y-averaged solution with the exact cell averages."""
+    """Run the tube on the GPU to t_end and compare the y-averaged solution with the exact cell averages.
+    method: a WENO5 method of the 2D path ("js", "z", "sr_f64", ...) or "w7_js" (WENO7-JS, Shu RK4)."""
     p = tube_params(tube, gamma)
-    state, res, ms = _run_padded(tube_initial_state(tube, gamma), p, tube.t_end, method, mlp_params, device)
+    if method == "w7_js":
+        state, res, ms = _run_w7(tube, gamma, device)
+    else:
+        state, res, ms = _run_padded(tube_initial_state(tube, gamma), p, tube.t_end, method, mlp_params, device)
     conserved = state.mean(axis=0)
     x = tube.x_min + (np.arange(tube.nx) + 0.5) * p.dx
     exact = cell_averages(x, p.dx, tube.t_end, tube.x0, tube.left, tube.right, gamma, 15, tube.split_exact)
