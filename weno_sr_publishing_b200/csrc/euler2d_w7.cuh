@@ -30,17 +30,50 @@ __device__ __forceinline__ int map7(int p, int n, int bc) {
 }
 
 // Smoothness indicators of the four 4-point substencils (warp_weno7_ader4_helpers_classical_only.py:558-563),
-// each polynomial in the reference's term order.
+// each polynomial in the reference's term order and rounded operation by operation (no contraction): the
+// unnormalised coefficients (up to 17246) cancel to small betas on smooth data, where a fused multiply-add
+// would move the weights of the near-linear stencils.
+__device__ __forceinline__ double w7_t(double c, double a, double b) { return __dmul_rn(__dmul_rn(c, a), b); }
+
 __device__ __forceinline__ void w7_beta(const double q[7], double b[4]) {
   const double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
-  b[3] = 2107.0 * q3 * q3 - 9402.0 * q4 * q3 + 7042.0 * q3 * q5 - 1854.0 * q3 * q6 - 17246.0 * q4 * q5 -
-         3882.0 * q5 * q6 + 11003.0 * q4 * q4 + 7043.0 * q5 * q5 + 547.0 * q6 * q6 + 4642.0 * q4 * q6;
-  b[2] = 267.0 * q5 * q5 - 1642.0 * q5 * q4 + 1602.0 * q5 * q3 - 494.0 * q5 * q2 - 2522.0 * q3 * q2 +
-         3443.0 * q3 * q3 + 547.0 * q2 * q2 - 5966.0 * q4 * q3 + 2843.0 * q4 * q4 + 1922.0 * q4 * q2;
-  b[1] = 267.0 * q1 * q1 - 494.0 * q4 * q1 - 1642.0 * q2 * q1 + 1602.0 * q3 * q1 - 5966.0 * q3 * q2 +
-         3443.0 * q3 * q3 - 2522.0 * q4 * q3 + 2843.0 * q2 * q2 + 547.0 * q4 * q4 + 1922.0 * q4 * q2;
-  b[0] = 2107.0 * q3 * q3 + 7042.0 * q3 * q1 - 1854.0 * q3 * q0 - 9402.0 * q3 * q2 - 17246.0 * q2 * q1 +
-         4642.0 * q2 * q0 + 547.0 * q0 * q0 - 3882.0 * q1 * q0 + 11003.0 * q2 * q2 + 7043.0 * q1 * q1;
+  double s;
+  s = __dsub_rn(w7_t(2107.0, q3, q3), w7_t(9402.0, q4, q3));
+  s = __dadd_rn(s, w7_t(7042.0, q3, q5));
+  s = __dsub_rn(s, w7_t(1854.0, q3, q6));
+  s = __dsub_rn(s, w7_t(17246.0, q4, q5));
+  s = __dsub_rn(s, w7_t(3882.0, q5, q6));
+  s = __dadd_rn(s, w7_t(11003.0, q4, q4));
+  s = __dadd_rn(s, w7_t(7043.0, q5, q5));
+  s = __dadd_rn(s, w7_t(547.0, q6, q6));
+  b[3] = __dadd_rn(s, w7_t(4642.0, q4, q6));
+  s = __dsub_rn(w7_t(267.0, q5, q5), w7_t(1642.0, q5, q4));
+  s = __dadd_rn(s, w7_t(1602.0, q5, q3));
+  s = __dsub_rn(s, w7_t(494.0, q5, q2));
+  s = __dsub_rn(s, w7_t(2522.0, q3, q2));
+  s = __dadd_rn(s, w7_t(3443.0, q3, q3));
+  s = __dadd_rn(s, w7_t(547.0, q2, q2));
+  s = __dsub_rn(s, w7_t(5966.0, q4, q3));
+  s = __dadd_rn(s, w7_t(2843.0, q4, q4));
+  b[2] = __dadd_rn(s, w7_t(1922.0, q4, q2));
+  s = __dsub_rn(w7_t(267.0, q1, q1), w7_t(494.0, q4, q1));
+  s = __dsub_rn(s, w7_t(1642.0, q2, q1));
+  s = __dadd_rn(s, w7_t(1602.0, q3, q1));
+  s = __dsub_rn(s, w7_t(5966.0, q3, q2));
+  s = __dadd_rn(s, w7_t(3443.0, q3, q3));
+  s = __dsub_rn(s, w7_t(2522.0, q4, q3));
+  s = __dadd_rn(s, w7_t(2843.0, q2, q2));
+  s = __dadd_rn(s, w7_t(547.0, q4, q4));
+  b[1] = __dadd_rn(s, w7_t(1922.0, q4, q2));
+  s = __dadd_rn(w7_t(2107.0, q3, q3), w7_t(7042.0, q3, q1));
+  s = __dsub_rn(s, w7_t(1854.0, q3, q0));
+  s = __dsub_rn(s, w7_t(9402.0, q3, q2));
+  s = __dsub_rn(s, w7_t(17246.0, q2, q1));
+  s = __dadd_rn(s, w7_t(4642.0, q2, q0));
+  s = __dadd_rn(s, w7_t(547.0, q0, q0));
+  s = __dsub_rn(s, w7_t(3882.0, q1, q0));
+  s = __dadd_rn(s, w7_t(11003.0, q2, q2));
+  b[0] = __dadd_rn(s, w7_t(7043.0, q1, q1));
 }
 
 // Face candidates (stencil_weno7, dorder 0): location 1..5, four points each.
