@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--t0", type=float, default=0.125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--skip-extras", action="store_true", help="no JS arm, e2e, CPU baseline (profiling runs)")
-    ap.add_argument("--workload", default="euler2d", choices=["euler2d", "adv1d", "train1d", "euler3d"],
+    ap.add_argument("--workload", default="euler2d", choices=["euler2d", "adv1d", "train1d", "euler3d", "euler2d_w7"],
                     help="euler2d: the headline 2D step; adv1d: 4096 ragged 1D trajectories; train1d: closure "
                          "training steps (B=1024, N=256); euler3d: the 224x88x88 shock-bubble step")
     ap.add_argument("--scheme", type=int, default=5, choices=[5, 7], help="adv1d: WENO5/SSPRK3 or WENO7/Shu RK4")
@@ -202,6 +202,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "euler3d":
         bench_3d(args, world, rank, local)
+        return
+    if args.workload == "euler2d_w7":
+        bench_w7(args, world, rank, local)
         return
     if args.workload != "euler2d":
         bench_1d(args, world, rank, local)
@@ -675,6 +678,102 @@ def _oracle3d_sample(sb_seed, method, params, budget_s):
     cells = sb.nx * sb.ny * sb.nz
     return {"value": cells * steps / el, "unit": UNIT, "cores": O.num_threads(True), "kind": "port",
             "sample": f"{steps} step(s) of the same problem on 56x22x22 from t=0 (C oracle, OpenMP), {el:.1f} s"}
+
+
+def bench_w7(args, world, rank, local):
+    """WENO7-JS 2D with Shu RK4 on the periodic isentropic vortex (the reference's point_rk4 path) at
+    args.n^2 (default 1024 when the 2D default 2000 is given), K steps from t = 0."""
+    import torch
+    import torch.distributed as dist
+
+    from oracle import oracle as O
+    from weno_sr_publishing_b200 import euler2d_w7 as E7
+    from weno_sr_publishing_b200 import problems as PR
+    n = 1024 if args.n == 2000 else args.n
+    metric = f"2D Euler cell-updates/s, WENO7-JS Shu RK4, {n}x{n} isentropic vortex"
+    cfg = {"workload": f"2D periodic isentropic vortex {n}x{n} on [-10,10]^2 (2x2 Gauss averages), from t=0",
+           "scheme": "WENO7-JS characteristic + two-point Gauss transverse", "flux": "hllc",
+           "time_integrator": "Shu RK4 (L and L~)", "cfl": 0.4, "state_precision": "fp64",
+           "l2_policy": f"state {(n + 8) ** 2 * 32 / 1e6:.0f} MB, workspace {(n * n * 32 * 14) / 1e6:.0f} MB",
+           "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    init = PR.vortex_point_rk4(n, n, 0.0, 2)
+    K, W = args.steps, max(args.warmup, 0)
+
+    def cpu_sample():
+        m = 64
+        small = PR.vortex_point_rk4(m, m, 0.0, 2)
+        pm = E7.Params(nx=m, ny=m)
+        steps, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < args.cpu_seconds:
+            _, _, k, _ = O.w7_run(small, m, m, pm.dx, pm.dy, 0.4, 100.0, "periodic", max_steps=1, fast=True)
+            steps += k
+        el = time.perf_counter() - t0
+        return {"value": m * m * steps / el, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                "sample": f"{steps} step(s) of the same problem on {m}x{m} (C oracle, OpenMP), {el:.1f} s"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = cpu_sample()
+        print(json.dumps({"metric": metric, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "impl": "reference", "cpu_baseline": base,
+                          "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    p = E7.Params(nx=n, ny=n, cfl=0.4, t_end=1.0e30)
+    u0 = torch.as_tensor(init, device=dev).contiguous()
+    ws = E7.workspace(n, n, dev)
+    u = u0.clone()
+    if W:
+        E7.run(u, p, "periodic", max_steps=W, ws=ws)
+    u.copy_(u0)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        res = E7.run(u, p, "periodic", max_steps=K, ws=ws)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    line = {"metric": metric, "value": world * n * n * res.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": res.steps, "warmup": W, "ms_per_step": ms / max(res.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "clocks": clk.summary(), "gpu_launches": 1 + res.steps * (3 + 6 * 5 + 4),
+            "state_finite": bool(torch.isfinite(u).all())}
+    if not args.skip_extras:
+        host = torch.empty(u0.shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(u0.cpu())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):  # each step: pinned state in, one step, state out
+            u.copy_(host, non_blocking=True)
+            E7.run(u, p, "periodic", max_steps=1, ws=ws)
+            host.copy_(u, non_blocking=True)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        line["e2e"] = {"value": n * n * K / el, "unit": UNIT, "h2d_bytes_per_step": u.numel() * 8,
+                       "d2h_bytes_per_step": u.numel() * 8,
+                       "api": "weno_sr_publishing_b200.euler2d_w7.run (pinned host buffer, 1 step per call)"}
+        if rank == 0:
+            line["cpu_baseline"] = cpu_sample()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def bench_3d(args, world, rank, local):
