@@ -79,15 +79,17 @@ int wsr_closure_upload(wsr_ctx *ctx, int kind, const double *packed, int n);
 size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny);
 /* One right-hand side into rhs (interior [ny][nx][4]): L(u) (reverse = 0) or the downwind operator L~(u)
  * whose interface fluxes take the Gauss states in swapped order (reverse = 1); compute_rhs of
- * point_rk4.py:435-511. */
+ * point_rk4.py:435-511. method: WSR_METHOD_JS (classical weights) or WSR_METHOD_Z (WENO-Z, p = 3, betas / 240,
+ * eps = dx^3 along x and dy^3 along y: weno_z_borges_p2_results/weno7_point_rk4_z.py, weight_kind 1). */
 int wsr_euler2d_w7_rhs(wsr_ctx *ctx, const double *u, double *rhs, int nx, int ny, double dx, double dy,
-                       double gamma, int bc, int reverse, void *workspace, size_t workspace_bytes, void *stream);
+                       double gamma, int bc, int method, int reverse, void *workspace, size_t workspace_bytes,
+                       void *stream);
 /* Time loop of run_from_initial (point_rk4.py:568-600) on u in place from time t_start: dt = cfl min(dx, dy)
  * / max speed, the loop runs while t < t_end, a step that would pass t_end is shortened to reach it; at most
  * max_steps steps. dts_host (capacity max_steps) receives each step's dt. */
 int wsr_euler2d_w7_run(wsr_ctx *ctx, double *u, int nx, int ny, double dx, double dy, double gamma, double cfl,
-                       double t_start, double t_end, int bc, int max_steps, double *dts_host, int *steps_out,
-                       double *t_out, void *workspace, size_t workspace_bytes, void *stream);
+                       double t_start, double t_end, int bc, int method, int max_steps, double *dts_host,
+                       int *steps_out, double *t_out, void *workspace, size_t workspace_bytes, void *stream);
 
 /* Bytes of device workspace the 2D functions need for an nx x ny interior. */
 size_t wsr_euler2d_workspace_bytes(int nx, int ny);

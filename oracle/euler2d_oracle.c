@@ -901,15 +901,67 @@ double or_w7_gauss(const double *q, int lr) { /* weno7_gauss_lr_scalar */
     return w7_js_combine(q, s, d);
 }
 
-/* weno7_lr_vec_characteristic: Roe(q3, q4) for lr = 1, Roe(q2, q3) for lr = 2 */
-static vec4 w7_char_face(const vec4 *q, int lr, int dir, double g) {
+/* Betas of the WENO-Z module (weno7_helpers_z.py:557-588): the same quadratic forms (with the common factor
+ * 240) written as a sum of squares, non-negative in floating point. */
+static void w7_beta_sq(const double *q, double *b) {
+    double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
+    double c0 = 20.0 / 3.0, c1 = 260.0, c2 = 781.0 / 3.0;
+    double a00 = -2.0*q0 + 9.0*q1 - 18.0*q2 + 11.0*q3, a01 = -q0 + 4.0*q1 - 5.0*q2 + 2.0*q3, a02 = -q0 + 3.0*q1 - 3.0*q2 + q3;
+    b[0] = c0*a00*a00 + c1*a01*a01 + c2*a02*a02;
+    double a10 = q1 - 6.0*q2 + 3.0*q3 + 2.0*q4, a11 = q2 - 2.0*q3 + q4, a12 = -q1 + 3.0*q2 - 3.0*q3 + q4;
+    b[1] = c0*a10*a10 + c1*a11*a11 + c2*a12*a12;
+    double a20 = -2.0*q2 - 3.0*q3 + 6.0*q4 - q5, a21 = q2 - 2.0*q3 + q4, a22 = -q2 + 3.0*q3 - 3.0*q4 + q5;
+    b[2] = c0*a20*a20 + c1*a21*a21 + c2*a22*a22;
+    double a30 = -11.0*q3 + 18.0*q4 - 9.0*q5 + 2.0*q6, a31 = 2.0*q3 - 5.0*q4 + 4.0*q5 - q6, a32 = -q3 + 3.0*q4 - 3.0*q5 + q6;
+    b[3] = c0*a30*a30 + c1*a31*a31 + c2*a32*a32;
+}
+
+/* WENO-Z weights of the WENO7 path, weight_kind 1 (weno_z_borges_p2_results/weno7_helpers_z.py:900-957):
+ * betas / 240, tau = |-b0 - 3 b1 + 3 b2 + b3|, alpha = d (1 + (tau / (b + h^3))^3), value = sum (alpha/sum) s. */
+static double w7_z_combine(const double *q, const double *s, const double *d, double h) {
+    double bb[4];
+    w7_beta_sq(q, bb);
+    double inv240 = 1.0 / 240.0, eps = h * h * h;
+    double b0 = bb[0] * inv240, b1 = bb[1] * inv240, b2 = bb[2] * inv240, b3 = bb[3] * inv240;
+    double tau = fabs(-b0 - 3.0 * b1 + 3.0 * b2 + b3);
+    double r0 = tau / (b0 + eps), r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
+    double a0 = d[0] * (1.0 + r0 * r0 * r0), a1 = d[1] * (1.0 + r1 * r1 * r1), a2 = d[2] * (1.0 + r2 * r2 * r2),
+           a3 = d[3] * (1.0 + r3 * r3 * r3);
+    double asum = a0 + a1 + a2 + a3;
+    return a0 / asum * s[0] + a1 / asum * s[1] + a2 / asum * s[2] + a3 / asum * s[3];
+}
+
+double or_w7z_face(const double *q, int lr, double h) { /* weno7_lr_scalar_normalized */
+    double s[4];
+    int o = lr == 1 ? 1 : 2;
+    for (int k = 0; k < 4; ++k) s[k] = w7_face_cand(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+    double d1[4] = {1.0/35.0, 12.0/35.0, 18.0/35.0, 4.0/35.0}, d2[4] = {4.0/35.0, 18.0/35.0, 12.0/35.0, 1.0/35.0};
+    return w7_z_combine(q, s, lr == 1 ? d1 : d2, h);
+}
+
+double or_w7z_gauss(const double *q, int lr, double h) { /* weno7_gauss_lr_scalar_normalized */
+    double r3 = sqrt(3.0), s[4], d[4];
+    int o = lr == 1 ? 1 : 5;
+    for (int k = 0; k < 4; ++k) s[k] = w7_gauss_cand(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+    if (lr == 1) {
+        d[0] = 59.0/880.0 - 5.0*r3/16632.0; d[1] = 381.0/880.0 - 587.0*r3/194040.0;
+        d[2] = 381.0/880.0 + 587.0*r3/194040.0; d[3] = 59.0/880.0 + 5.0*r3/16632.0;
+    } else {
+        d[0] = 59.0/880.0 + 5.0*r3/16632.0; d[1] = 381.0/880.0 + 587.0*r3/194040.0;
+        d[2] = 381.0/880.0 - 587.0*r3/194040.0; d[3] = 59.0/880.0 - 5.0*r3/16632.0;
+    }
+    return w7_z_combine(q, s, d, h);
+}
+
+/* weno7_lr_vec_characteristic: Roe(q3, q4) for lr = 1, Roe(q2, q3) for lr = 2; h > 0 selects WENO-Z */
+static vec4 w7_char_face(const vec4 *q, int lr, int dir, double g, double h) {
     vec4 roe = lr == 2 ? roe_average_state(q[2], q[3], g) : roe_average_state(q[3], q[4], g);
     vec4 c[7], cf;
     for (int k = 0; k < 7; ++k) c[k] = con_to_char(q[k], roe, dir, g);
     for (int f = 0; f < 4; ++f) {
         double s[7];
         for (int k = 0; k < 7; ++k) s[k] = c[k].v[f];
-        cf.v[f] = or_w7_face(s, lr);
+        cf.v[f] = h > 0.0 ? or_w7z_face(s, lr, h) : or_w7_face(s, lr);
     }
     return char_to_con(cf, roe, dir, g);
 }
@@ -932,7 +984,7 @@ static void w7_fill_bc(double *u, int nx, int ny, int bc) { /* apply_(periodic_)
 
 /* compute_rhs (point_rk4.py:435-511): rhs interior [ny][nx][4]. src's ghost cells are filled in place.
  * Returns 0, or -1 on allocation failure. */
-int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, double g, int bc, int reverse) {
+int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, double g, int bc, int reverse, int z) {
     int nxt = nx + 2 * G7, nyt = ny + 2 * G7;
     size_t np = (size_t)nxt * nyt * 4;
     double *xl = calloc(np, 8), *xr = calloc(np, 8), *yl = calloc(np, 8), *yr = calloc(np, 8);
@@ -945,8 +997,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
         for (int i = 0; i < nx + 2; ++i) {
             vec4 q[7];
             for (int k = 0; k < 7; ++k) q[k] = load4(src, nxt, j, i + k);
-            store4(xl, nxt, j, i, w7_char_face(q, 2, 1, g));
-            store4(xr, nxt, j, i, w7_char_face(q, 1, 1, g));
+            store4(xl, nxt, j, i, w7_char_face(q, 2, 1, g, z ? dx : 0.0));
+            store4(xr, nxt, j, i, w7_char_face(q, 1, 1, g, z ? dx : 0.0));
         }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int j = 0; j < ny; ++j)
@@ -959,8 +1011,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
                         a[k] = xr[((size_t)(j + 1 + k) * nxt + i) * 4 + comp];
                         b[k] = xl[((size_t)(j + 1 + k) * nxt + i + 1) * 4 + comp];
                     }
-                    sl.v[comp] = or_w7_gauss(a, loca);
-                    sr.v[comp] = or_w7_gauss(b, loca);
+                    sl.v[comp] = z ? or_w7z_gauss(a, loca, dy) : or_w7_gauss(a, loca);
+                    sr.v[comp] = z ? or_w7z_gauss(b, loca, dy) : or_w7_gauss(b, loca);
                 }
                 vec4 f = reverse ? or_hllc_flux(sr, sl, 1, g) : or_hllc_flux(sl, sr, 1, g);
                 store4(loca == 1 ? f1 : f2, nxt, j, i, f);
@@ -970,8 +1022,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
         for (int i = 0; i < nx + 8; ++i) {
             vec4 q[7];
             for (int k = 0; k < 7; ++k) q[k] = load4(src, nxt, j + k, i);
-            store4(yl, nxt, j, i, w7_char_face(q, 2, 2, g));
-            store4(yr, nxt, j, i, w7_char_face(q, 1, 2, g));
+            store4(yl, nxt, j, i, w7_char_face(q, 2, 2, g, z ? dy : 0.0));
+            store4(yr, nxt, j, i, w7_char_face(q, 1, 2, g, z ? dy : 0.0));
         }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int j = 0; j < ny + 1; ++j)
@@ -984,8 +1036,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
                         a[k] = yr[((size_t)j * nxt + i + 1 + k) * 4 + comp];
                         b[k] = yl[((size_t)(j + 1) * nxt + i + 1 + k) * 4 + comp];
                     }
-                    sl.v[comp] = or_w7_gauss(a, loca);
-                    sr.v[comp] = or_w7_gauss(b, loca);
+                    sl.v[comp] = z ? or_w7z_gauss(a, loca, dx) : or_w7_gauss(a, loca);
+                    sr.v[comp] = z ? or_w7z_gauss(b, loca, dx) : or_w7_gauss(b, loca);
                 }
                 vec4 f = reverse ? or_hllc_flux(sr, sl, 2, g) : or_hllc_flux(sl, sr, 2, g);
                 store4(loca == 1 ? h1 : h2, nxt, j, i, f);
@@ -1022,7 +1074,7 @@ static double w7_max_speed(const double *u, int nx, int ny, double g) {
 
 /* run_from_initial (point_rk4.py:568-600) with launch_shu_rk4_step (514-538): u is advanced in place.
  * Returns the step count (dts receives up to max_dts values) or -1 on allocation failure. */
-int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double cfl, double t_end, int bc,
+int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double cfl, double t_end, int bc, int z,
               int max_steps, double *dts, int max_dts, double *t_out) {
     size_t np = (size_t)(nx + 2 * G7) * (ny + 2 * G7) * 4, ni = (size_t)nx * ny * 4;
     double *u1 = calloc(np, 8), *u2 = calloc(np, 8), *u3 = calloc(np, 8);
@@ -1038,23 +1090,23 @@ int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double 
         if (dt <= 0.0) break;
 #define IN7(a, j, i, c) (a)[((size_t)((j) + G7) * nxt + (i) + G7) * 4 + (c)]
 #define RI7(a, j, i, c) (a)[((size_t)(j) * nx + (i)) * 4 + (c)]
-        if (or_w7_rhs(u, r0, nx, ny, dx, dy, g, bc, 0)) { step = -1; goto done; }
+        if (or_w7_rhs(u, r0, nx, ny, dx, dy, g, bc, 0, z)) { step = -1; goto done; }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u1, j, i, c) = IN7(u, j, i, c) + 0.5 * dt * RI7(r0, j, i, c);
-        if (or_w7_rhs(u, rt0, nx, ny, dx, dy, g, bc, 1) || or_w7_rhs(u1, r1, nx, ny, dx, dy, g, bc, 0)) {
+        if (or_w7_rhs(u, rt0, nx, ny, dx, dy, g, bc, 1, z) || or_w7_rhs(u1, r1, nx, ny, dx, dy, g, bc, 0, z)) {
             step = -1; goto done;
         }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u2, j, i, c) = 649.0/1600.0 * IN7(u, j, i, c) - 10890423.0/25193600.0 * dt * RI7(rt0, j, i, c)
                                + 951.0/1600.0 * IN7(u1, j, i, c) + 5000.0/7873.0 * dt * RI7(r1, j, i, c);
-        if (or_w7_rhs(u1, rt1, nx, ny, dx, dy, g, bc, 1) || or_w7_rhs(u2, r2, nx, ny, dx, dy, g, bc, 0)) {
+        if (or_w7_rhs(u1, rt1, nx, ny, dx, dy, g, bc, 1, z) || or_w7_rhs(u2, r2, nx, ny, dx, dy, g, bc, 0, z)) {
             step = -1; goto done;
         }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u3, j, i, c) = 53989.0/2500000.0 * IN7(u, j, i, c) - 102261.0/5000000.0 * dt * RI7(rt0, j, i, c)
                                + 4806213.0/20000000.0 * IN7(u1, j, i, c) - 5121.0/20000.0 * dt * RI7(rt1, j, i, c)
                                + 23619.0/32000.0 * IN7(u2, j, i, c) + 7873.0/10000.0 * dt * RI7(r2, j, i, c);
-        if (or_w7_rhs(u3, r3, nx, ny, dx, dy, g, bc, 0)) { step = -1; goto done; }
+        if (or_w7_rhs(u3, r3, nx, ny, dx, dy, g, bc, 0, z)) { step = -1; goto done; }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u, j, i, c) = 1.0/5.0 * IN7(u, j, i, c) + 1.0/10.0 * dt * RI7(r0, j, i, c)
                               + 6127.0/30000.0 * IN7(u1, j, i, c) + 1.0/6.0 * dt * RI7(r1, j, i, c)

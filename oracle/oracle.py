@@ -63,10 +63,15 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_w7_gauss.restype = C.c_double
         lib.or_w7_gauss.argtypes = [_dp, C.c_int]
         lib.or_w7_rhs.restype = C.c_int
-        lib.or_w7_rhs.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
+        lib.or_w7_rhs.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                  C.c_int]
+        lib.or_w7z_face.restype = C.c_double
+        lib.or_w7z_face.argtypes = [_dp, C.c_int, C.c_double]
+        lib.or_w7z_gauss.restype = C.c_double
+        lib.or_w7z_gauss.argtypes = [_dp, C.c_int, C.c_double]
         lib.or_w7_run.restype = C.c_int
         lib.or_w7_run.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
-                                  C.c_int, C.c_int, _dp, C.c_int, C.POINTER(C.c_double)]
+                                  C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(C.c_double)]
         lib.or_evilin5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, _dp]
         _LIBS[name] = lib
     return _LIBS[name]
@@ -223,22 +228,33 @@ def w7_gauss(q, lr: int) -> np.ndarray:
     return np.array([_lib().or_w7_gauss(np.ascontiguousarray(r), lr) for r in q])
 
 
-def w7_rhs(u, nx, ny, dx, dy, bc="periodic", reverse=False, gamma=1.4) -> np.ndarray:
-    """L(u) (or L~(u)) on the interior [ny][nx][4]."""
+def w7z_face(q, lr: int, h: float) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    return np.array([_lib().or_w7z_face(np.ascontiguousarray(r), lr, h) for r in q])
+
+
+def w7z_gauss(q, lr: int, h: float) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    return np.array([_lib().or_w7z_gauss(np.ascontiguousarray(r), lr, h) for r in q])
+
+
+def w7_rhs(u, nx, ny, dx, dy, bc="periodic", reverse=False, gamma=1.4, method="js") -> np.ndarray:
+    """L(u) (or L~(u)) on the interior [ny][nx][4]; method "js" or "z" (WENO-Z, eps = h^3)."""
     src = np.array(u, dtype=np.float64, copy=True, order="C")
     out = np.zeros((ny, nx, 4))
-    if _lib().or_w7_rhs(src, out, nx, ny, dx, dy, gamma, BC7[bc], int(bool(reverse))):
+    if _lib().or_w7_rhs(src, out, nx, ny, dx, dy, gamma, BC7[bc], int(bool(reverse)), int(method == "z")):
         raise MemoryError("oracle allocation failed")
     return out
 
 
-def w7_run(u, nx, ny, dx, dy, cfl, t_end, bc="periodic", max_steps=1_000_000, gamma=1.4, fast=False):
+def w7_run(u, nx, ny, dx, dy, cfl, t_end, bc="periodic", max_steps=1_000_000, gamma=1.4, fast=False,
+           method="js"):
     """run_from_initial of the WENO7 point RK4 path. Returns (final padded state, dts, steps, t)."""
     out = np.array(u, dtype=np.float64, copy=True, order="C")
     dts = np.zeros(min(max_steps, 1 << 20))
     t = C.c_double(0.0)
-    steps = _lib(fast).or_w7_run(out, nx, ny, dx, dy, gamma, cfl, t_end, BC7[bc], max_steps, dts, dts.size,
-                                 C.byref(t))
+    steps = _lib(fast).or_w7_run(out, nx, ny, dx, dy, gamma, cfl, t_end, BC7[bc], int(method == "z"), max_steps,
+                                 dts, dts.size, C.byref(t))
     if steps < 0:
         raise MemoryError("oracle allocation failed")
     return out, list(dts[:steps]), steps, t.value

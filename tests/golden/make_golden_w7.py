@@ -78,6 +78,31 @@ def main() -> None:
         out[f"{name}_steps"] = summary["steps"]
         out[f"{name}_t"] = summary["t"]
         print(f"{name}: steps={summary['steps']} t={summary['t']:.6g} ({time.time() - t0:.1f}s)", flush=True)
+    zh = importlib.import_module("weno_z_borges_p2_results.weno7_helpers_z")
+    zr = importlib.import_module("weno_z_borges_p2_results.weno7_point_rk4_z")
+    for hi, h in enumerate((0.1, 1.0)):
+        for lr in (1, 2):
+            out[f"z_face_lr{lr}_h{hi}"] = np.array([zh.weno7_lr_scalar_normalized(*map(float, r), lr, h, 0, 1)
+                                                    for r in q])
+            out[f"z_gauss_lr{lr}_h{hi}"] = np.array([zh.weno7_gauss_lr_scalar_normalized(*map(float, r), lr, h, 0, 1)
+                                                     for r in q])
+    out["z_h"] = np.array([0.1, 1.0])
+    for name, (params, seed, bc) in cases.items():
+        zp = zr.Params(nx=params.nx, ny=params.ny, x_min=params.x_min, x_max=params.x_max, y_min=params.y_min,
+                       y_max=params.y_max, t_end=params.t_end)
+        init = out[f"{name}_initial"]
+        for rev in (0, 1):
+            arrays = zr.allocate_arrays(init, zp, "cpu")
+            zr.compute_rhs(arrays, zp, "u", "rhs0", 0.01, "cpu", solver_kind=1, characteristic=True,
+                           reverse_upwind=bool(rev), boundary=bc, weight_kind=1)
+            g = zp.ghost
+            out[f"z_{name}_rhs_rev{rev}"] = np.asarray(arrays["rhs0"])[g:g + zp.ny, g:g + zp.nx]
+        final, summary = zr.run_from_initial(init, zp, device="cpu", riemann_solver="hllc", characteristic=True,
+                                             boundary=bc, weight_kind=1)
+        out[f"z_{name}_final"] = np.asarray(final)
+        out[f"z_{name}_steps"] = summary["steps"]
+        out[f"z_{name}_t"] = summary["t"]
+        print(f"z {name}: steps={summary['steps']} t={summary['t']:.6g}", flush=True)
     np.savez_compressed(HERE / "euler2d_w7.npz", **out)
     print("euler2d_w7.npz written")
 

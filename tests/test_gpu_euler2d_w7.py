@@ -1,5 +1,5 @@
-"""CUDA 2D WENO7-JS with Shu RK4 (C ABI) against the reference's solver fixtures, the oracle, and the
-reference's published vortex, Sod and Lax tables."""
+"""CUDA 2D WENO7 (JS and Z weights) with Shu RK4 (C ABI) against the reference's solver fixtures, the
+oracle, and the reference's published vortex, Sod and Lax tables."""
 from __future__ import annotations
 
 from pathlib import Path
@@ -110,6 +110,68 @@ def test_sod_and_lax_tables():
             assert abs(got / rv - 1.0) <= 1e-9, (field, got, rv)
 
 
+@pytest.mark.parametrize("name", ["vortex", "rough"])
+@pytest.mark.parametrize("rev", [0, 1])
+def test_z_rhs_matches_reference(name, rev):
+    """weno7_point_rk4_z (weight_kind 1: p = 3, betas / 240, eps = h^3) right-hand sides."""
+    g = _gold()
+    p = _params(g, name)
+    u = torch.as_tensor(g[f"{name}_initial"], device=DEV).contiguous()
+    got = E7.rhs(u, p, str(g[f"{name}_bc"]), reverse=bool(rev), method="z").cpu().numpy()
+    ref = g[f"z_{name}_rhs_rev{rev}"]
+    assert np.abs(got - ref).max() <= RHS_TOL * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["vortex", "rough"])
+def test_z_run_from_initial_matches_reference(name):
+    g = _gold()
+    p = _params(g, name)
+    final, summary = E7.run_from_initial(g[f"{name}_initial"], p, device=DEV, boundary=str(g[f"{name}_bc"]),
+                                         method="z")
+    assert summary["steps"] == int(g[f"z_{name}_steps"]) and abs(summary["t"] - float(g[f"z_{name}_t"])) <= 1e-14
+    assert _rel(final[4:-4, 4:-4], g[f"z_{name}_final"][4:-4, 4:-4]) <= RUN_TOL
+
+
+@pytest.mark.parametrize("bc", ["periodic", "transmissive"])
+def test_z_ragged_grid_against_oracle(bc):
+    nx, ny = 29, 41
+    p = E7.Params(nx=nx, ny=ny, cfl=0.4, t_end=0.5)
+    init = problems.vortex_point_rk4(nx, ny, 0.0, 3)
+    ref, rdts, rsteps, rt = O.w7_run(init, nx, ny, p.dx, p.dy, 0.4, 0.5, bc, method="z")
+    u = torch.as_tensor(init, device=DEV).contiguous()
+    res = E7.run(u, p, bc, method="z")
+    assert res.steps == rsteps and res.t == pytest.approx(rt, abs=1e-15)
+    np.testing.assert_allclose(res.dts, rdts, rtol=1e-12)
+    assert _rel(u.cpu().numpy()[4:-4, 4:-4], ref[4:-4, 4:-4]) <= RUN_TOL
+
+
+# WENO7-Z-RK4 rows of experiments/05_isentropic_vortex/tables/vortex_convergence.md: (L1, L2) of rho
+VORTEX_Z = {25: (9.24722844e-04, 3.80751034e-03), 50: (8.30137623e-05, 4.47443425e-04),
+            100: (2.38982847e-06, 1.31101155e-05), 200: (2.93282637e-08, 1.71997176e-07)}
+
+
+@pytest.mark.parametrize("n", [25, 50, 100, 200])
+def test_z_vortex_table(n):
+    r = A.vortex7_run(n, DEV, method="z")
+    for got, ref in zip((r.l1, r.l2), VORTEX_Z[n]):
+        assert abs(got / ref - 1.0) <= 1e-8, (n, got, ref)
+
+
+def test_z_sod_and_lax_tables():
+    """weno7_z_p3 rows of experiments/02 (Sod: rho L1, L2, Linf) and 03 (Lax: rho, u, p)."""
+    r = R.shock_tube_run(R.SOD, "w7_z", device=DEV)
+    for got, ref in zip((r["rho_l1_mean"], r["rho_l2"], r["rho_linf"]),
+                        (0.005067383382686812, 0.010572181673056028, 0.05182032580354834)):
+        assert abs(got / ref - 1.0) <= 1e-9, (got, ref)
+    r = R.shock_tube_run(R.LAX, "w7_z", device=DEV)
+    lax = {"rho": (0.006104027658765422, 0.03149785277140588, 0.3313187561959483),
+           "velocity": (0.006087585881834266, 0.027071085748154113, 0.3470615588986299),
+           "pressure": (0.007345408696330224, 0.02675261391710653, 0.24739722211405157)}
+    for field, ref in lax.items():
+        for got, rv in zip((r[f"{field}_l1_mean"], r[f"{field}_l2"], r[f"{field}_linf"]), ref):
+            assert abs(got / rv - 1.0) <= 1e-9, (field, got, rv)
+
+
 def test_invalid_arguments_raise():
     p = E7.Params(nx=3, ny=8)
     with pytest.raises(ValueError):
@@ -119,3 +181,5 @@ def test_invalid_arguments_raise():
         E7.run(torch.zeros(p.padded_shape, dtype=torch.float64, device=DEV), p, "reflective")
     with pytest.raises(NotImplementedError):
         E7.run_from_initial(np.zeros(p.padded_shape), p, device=DEV, riemann_solver="evilin")
+    with pytest.raises(ValueError):
+        E7.rhs(torch.zeros(p.padded_shape, dtype=torch.float64, device=DEV), p, method="sr_f32")

@@ -50,3 +50,29 @@ def test_run_matches_reference(gold, name):
 def test_vortex_initial_state_matches_reference(gold):
     from weno_sr_publishing_b200 import problems  # noqa: PLC0415
     np.testing.assert_array_equal(problems.vortex_point_rk4(12, 10, 0.0, 5), gold["vortex_initial"])
+
+
+# WENO-Z variant of the same path (weno_z_borges_p2_results/weno7_point_rk4_z.py, weight_kind 1)
+@pytest.mark.parametrize("hi", [0, 1])
+@pytest.mark.parametrize("lr", [1, 2])
+def test_z_reconstructions_bitwise(gold, lr, hi):
+    h = float(gold["z_h"][hi])
+    np.testing.assert_array_equal(O.w7z_face(gold["q"], lr, h), gold[f"z_face_lr{lr}_h{hi}"])
+    np.testing.assert_array_equal(O.w7z_gauss(gold["q"], lr, h), gold[f"z_gauss_lr{lr}_h{hi}"])
+
+
+@pytest.mark.parametrize("name", ["vortex", "rough"])
+@pytest.mark.parametrize("rev", [0, 1])
+def test_z_rhs_matches_reference(gold, name, rev):
+    nx, ny, dx, dy, _, _, bc = _meta(gold, name)
+    got = O.w7_rhs(gold[f"{name}_initial"], nx, ny, dx, dy, bc, reverse=rev, method="z")
+    np.testing.assert_array_equal(got, gold[f"z_{name}_rhs_rev{rev}"])
+
+
+@pytest.mark.parametrize("name", ["vortex", "rough"])
+def test_z_run_matches_reference(gold, name):
+    nx, ny, dx, dy, cfl, t_end, bc = _meta(gold, name)
+    fin, dts, steps, t = O.w7_run(gold[f"{name}_initial"], nx, ny, dx, dy, cfl, t_end, bc, method="z")
+    assert steps == int(gold[f"z_{name}_steps"]) and t == float(gold[f"z_{name}_t"])
+    g = 4
+    np.testing.assert_array_equal(fin[g:g + ny, g:g + nx], gold[f"z_{name}_final"][g:g + ny, g:g + nx])

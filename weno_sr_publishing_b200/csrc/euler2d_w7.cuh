@@ -158,15 +158,75 @@ __device__ __forceinline__ void w7_js_gauss(const double q[7], double& g1, doubl
   g2 = w7_combine(r, db, s);
 }
 
+// Betas of the WENO-Z module (weno_z_borges_p2_results/weno7_helpers_z.py:557-588): the same quadratic
+// forms as w7_beta written as sums of squares with c = 20/3, 260, 781/3, so they stay non-negative.
+__device__ __forceinline__ void w7_beta_sq(const double q[7], double b[4]) {
+  const double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
+  constexpr double c0 = 20.0 / 3.0, c1 = 260.0, c2 = 781.0 / 3.0;
+  double a0 = -2.0 * q0 + 9.0 * q1 - 18.0 * q2 + 11.0 * q3, a1 = -q0 + 4.0 * q1 - 5.0 * q2 + 2.0 * q3,
+         a2 = -q0 + 3.0 * q1 - 3.0 * q2 + q3;
+  b[0] = c0 * a0 * a0 + c1 * a1 * a1 + c2 * a2 * a2;
+  a0 = q1 - 6.0 * q2 + 3.0 * q3 + 2.0 * q4, a1 = q2 - 2.0 * q3 + q4, a2 = -q1 + 3.0 * q2 - 3.0 * q3 + q4;
+  b[1] = c0 * a0 * a0 + c1 * a1 * a1 + c2 * a2 * a2;
+  a0 = -2.0 * q2 - 3.0 * q3 + 6.0 * q4 - q5, a1 = q2 - 2.0 * q3 + q4, a2 = -q2 + 3.0 * q3 - 3.0 * q4 + q5;
+  b[2] = c0 * a0 * a0 + c1 * a1 * a1 + c2 * a2 * a2;
+  a0 = -11.0 * q3 + 18.0 * q4 - 9.0 * q5 + 2.0 * q6, a1 = 2.0 * q3 - 5.0 * q4 + 4.0 * q5 - q6,
+  a2 = -q3 + 3.0 * q4 - 3.0 * q5 + q6;
+  b[3] = c0 * a0 * a0 + c1 * a1 * a1 + c2 * a2 * a2;
+}
+
+// WENO-Z weights of the WENO7 path (weno_z_borges_p2_results/weno7_helpers_z.py:900-957, weight_kind 1):
+// betas scaled by 1/240, tau = |-b0 - 3 b1 + 3 b2 + b3|, alpha_k = d_k (1 + (tau / (b_k + h^3))^3),
+// w = alpha / sum, value = sum w_k s_k.
+__device__ __forceinline__ double w7_z_value(const double b[4], const double d[4], const double s[4], double eps) {
+  constexpr double inv240 = 1.0 / 240.0;
+  const double b0 = b[0] * inv240, b1 = b[1] * inv240, b2 = b[2] * inv240, b3 = b[3] * inv240;
+  const double tau = fabs(-b0 - 3.0 * b1 + 3.0 * b2 + b3);
+  const double r0 = tau * rcp64(b0 + eps), r1 = tau * rcp64(b1 + eps), r2 = tau * rcp64(b2 + eps),
+               r3 = tau * rcp64(b3 + eps);
+  const double a0 = d[0] * (1.0 + r0 * r0 * r0), a1 = d[1] * (1.0 + r1 * r1 * r1), a2 = d[2] * (1.0 + r2 * r2 * r2),
+               a3 = d[3] * (1.0 + r3 * r3 * r3);
+  const double inv = rcp64(a0 + a1 + a2 + a3);
+  return a0 * inv * s[0] + a1 * inv * s[1] + a2 * inv * s[2] + a3 * inv * s[3];
+}
+
+// Face value with WENO-Z weights (weno7_lr_scalar_normalized), eps = h^3 of the reconstruction direction.
+__device__ __forceinline__ double w7_z_face(const double q[7], int lr, double eps) {
+  double b[4], s[4];
+  w7_beta_sq(q, b);
+  const int o = lr == 1 ? 1 : 2;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_face(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  const double d1[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
+  const double d2[4] = {4.0 / 35.0, 18.0 / 35.0, 12.0 / 35.0, 1.0 / 35.0};
+  return w7_z_value(b, lr == 1 ? d1 : d2, s, eps);
+}
+
+__device__ __forceinline__ void w7_z_gauss(const double q[7], double eps, double& g1, double& g2) {
+  double b[4], s[4];
+  w7_beta_sq(q, b);
+  constexpr double s3 = kS3;
+  const double e0 = 59.0 / 880.0, e1 = 5.0 * s3 / 16632.0, f0 = 381.0 / 880.0, f1 = 587.0 * s3 / 194040.0;
+  const double da[4] = {e0 - e1, f0 - f1, f0 + f1, e0 + e1};
+  const double db[4] = {e0 + e1, f0 + f1, f0 - f1, e0 - e1};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_gauss(1 + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  g1 = w7_z_value(b, da, s, eps);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_gauss(5 + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  g2 = w7_z_value(b, db, s, eps);
+}
+
 // Normal reconstruction, one thread per face.
 // DIR=1: face (r, c), r in [1, ny+7), c in [0, nx]: padded row r, cells c..c+7; face between cells c+3 and
 //        c+4. Writes out_r[r][c] (lr=1 of cell c+3) and out_l[r][c+1] (lr=2 of cell c+4); arrays [ny+8][nx+2].
 // DIR=2: face (r, c), r in [0, ny], c in [1, nx+7): padded column c, cells r..r+7; writes out_r[r][c] and
 //        out_l[r+1][c]; arrays [ny+2][nx+8].
-template <int DIR>
+// Z = true: WENO-Z weights with eps = h^3 of this direction (eps_n).
+template <int DIR, bool Z>
 __global__ void __launch_bounds__(kBlock7, 4) k7_normal(const double* __restrict__ u, double* __restrict__ out_l,
                                                        double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
-                                                       const StepCtl* __restrict__ ctl) {
+                                                       double eps_n, const StepCtl* __restrict__ ctl) {
   __shared__ double s_ch[4][8][kBlock7];
   if (ctl->done) return;
   const int t = threadIdx.x;
@@ -198,7 +258,7 @@ __global__ void __launch_bounds__(kBlock7, 4) k7_normal(const double* __restrict
       double q[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][t];
-      cf[f] = w7_js_face(q, side == 0 ? 1 : 2);
+      cf[f] = Z ? w7_z_face(q, side == 0 ? 1 : 2, eps_n) : w7_js_face(q, side == 0 ? 1 : 2);
     }
     const d4 face = char_to_con<DIR>(cf, J);
     const size_t idx = DIR == 1 ? (size_t)r * (nx + 2) + c + side : (size_t)(r + side) * (nx + 8) + c;
@@ -210,10 +270,11 @@ __global__ void __launch_bounds__(kBlock7, 4) k7_normal(const double* __restrict
 // x faces (j, i), j in [0, ny), i in [0, nx]: u_L from xr[j+1..j+7][i], u_R from xl[j+1..j+7][i+1].
 // y faces (j, i), j in [0, ny], i in [0, nx): u_L from yr[j][i+1..i+7], u_R from yl[j+1][i+1..i+7].
 // Output f[j][i] = F(g1) + F(g2) (unscaled); with `reverse` the Riemann problem takes (u_R, u_L).
-template <int DIR>
+// Z = true: WENO-Z weights with eps = h^3 of the transverse direction (eps_t).
+template <int DIR, bool Z>
 __global__ void __launch_bounds__(kBlock7, 4) k7_flux(const double* __restrict__ fl, const double* __restrict__ fr,
                                                      double* __restrict__ fout, int nx, int ny, Gas gas, int reverse,
-                                                     const StepCtl* __restrict__ ctl) {
+                                                     double eps_t, const StepCtl* __restrict__ ctl) {
   if (ctl->done) return;
   const int t = threadIdx.x;
   const int i = DIR == 1 ? blockIdx.x * 32 + (t & 31) : blockIdx.x * kBlock7 + t;
@@ -236,7 +297,10 @@ __global__ void __launch_bounds__(kBlock7, 4) k7_flux(const double* __restrict__
       for (int k = 0; k < 7; ++k) q[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
     }
     double g1, g2;
-    w7_js_gauss(q, g1, g2);
+    if (Z)
+      w7_z_gauss(q, eps_t, g1, g2);
+    else
+      w7_js_gauss(q, g1, g2);
     if (side == 0) {
       l1.v[comp] = g1;
       l2.v[comp] = g2;

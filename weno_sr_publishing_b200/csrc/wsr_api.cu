@@ -776,8 +776,10 @@ Ws7 carve7(void* base, int nx, int ny) {
   return w;
 }
 
-int check7(wsr_ctx* ctx, int nx, int ny, int bc, void* ws, size_t wsb) {
+int check7(wsr_ctx* ctx, int nx, int ny, int bc, int method, void* ws, size_t wsb) {
   if (!ctx) return WSR_ERR_ARG;
+  if (method != WSR_METHOD_JS && method != WSR_METHOD_Z)
+    return fail(ctx, WSR_ERR_ARG, "WENO7 2D method must be WSR_METHOD_JS or WSR_METHOD_Z (got %d)", method);
   if (nx < 4 || ny < 4) return fail(ctx, WSR_ERR_ARG, "nx and ny must be >= 4 (got %d, %d)", nx, ny);
   if ((long long)(nx + 8) * (ny + 8) > (1ll << 31) / 4)
     return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
@@ -789,21 +791,32 @@ int check7(wsr_ctx* ctx, int nx, int ny, int bc, void* ws, size_t wsb) {
   return WSR_OK;
 }
 
-// One right-hand side L(src) (reverse = 0) or L~(src) (reverse = 1) into rhs: 5 launches.
-int launch_rhs7(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g, int bc,
-                int reverse, const Ws7& w, cudaStream_t st) {
+// One right-hand side L(src) (reverse = 0) or L~(src) (reverse = 1) into rhs: 5 launches. z: WENO-Z
+// weights with eps = dx^3 along x and dy^3 along y.
+template <bool Z>
+int launch_rhs7_t(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g,
+                  int bc, int reverse, const Ws7& w, cudaStream_t st) {
   const Gas gas = make_gas(g);
-  w7::k7_normal<1><<<dim3((nx + 1 + 127) / 128, ny + 7), 128, 0, st>>>(src, w.xl, w.xr, nx, ny, bc, gas, w.ctl);
+  const double ex = dx * dx * dx, ey = dy * dy * dy;
+  w7::k7_normal<1, Z><<<dim3((nx + 1 + 127) / 128, ny + 7), 128, 0, st>>>(src, w.xl, w.xr, nx, ny, bc, gas, ex, w.ctl);
   WSR_LAUNCHED(ctx, "k7_normal<x>");
-  w7::k7_normal<2><<<dim3((nx + 7 + 31) / 32, (ny + 1 + 3) / 4), 128, 0, st>>>(src, w.yl, w.yr, nx, ny, bc, gas, w.ctl);
+  w7::k7_normal<2, Z><<<dim3((nx + 7 + 31) / 32, (ny + 1 + 3) / 4), 128, 0, st>>>(src, w.yl, w.yr, nx, ny, bc, gas, ey,
+                                                                                w.ctl);
   WSR_LAUNCHED(ctx, "k7_normal<y>");
-  w7::k7_flux<1><<<dim3((nx + 1 + 31) / 32, (ny + 3) / 4), 128, 0, st>>>(w.xl, w.xr, w.fx, nx, ny, gas, reverse, w.ctl);
+  w7::k7_flux<1, Z><<<dim3((nx + 1 + 31) / 32, (ny + 3) / 4), 128, 0, st>>>(w.xl, w.xr, w.fx, nx, ny, gas, reverse,
+                                                                           ey, w.ctl);
   WSR_LAUNCHED(ctx, "k7_flux<x>");
-  w7::k7_flux<2><<<dim3((nx + 127) / 128, ny + 1), 128, 0, st>>>(w.yl, w.yr, w.fy, nx, ny, gas, reverse, w.ctl);
+  w7::k7_flux<2, Z><<<dim3((nx + 127) / 128, ny + 1), 128, 0, st>>>(w.yl, w.yr, w.fy, nx, ny, gas, reverse, ex, w.ctl);
   WSR_LAUNCHED(ctx, "k7_flux<y>");
   w7::k7_rhs<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(w.fx, w.fy, rhs, nx, ny, 1.0 / dx, 1.0 / dy, w.ctl);
   WSR_LAUNCHED(ctx, "k7_rhs");
   return WSR_OK;
+}
+
+int launch_rhs7(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g, int bc,
+                int reverse, bool z, const Ws7& w, cudaStream_t st) {
+  return z ? launch_rhs7_t<true>(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st)
+           : launch_rhs7_t<false>(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st);
 }
 
 template <int S>
@@ -815,23 +828,23 @@ int launch_shu7(wsr_ctx* ctx, const w7::ShuArgs& a, int nx, int ny, const Ws7& w
 
 // One Shu RK4 step of u (in place): L(u), L~(u), L(u1), L~(u1), L(u2), L(u3) and four combinations
 // (point_rk4.py:514-538).
-int shu_step7(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double g, int bc, const Ws7& w,
+int shu_step7(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double g, int bc, bool z, const Ws7& w,
               cudaStream_t st) {
   int rc;
   double* const* R = w.rhs;
   w7::ShuArgs a{u, w.u1, w.u2, w.u3, R[0], R[1], R[2], R[3], R[4], R[5], nullptr};
-  if ((rc = launch_rhs7(ctx, u, R[0], nx, ny, dx, dy, g, bc, 0, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, u, R[0], nx, ny, dx, dy, g, bc, 0, z, w, st))) return rc;
   a.out = w.u1;
   if ((rc = launch_shu7<1>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, u, R[1], nx, ny, dx, dy, g, bc, 1, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u1, R[2], nx, ny, dx, dy, g, bc, 0, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, u, R[1], nx, ny, dx, dy, g, bc, 1, z, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u1, R[2], nx, ny, dx, dy, g, bc, 0, z, w, st))) return rc;
   a.out = w.u2;
   if ((rc = launch_shu7<2>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u1, R[3], nx, ny, dx, dy, g, bc, 1, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u2, R[4], nx, ny, dx, dy, g, bc, 0, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u1, R[3], nx, ny, dx, dy, g, bc, 1, z, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u2, R[4], nx, ny, dx, dy, g, bc, 0, z, w, st))) return rc;
   a.out = w.u3;
   if ((rc = launch_shu7<3>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u3, R[5], nx, ny, dx, dy, g, bc, 0, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u3, R[5], nx, ny, dx, dy, g, bc, 0, z, w, st))) return rc;
   a.out = u;
   return launch_shu7<4>(ctx, a, nx, ny, w, st);
 }
@@ -861,9 +874,9 @@ extern "C" size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny) {
 }
 
 extern "C" int wsr_euler2d_w7_rhs(wsr_ctx* ctx, const double* u, double* rhs, int nx, int ny, double dx, double dy,
-                                  double gamma, int bc, int reverse, void* workspace, size_t workspace_bytes,
-                                  void* stream) {
-  int rc = check7(ctx, nx, ny, bc, workspace, workspace_bytes);
+                                  double gamma, int bc, int method, int reverse, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  int rc = check7(ctx, nx, ny, bc, method, workspace, workspace_bytes);
   if (rc) return rc;
   if (!u || !rhs) return fail(ctx, WSR_ERR_ARG, "null pointer");
   if (misaligned(u) || misaligned(rhs)) return fail(ctx, WSR_ERR_ARG, "arrays must be 16-byte aligned");
@@ -873,14 +886,14 @@ extern "C" int wsr_euler2d_w7_rhs(wsr_ctx* ctx, const double* u, double* rhs, in
   Ws7 w = carve7(workspace, nx, ny);
   k7_init<<<1, 1, 0, st>>>(w.ctl, 0.0, 1.0, 0.0, 0.0, 1);
   WSR_LAUNCHED(ctx, "k7_init");
-  return launch_rhs7(ctx, u, rhs, nx, ny, dx, dy, gamma, bc, reverse != 0, w, st);
+  return launch_rhs7(ctx, u, rhs, nx, ny, dx, dy, gamma, bc, reverse != 0, method == WSR_METHOD_Z, w, st);
 }
 
 extern "C" int wsr_euler2d_w7_run(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double gamma,
-                                  double cfl, double t_start, double t_end, int bc, int max_steps, double* dts_host,
-                                  int* steps_out, double* t_out, void* workspace, size_t workspace_bytes,
-                                  void* stream) {
-  int rc = check7(ctx, nx, ny, bc, workspace, workspace_bytes);
+                                  double cfl, double t_start, double t_end, int bc, int method, int max_steps,
+                                  double* dts_host, int* steps_out, double* t_out, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  int rc = check7(ctx, nx, ny, bc, method, workspace, workspace_bytes);
   if (rc) return rc;
   if (!u) return fail(ctx, WSR_ERR_ARG, "null state");
   if (misaligned(u)) return fail(ctx, WSR_ERR_ARG, "state must be 16-byte aligned");
@@ -902,7 +915,7 @@ extern "C" int wsr_euler2d_w7_run(wsr_ctx* ctx, double* u, int nx, int ny, doubl
       w7::k7_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, w.ctl);
       w7::k7_step_begin<<<1, 1, 0, st>>>(w.ctl, w.dts, kDtsRing);
       WSR_LAUNCHED(ctx, "k7_step_begin");
-      if ((rc = shu_step7(ctx, u, nx, ny, dx, dy, gamma, bc, w, st))) return rc;
+      if ((rc = shu_step7(ctx, u, nx, ny, dx, dy, gamma, bc, method == WSR_METHOD_Z, w, st))) return rc;
       k_step_end<<<1, 1, 0, st>>>(w.ctl);
       WSR_LAUNCHED(ctx, "k_step_end");
     }

@@ -1,4 +1,4 @@
-"""2D Euler WENO7-JS with Shu's fourth-order TVD Runge-Kutta on the GPU (libwsr.so underneath).
+"""2D Euler WENO7 (JS or Z weights) with Shu's fourth-order TVD Runge-Kutta on the GPU (libwsr.so underneath).
 
 The reference's point-value WENO7 path (weno7_point_rk4_shu/point_rk4.py): characteristic WENO7 normal
 reconstruction, conservative two-point Gauss WENO7 transverse reconstruction, HLLC, and Shu's RK4 with the
@@ -17,6 +17,8 @@ from . import _native as N
 _ALIGN = 256
 GHOST = 4
 BC = {"transmissive": 0, "outflow": 0, "periodic": 1}
+# "js": classical WENO7 weights; "z": WENO-Z (p = 3, betas / 240, eps = h^3 per direction)
+METHOD = {"js": 0, "z": 4}
 
 
 @dataclass(frozen=True)
@@ -88,8 +90,14 @@ def _stream(dev: int):
     return C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
 
+def _method(method: str) -> int:
+    if method not in METHOD:
+        raise ValueError(f"unsupported WENO7 method {method!r}")
+    return METHOD[method]
+
+
 def rhs(u: torch.Tensor, params: Params, boundary: str = "periodic", reverse: bool = False,
-        ws: Workspace | None = None) -> torch.Tensor:
+        ws: Workspace | None = None, method: str = "js") -> torch.Tensor:
     """L(u) (or the downwind L~(u)) on the interior, shape [ny, nx, 4] (compute_rhs, point_rk4.py:435-511)."""
     _check(u, params)
     bc = _bc(boundary)
@@ -99,7 +107,8 @@ def rhs(u: torch.Tensor, params: Params, boundary: str = "periodic", reverse: bo
     out = torch.empty((params.ny, params.nx, 4), dtype=torch.float64, device=u.device)
     ctx.check(N.lib().wsr_euler2d_w7_rhs(ctx.handle, C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),
                                          params.nx, params.ny, params.dx, params.dy, params.gamma, bc,
-                                         int(bool(reverse)), C.c_void_p(ws.ptr), ws.nbytes, _stream(dev)))
+                                         _method(method), int(bool(reverse)), C.c_void_p(ws.ptr), ws.nbytes,
+                                         _stream(dev)))
     return out
 
 
@@ -111,7 +120,8 @@ class RunResult:
 
 
 def run(u: torch.Tensor, params: Params, boundary: str = "periodic", t_end: float | None = None,
-        max_steps: int = 10_000_000, t_start: float = 0.0, ws: Workspace | None = None) -> RunResult:
+        max_steps: int = 10_000_000, t_start: float = 0.0, ws: Workspace | None = None,
+        method: str = "js") -> RunResult:
     """Advance u in place from t_start to t_end with the device-resident Shu RK4 loop (run_from_initial's
     stopping rule)."""
     _check(u, params)
@@ -125,8 +135,8 @@ def run(u: torch.Tensor, params: Params, boundary: str = "periodic", t_end: floa
     steps, t = C.c_int(0), C.c_double(0.0)
     ctx.check(N.lib().wsr_euler2d_w7_run(
         ctx.handle, C.c_void_p(u.data_ptr()), params.nx, params.ny, params.dx, params.dy, params.gamma, params.cfl,
-        float(t_start), t_end, bc, cap, dts.ctypes.data_as(C.POINTER(C.c_double)), C.byref(steps), C.byref(t),
-        C.c_void_p(ws.ptr), ws.nbytes, _stream(dev)))
+        float(t_start), t_end, bc, _method(method), cap, dts.ctypes.data_as(C.POINTER(C.c_double)),
+        C.byref(steps), C.byref(t), C.c_void_p(ws.ptr), ws.nbytes, _stream(dev)))
     return RunResult([float(x) for x in dts[:steps.value]], steps.value, t.value)
 
 
@@ -145,8 +155,9 @@ def interior_stats(u_host: np.ndarray, params: Params) -> dict[str, float]:
 
 def run_from_initial(u0: np.ndarray, params: Params, *, device: str = "cuda", riemann_solver: str = "hllc",
                      characteristic: bool = True, report_interval: int = 0, max_steps: int = 10_000_000,
-                     boundary: str = "periodic") -> tuple[np.ndarray, dict]:
+                     boundary: str = "periodic", method: str = "js") -> tuple[np.ndarray, dict]:
     """point_rk4.run_from_initial (point_rk4.py:568-616): numpy in, (final padded state, summary) out.
+    method "z" is weno7_point_rk4_z.run_from_initial with weight_kind 1 (the reference's WENO7-Z runs).
 
     Only the characteristic HLLC configuration of the paper runs is provided; the EVILIN flux and the
     conservative-variable normal reconstruction raise NotImplementedError."""
@@ -161,7 +172,8 @@ def run_from_initial(u0: np.ndarray, params: Params, *, device: str = "cuda", ri
         dts, t, steps = [], 0.0, 0
         while t < params.t_end and steps < max_steps:
             chunk = 1 if steps == 0 else report_interval - steps % report_interval
-            res = run(u, params, boundary, max_steps=min(chunk, max_steps - steps), t_start=t, ws=ws)
+            res = run(u, params, boundary, max_steps=min(chunk, max_steps - steps), t_start=t, ws=ws,
+                      method=method)
             if res.steps == 0:
                 break
             dts += res.dts
@@ -174,7 +186,7 @@ def run_from_initial(u0: np.ndarray, params: Params, *, device: str = "cuda", ri
             if stats["nan_count"] or stats["rho_neg"] or stats["p_neg"]:
                 break
     else:
-        res = run(u, params, boundary, max_steps=max_steps, ws=ws)
+        res = run(u, params, boundary, max_steps=max_steps, ws=ws, method=method)
         dts, steps, t = res.dts, res.steps, res.t
     final = u.cpu().numpy()
     return final, {"steps": int(steps), "t": float(t), "dt_min": float(np.min(dts)) if dts else 0.0,
