@@ -834,7 +834,7 @@ void or_mlp_ratios_batch(const double *x, int n, int prec, const double *P64, co
 }
 
 /* ------------------------------------------------------------------------------------------ */
-/* 2D Euler WENO7-JS with Shu's fourth-order TVD RK (weno7_point_rk4_shu/point_rk4.py:150-616,       */
+/* 2D Euler WENO7 (JS, Z, SR) with Shu's fourth-order TVD RK (weno7_point_rk4_shu/point_rk4.py:150-616, */
 /* weno7_external_clean/warp_weno7_ader4_helpers_classical_only.py:557-855, 2147-2202).              */
 /* Padded arrays [ny+8][nx+8][4], ghost width 4, filled in place before each right-hand side.        */
 /* ------------------------------------------------------------------------------------------ */
@@ -953,15 +953,150 @@ double or_w7z_gauss(const double *q, int lr, double h) { /* weno7_gauss_lr_scala
     return w7_z_combine(q, s, d, h);
 }
 
-/* weno7_lr_vec_characteristic: Roe(q3, q4) for lr = 1, Roe(q2, q3) for lr = 2; h > 0 selects WENO-Z */
-static vec4 w7_char_face(const vec4 *q, int lr, int dir, double g, double h) {
+/* WENO7-SR: betas from the reflection-symmetric closure, evaluated by torch in the reference
+ * (teacherfree_lab_weno7_rk4_distance_balanced_fast/warp_sod/beta_provider.py:27-33, 164-219 and
+ * weno7_core.py:139-212, 266-324: features, MLP 6 -> 24 -> 16 -> 16 -> 4 with swish, 6 tanh(raw/6), softmax,
+ * averaged with the output of the reflected features; beta = 4 ratio, all ones on a plateau), then consumed by
+ * the Warp reconstruction (warp_sod/warp_weno7_external_overwrite_fullall.py:67-143: alpha = d / (beta + 1e-12)^2,
+ * w = alpha / max(sum, 1e-300)). The lr = 2 face and the second Gauss point take flip(beta(flip(q))). */
+#define W7_H1 24
+#define W7_H2 16
+#define W7_H3 16
+#define W7_NPARAM (6 * W7_H1 + W7_H1 + W7_H1 * W7_H2 + W7_H2 + W7_H2 * W7_H3 + W7_H3 + W7_H3 * 4 + 4)
+
+static void w7sr_raw(const double *P, const double *f, double *out) { /* raw_forward, weno7_core.py:311-318 */
+    const double *w1 = P, *b1 = w1 + 6 * W7_H1, *w2 = b1 + W7_H1, *b2 = w2 + W7_H1 * W7_H2, *w3 = b2 + W7_H2;
+    const double *b3 = w3 + W7_H2 * W7_H3, *w4 = b3 + W7_H3, *b4 = w4 + W7_H3 * 4;
+    double h1[W7_H1], h2[W7_H2], h3[W7_H3], z[4];
+    for (int o = 0; o < W7_H1; ++o) {
+        double a = 0.0;
+        for (int k = 0; k < 6; ++k) a += f[k] * w1[k * W7_H1 + o];
+        a += b1[o];
+        h1[o] = a * (1.0 / (1.0 + exp(-a)));
+    }
+    for (int o = 0; o < W7_H2; ++o) {
+        double a = 0.0;
+        for (int k = 0; k < W7_H1; ++k) a += h1[k] * w2[k * W7_H2 + o];
+        a += b2[o];
+        h2[o] = a * (1.0 / (1.0 + exp(-a)));
+    }
+    for (int o = 0; o < W7_H3; ++o) {
+        double a = 0.0;
+        for (int k = 0; k < W7_H2; ++k) a += h2[k] * w3[k * W7_H3 + o];
+        a += b3[o];
+        h3[o] = a * (1.0 / (1.0 + exp(-a)));
+    }
+    double m = -INFINITY, sum = 0.0;
+    for (int o = 0; o < 4; ++o) {
+        double a = 0.0;
+        for (int k = 0; k < W7_H3; ++k) a += h3[k] * w4[k * 4 + o];
+        a += b4[o];
+        z[o] = 6.0 * tanh(a / 6.0);
+        if (z[o] > m) m = z[o];
+    }
+    for (int o = 0; o < 4; ++o) {
+        z[o] = exp(z[o] - m);
+        sum += z[o];
+    }
+    for (int o = 0; o < 4; ++o) out[o] = z[o] / sum;
+}
+
+/* _mlp_beta of the beta provider on one 7-point stencil */
+void or_w7sr_beta(const double *q, const double *P, double *beta) {
+    double delta[4], dmax, qs = 1.0, g = 0.0, f[6], fr[6], ra[4], rb[4];
+    double fm[4][3] = {
+        {-2.0*q[0] + 9.0*q[1] - 18.0*q[2] + 11.0*q[3], -q[0] + 4.0*q[1] - 5.0*q[2] + 2.0*q[3], -q[0] + 3.0*q[1] - 3.0*q[2] + q[3]},
+        {q[1] - 6.0*q[2] + 3.0*q[3] + 2.0*q[4], q[2] - 2.0*q[3] + q[4], -q[1] + 3.0*q[2] - 3.0*q[3] + q[4]},
+        {-2.0*q[2] - 3.0*q[3] + 6.0*q[4] - q[5], q[2] - 2.0*q[3] + q[4], -q[2] + 3.0*q[3] - 3.0*q[4] + q[5]},
+        {-11.0*q[3] + 18.0*q[4] - 9.0*q[5] + 2.0*q[6], 2.0*q[3] - 5.0*q[4] + 4.0*q[5] - q[6], -q[3] + 3.0*q[4] - 3.0*q[5] + q[6]}};
+    for (int k = 0; k < 4; ++k)
+        delta[k] = fabs(fm[k][0]) * (1.0 / 36.0) + fabs(fm[k][1]) * (13.0 / 12.0) + fabs(fm[k][2]) * (781.0 / 720.0);
+    dmax = fmax(fmax(delta[0], delta[1]), fmax(delta[2], delta[3]));
+    for (int k = 0; k < 7; ++k) qs = fmax(qs, fabs(q[k]));
+    if (dmax <= 1.0e-13 * qs) { /* plateau_mask */
+        for (int k = 0; k < 4; ++k) beta[k] = 1.0;
+        return;
+    }
+    for (int k = 0; k < 4; ++k) f[k] = delta[k] / fmax(dmax, 1.0e-15);
+    for (int k = 0; k < 5; ++k) {
+        double d2 = q[k] - 2.0 * q[k + 1] + q[k + 2];
+        g = fmax(g, fabs(d2) / (fabs(q[k + 1] - q[k]) + fabs(q[k + 2] - q[k + 1]) + 1.0e-15));
+    }
+    f[4] = fmin(fmax(g, 0.0), 1.0);
+    f[5] = fmin(fmax((log10(fmax(dmax / qs, 1.0e-30)) + 16.0) / 16.0, 0.0), 1.0);
+    for (int k = 0; k < 4; ++k) fr[k] = f[3 - k];
+    fr[4] = f[4];
+    fr[5] = f[5];
+    w7sr_raw(P, f, ra);
+    w7sr_raw(P, fr, rb);
+    for (int k = 0; k < 4; ++k) beta[k] = 4.0 * (0.5 * (ra[k] + rb[3 - k]));
+}
+
+/* betas of side lr: lr = 1 (and Gauss point 1) the stencil itself, lr = 2 (Gauss point 2) the flipped one */
+static void w7sr_side_beta(const double *q, int lr, const double *P, double *beta) {
+    if (lr == 1) {
+        or_w7sr_beta(q, P, beta);
+        return;
+    }
+    double r[7], b[4];
+    for (int k = 0; k < 7; ++k) r[k] = q[6 - k];
+    or_w7sr_beta(r, P, b);
+    for (int k = 0; k < 4; ++k) beta[k] = b[3 - k];
+}
+
+static double w7sr_combine(const double *s, const double *d, const double *beta) { /* _weights_from_beta */
+    double ib0 = 1.0 / (beta[0] + 1.0e-12), ib1 = 1.0 / (beta[1] + 1.0e-12), ib2 = 1.0 / (beta[2] + 1.0e-12),
+           ib3 = 1.0 / (beta[3] + 1.0e-12);
+    double a0 = d[0] * ib0 * ib0, a1 = d[1] * ib1 * ib1, a2 = d[2] * ib2 * ib2, a3 = d[3] * ib3 * ib3;
+    double m = fmax(a0 + a1 + a2 + a3, 1.0e-300);
+    return a0 / m * s[0] + a1 / m * s[1] + a2 / m * s[2] + a3 / m * s[3];
+}
+
+double or_w7sr_face(const double *q, int lr, const double *P) { /* _weno7_lr_scalar_external_beta */
+    double s[4], beta[4];
+    int o = lr == 1 ? 1 : 2;
+    for (int k = 0; k < 4; ++k) s[k] = w7_face_cand(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+    double d1[4] = {1.0/35.0, 12.0/35.0, 18.0/35.0, 4.0/35.0}, d2[4] = {4.0/35.0, 18.0/35.0, 12.0/35.0, 1.0/35.0};
+    w7sr_side_beta(q, lr, P, beta);
+    return w7sr_combine(s, lr == 1 ? d1 : d2, beta);
+}
+
+double or_w7sr_gauss(const double *q, int lr, const double *P) { /* _weno7_gauss_lr_scalar_external_beta */
+    double r3 = sqrt(3.0), s[4], d[4], beta[4];
+    int o = lr == 1 ? 1 : 5;
+    for (int k = 0; k < 4; ++k) s[k] = w7_gauss_cand(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+    if (lr == 1) {
+        d[0] = 59.0/880.0 - 5.0*r3/16632.0; d[1] = 381.0/880.0 - 587.0*r3/194040.0;
+        d[2] = 381.0/880.0 + 587.0*r3/194040.0; d[3] = 59.0/880.0 + 5.0*r3/16632.0;
+    } else {
+        d[0] = 59.0/880.0 + 5.0*r3/16632.0; d[1] = 381.0/880.0 + 587.0*r3/194040.0;
+        d[2] = 381.0/880.0 - 587.0*r3/194040.0; d[3] = 59.0/880.0 - 5.0*r3/16632.0;
+    }
+    w7sr_side_beta(q, lr, P, beta);
+    return w7sr_combine(s, d, beta);
+}
+
+/* Method of a WENO7 right-hand side: kind 0 JS, 1 Z (eps = h^3 of the reconstruction direction), 2 SR with
+ * the FP64 closure P (908 packed parameters). */
+enum { W7_JS = 0, W7_Z = 1, W7_SR = 2 };
+
+static double w7_face_m(const double *s, int lr, int kind, double h, const double *P) {
+    return kind == W7_Z ? or_w7z_face(s, lr, h) : kind == W7_SR ? or_w7sr_face(s, lr, P) : or_w7_face(s, lr);
+}
+
+static double w7_gauss_m(const double *s, int lr, int kind, double h, const double *P) {
+    return kind == W7_Z ? or_w7z_gauss(s, lr, h) : kind == W7_SR ? or_w7sr_gauss(s, lr, P) : or_w7_gauss(s, lr);
+}
+
+/* weno7_lr_vec_characteristic: Roe(q3, q4) for lr = 1, Roe(q2, q3) for lr = 2 */
+static vec4 w7_char_face(const vec4 *q, int lr, int dir, double g, int kind, double h, const double *P) {
     vec4 roe = lr == 2 ? roe_average_state(q[2], q[3], g) : roe_average_state(q[3], q[4], g);
     vec4 c[7], cf;
     for (int k = 0; k < 7; ++k) c[k] = con_to_char(q[k], roe, dir, g);
     for (int f = 0; f < 4; ++f) {
         double s[7];
         for (int k = 0; k < 7; ++k) s[k] = c[k].v[f];
-        cf.v[f] = h > 0.0 ? or_w7z_face(s, lr, h) : or_w7_face(s, lr);
+        cf.v[f] = w7_face_m(s, lr, kind, h, P);
     }
     return char_to_con(cf, roe, dir, g);
 }
@@ -982,9 +1117,10 @@ static void w7_fill_bc(double *u, int nx, int ny, int bc) { /* apply_(periodic_)
         }
 }
 
-/* compute_rhs (point_rk4.py:435-511): rhs interior [ny][nx][4]. src's ghost cells are filled in place.
- * Returns 0, or -1 on allocation failure. */
-int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, double g, int bc, int reverse, int z) {
+/* compute_rhs (point_rk4.py:435-511; compute_rhs_mlp, warp_sod/point_rk4_mlp.py:198-277, for kind 2): rhs
+ * interior [ny][nx][4]. src's ghost cells are filled in place. Returns 0, or -1 on allocation failure. */
+int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, double g, int bc, int reverse, int kind,
+              const double *P) {
     int nxt = nx + 2 * G7, nyt = ny + 2 * G7;
     size_t np = (size_t)nxt * nyt * 4;
     double *xl = calloc(np, 8), *xr = calloc(np, 8), *yl = calloc(np, 8), *yr = calloc(np, 8);
@@ -997,8 +1133,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
         for (int i = 0; i < nx + 2; ++i) {
             vec4 q[7];
             for (int k = 0; k < 7; ++k) q[k] = load4(src, nxt, j, i + k);
-            store4(xl, nxt, j, i, w7_char_face(q, 2, 1, g, z ? dx : 0.0));
-            store4(xr, nxt, j, i, w7_char_face(q, 1, 1, g, z ? dx : 0.0));
+            store4(xl, nxt, j, i, w7_char_face(q, 2, 1, g, kind, dx, P));
+            store4(xr, nxt, j, i, w7_char_face(q, 1, 1, g, kind, dx, P));
         }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int j = 0; j < ny; ++j)
@@ -1011,8 +1147,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
                         a[k] = xr[((size_t)(j + 1 + k) * nxt + i) * 4 + comp];
                         b[k] = xl[((size_t)(j + 1 + k) * nxt + i + 1) * 4 + comp];
                     }
-                    sl.v[comp] = z ? or_w7z_gauss(a, loca, dy) : or_w7_gauss(a, loca);
-                    sr.v[comp] = z ? or_w7z_gauss(b, loca, dy) : or_w7_gauss(b, loca);
+                    sl.v[comp] = w7_gauss_m(a, loca, kind, dy, P);
+                    sr.v[comp] = w7_gauss_m(b, loca, kind, dy, P);
                 }
                 vec4 f = reverse ? or_hllc_flux(sr, sl, 1, g) : or_hllc_flux(sl, sr, 1, g);
                 store4(loca == 1 ? f1 : f2, nxt, j, i, f);
@@ -1022,8 +1158,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
         for (int i = 0; i < nx + 8; ++i) {
             vec4 q[7];
             for (int k = 0; k < 7; ++k) q[k] = load4(src, nxt, j + k, i);
-            store4(yl, nxt, j, i, w7_char_face(q, 2, 2, g, z ? dy : 0.0));
-            store4(yr, nxt, j, i, w7_char_face(q, 1, 2, g, z ? dy : 0.0));
+            store4(yl, nxt, j, i, w7_char_face(q, 2, 2, g, kind, dy, P));
+            store4(yr, nxt, j, i, w7_char_face(q, 1, 2, g, kind, dy, P));
         }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int j = 0; j < ny + 1; ++j)
@@ -1036,8 +1172,8 @@ int or_w7_rhs(double *src, double *rhs, int nx, int ny, double dx, double dy, do
                         a[k] = yr[((size_t)j * nxt + i + 1 + k) * 4 + comp];
                         b[k] = yl[((size_t)(j + 1) * nxt + i + 1 + k) * 4 + comp];
                     }
-                    sl.v[comp] = z ? or_w7z_gauss(a, loca, dx) : or_w7_gauss(a, loca);
-                    sr.v[comp] = z ? or_w7z_gauss(b, loca, dx) : or_w7_gauss(b, loca);
+                    sl.v[comp] = w7_gauss_m(a, loca, kind, dx, P);
+                    sr.v[comp] = w7_gauss_m(b, loca, kind, dx, P);
                 }
                 vec4 f = reverse ? or_hllc_flux(sr, sl, 2, g) : or_hllc_flux(sl, sr, 2, g);
                 store4(loca == 1 ? h1 : h2, nxt, j, i, f);
@@ -1074,8 +1210,8 @@ static double w7_max_speed(const double *u, int nx, int ny, double g) {
 
 /* run_from_initial (point_rk4.py:568-600) with launch_shu_rk4_step (514-538): u is advanced in place.
  * Returns the step count (dts receives up to max_dts values) or -1 on allocation failure. */
-int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double cfl, double t_end, int bc, int z,
-              int max_steps, double *dts, int max_dts, double *t_out) {
+int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double cfl, double t_end, int bc, int kind,
+              const double *P, int max_steps, double *dts, int max_dts, double *t_out) {
     size_t np = (size_t)(nx + 2 * G7) * (ny + 2 * G7) * 4, ni = (size_t)nx * ny * 4;
     double *u1 = calloc(np, 8), *u2 = calloc(np, 8), *u3 = calloc(np, 8);
     double *r0 = calloc(ni, 8), *rt0 = calloc(ni, 8), *r1 = calloc(ni, 8), *rt1 = calloc(ni, 8),
@@ -1090,23 +1226,23 @@ int or_w7_run(double *u, int nx, int ny, double dx, double dy, double g, double 
         if (dt <= 0.0) break;
 #define IN7(a, j, i, c) (a)[((size_t)((j) + G7) * nxt + (i) + G7) * 4 + (c)]
 #define RI7(a, j, i, c) (a)[((size_t)(j) * nx + (i)) * 4 + (c)]
-        if (or_w7_rhs(u, r0, nx, ny, dx, dy, g, bc, 0, z)) { step = -1; goto done; }
+        if (or_w7_rhs(u, r0, nx, ny, dx, dy, g, bc, 0, kind, P)) { step = -1; goto done; }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u1, j, i, c) = IN7(u, j, i, c) + 0.5 * dt * RI7(r0, j, i, c);
-        if (or_w7_rhs(u, rt0, nx, ny, dx, dy, g, bc, 1, z) || or_w7_rhs(u1, r1, nx, ny, dx, dy, g, bc, 0, z)) {
+        if (or_w7_rhs(u, rt0, nx, ny, dx, dy, g, bc, 1, kind, P) || or_w7_rhs(u1, r1, nx, ny, dx, dy, g, bc, 0, kind, P)) {
             step = -1; goto done;
         }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u2, j, i, c) = 649.0/1600.0 * IN7(u, j, i, c) - 10890423.0/25193600.0 * dt * RI7(rt0, j, i, c)
                                + 951.0/1600.0 * IN7(u1, j, i, c) + 5000.0/7873.0 * dt * RI7(r1, j, i, c);
-        if (or_w7_rhs(u1, rt1, nx, ny, dx, dy, g, bc, 1, z) || or_w7_rhs(u2, r2, nx, ny, dx, dy, g, bc, 0, z)) {
+        if (or_w7_rhs(u1, rt1, nx, ny, dx, dy, g, bc, 1, kind, P) || or_w7_rhs(u2, r2, nx, ny, dx, dy, g, bc, 0, kind, P)) {
             step = -1; goto done;
         }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u3, j, i, c) = 53989.0/2500000.0 * IN7(u, j, i, c) - 102261.0/5000000.0 * dt * RI7(rt0, j, i, c)
                                + 4806213.0/20000000.0 * IN7(u1, j, i, c) - 5121.0/20000.0 * dt * RI7(rt1, j, i, c)
                                + 23619.0/32000.0 * IN7(u2, j, i, c) + 7873.0/10000.0 * dt * RI7(r2, j, i, c);
-        if (or_w7_rhs(u3, r3, nx, ny, dx, dy, g, bc, 0, z)) { step = -1; goto done; }
+        if (or_w7_rhs(u3, r3, nx, ny, dx, dy, g, bc, 0, kind, P)) { step = -1; goto done; }
         for (int j = 0; j < ny; ++j) for (int i = 0; i < nx; ++i) for (int c = 0; c < 4; ++c)
             IN7(u, j, i, c) = 1.0/5.0 * IN7(u, j, i, c) + 1.0/10.0 * dt * RI7(r0, j, i, c)
                               + 6127.0/30000.0 * IN7(u1, j, i, c) + 1.0/6.0 * dt * RI7(r1, j, i, c)

@@ -64,14 +64,20 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_w7_gauss.argtypes = [_dp, C.c_int]
         lib.or_w7_rhs.restype = C.c_int
         lib.or_w7_rhs.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
-                                  C.c_int]
+                                  C.c_int, _dp]
+        lib.or_w7sr_beta.restype = None
+        lib.or_w7sr_beta.argtypes = [_dp, _dp, _dp]
+        lib.or_w7sr_face.restype = C.c_double
+        lib.or_w7sr_face.argtypes = [_dp, C.c_int, _dp]
+        lib.or_w7sr_gauss.restype = C.c_double
+        lib.or_w7sr_gauss.argtypes = [_dp, C.c_int, _dp]
         lib.or_w7z_face.restype = C.c_double
         lib.or_w7z_face.argtypes = [_dp, C.c_int, C.c_double]
         lib.or_w7z_gauss.restype = C.c_double
         lib.or_w7z_gauss.argtypes = [_dp, C.c_int, C.c_double]
         lib.or_w7_run.restype = C.c_int
         lib.or_w7_run.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
-                                  C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(C.c_double)]
+                                  C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int, C.POINTER(C.c_double)]
         lib.or_evilin5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_double, _dp]
         _LIBS[name] = lib
     return _LIBS[name]
@@ -238,22 +244,65 @@ def w7z_gauss(q, lr: int, h: float) -> np.ndarray:
     return np.array([_lib().or_w7z_gauss(np.ascontiguousarray(r), lr, h) for r in q])
 
 
-def w7_rhs(u, nx, ny, dx, dy, bc="periodic", reverse=False, gamma=1.4, method="js") -> np.ndarray:
-    """L(u) (or L~(u)) on the interior [ny][nx][4]; method "js" or "z" (WENO-Z, eps = h^3)."""
+W7_KIND = {"js": 0, "z": 1, "sr_f64": 2}
+N_PARAMS7 = 908
+
+
+def _w7_params(method: str, params) -> np.ndarray:
+    if method not in W7_KIND:
+        raise ValueError(f"unsupported WENO7 method {method!r}")
+    if method != "sr_f64":
+        return np.zeros(N_PARAMS7)
+    packed = pack_params(params, np.float64) if isinstance(params, dict) else np.ascontiguousarray(params, np.float64)
+    if packed.size != N_PARAMS7:
+        raise ValueError(f"WENO7 closure needs {N_PARAMS7} parameters, got {packed.size}")
+    return packed
+
+
+def w7sr_beta(q, params) -> np.ndarray:
+    """Betas of the WENO7-SR closure (the beta provider's _mlp_beta) on 7-point stencils, [n][4]."""
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    p = _w7_params("sr_f64", params)
+    out = np.zeros((q.shape[0], 4))
+    for r in range(q.shape[0]):
+        b = np.zeros(4)
+        _lib().or_w7sr_beta(np.ascontiguousarray(q[r]), p, b)
+        out[r] = b
+    return out
+
+
+def w7sr_face(q, lr: int, params) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    p = _w7_params("sr_f64", params)
+    return np.array([_lib().or_w7sr_face(np.ascontiguousarray(r), lr, p) for r in q])
+
+
+def w7sr_gauss(q, lr: int, params) -> np.ndarray:
+    q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1, 7)
+    p = _w7_params("sr_f64", params)
+    return np.array([_lib().or_w7sr_gauss(np.ascontiguousarray(r), lr, p) for r in q])
+
+
+def w7_rhs(u, nx, ny, dx, dy, bc="periodic", reverse=False, gamma=1.4, method="js", params=None) -> np.ndarray:
+    """L(u) (or L~(u)) on the interior [ny][nx][4]; method "js", "z" (WENO-Z, eps = h^3) or "sr_f64" (the
+    FP64 WENO7 closure `params`, a checkpoint dict or 908 packed values)."""
+    p = _w7_params(method, params)
     src = np.array(u, dtype=np.float64, copy=True, order="C")
     out = np.zeros((ny, nx, 4))
-    if _lib().or_w7_rhs(src, out, nx, ny, dx, dy, gamma, BC7[bc], int(bool(reverse)), int(method == "z")):
+    if _lib().or_w7_rhs(src, out, nx, ny, dx, dy, gamma, BC7[bc], int(bool(reverse)), W7_KIND[method], p):
         raise MemoryError("oracle allocation failed")
     return out
 
 
 def w7_run(u, nx, ny, dx, dy, cfl, t_end, bc="periodic", max_steps=1_000_000, gamma=1.4, fast=False,
-           method="js"):
-    """run_from_initial of the WENO7 point RK4 path. Returns (final padded state, dts, steps, t)."""
+           method="js", params=None):
+    """run_from_initial of the WENO7 point RK4 path (run_from_initial_mlp for "sr_f64"). Returns (final padded
+    state, dts, steps, t)."""
+    p = _w7_params(method, params)
     out = np.array(u, dtype=np.float64, copy=True, order="C")
     dts = np.zeros(min(max_steps, 1 << 20))
     t = C.c_double(0.0)
-    steps = _lib(fast).or_w7_run(out, nx, ny, dx, dy, gamma, cfl, t_end, BC7[bc], int(method == "z"), max_steps,
+    steps = _lib(fast).or_w7_run(out, nx, ny, dx, dy, gamma, cfl, t_end, BC7[bc], W7_KIND[method], p, max_steps,
                                  dts, dts.size, C.byref(t))
     if steps < 0:
         raise MemoryError("oracle allocation failed")

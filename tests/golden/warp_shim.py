@@ -243,6 +243,13 @@ def synchronize():
     return None
 
 
+def to_torch(arr):
+    """A torch view of the array's memory (writes through it land in the array), as wp.to_torch."""
+    import torch  # noqa: PLC0415
+
+    return torch.from_numpy(np.asarray(arr))
+
+
 class Tape:  # pragma: no cover - the differentiable paths are not exercised
     def __init__(self, *a, **k):
         raise RuntimeError("warp_shim does not implement Tape")
