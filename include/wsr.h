@@ -72,15 +72,19 @@ const char *wsr_last_error(const wsr_ctx *ctx);
  * values rounded to their precision. */
 int wsr_closure_upload(wsr_ctx *ctx, int kind, const double *packed, int n);
 
-/* ---- 2D Euler WENO7-JS with Shu's fourth-order TVD Runge-Kutta (weno7_point_rk4_shu/point_rk4.py) ----
+/* ---- 2D Euler WENO7 with Shu's fourth-order TVD Runge-Kutta (weno7_point_rk4_shu/point_rk4.py) ----
  * State: padded [ny+8][nx+8][4] FP64 conserved (ghost width 4); characteristic WENO7 normal reconstruction,
  * conservative two-point Gauss WENO7 transverse reconstruction, HLLC; boundary WSR_BC_TRANSMISSIVE or
  * WSR_BC_PERIODIC (ghost cells are derived, never read from u). */
 size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny);
 /* One right-hand side into rhs (interior [ny][nx][4]): L(u) (reverse = 0) or the downwind operator L~(u)
  * whose interface fluxes take the Gauss states in swapped order (reverse = 1); compute_rhs of
- * point_rk4.py:435-511. method: WSR_METHOD_JS (classical weights) or WSR_METHOD_Z (WENO-Z, p = 3, betas / 240,
- * eps = dx^3 along x and dy^3 along y: weno_z_borges_p2_results/weno7_point_rk4_z.py, weight_kind 1). */
+ * point_rk4.py:435-511. method: WSR_METHOD_JS (classical weights), WSR_METHOD_Z (WENO-Z, p = 3, betas / 240,
+ * eps = dx^3 along x and dy^3 along y: weno_z_borges_p2_results/weno7_point_rk4_z.py, weight_kind 1) or
+ * WSR_METHOD_SR_F64 (betas of the FP64 WENO7 closure uploaded with wsr_closure_upload(ctx, 7, ...), the lr = 2
+ * face and the second Gauss point from the flipped stencil; compute_rhs_mlp of
+ * teacherfree_lab_weno7_rk4_distance_balanced_fast/warp_sod/point_rk4_mlp.py:198-277 with eno_cutoff off).
+ * WSR_METHOD_SR_F64 without an uploaded WENO7 closure returns WSR_ERR_NO_CLOSURE. */
 int wsr_euler2d_w7_rhs(wsr_ctx *ctx, const double *u, double *rhs, int nx, int ny, double dx, double dy,
                        double gamma, int bc, int method, int reverse, void *workspace, size_t workspace_bytes,
                        void *stream);
@@ -90,6 +94,11 @@ int wsr_euler2d_w7_rhs(wsr_ctx *ctx, const double *u, double *rhs, int nx, int n
 int wsr_euler2d_w7_run(wsr_ctx *ctx, double *u, int nx, int ny, double dx, double dy, double gamma, double cfl,
                        double t_start, double t_end, int bc, int method, int max_steps, double *dts_host,
                        int *steps_out, double *t_out, void *workspace, size_t workspace_bytes, void *stream);
+/* WSR_METHOD_SR_F64 closure evaluations (stencils that ran the MLP pair) since the last wsr_euler2d_w7_rhs /
+ * wsr_euler2d_w7_run on this workspace: out_host[4] = normal x, normal y, transverse x, transverse y.
+ * Synchronous. */
+int wsr_euler2d_w7_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny,
+                            unsigned long long *out_host);
 
 /* Bytes of device workspace the 2D functions need for an nx x ny interior. */
 size_t wsr_euler2d_workspace_bytes(int nx, int ny);

@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_w7_rhs.argtypes = [vp, vp, vp, i, i, d, d, d, i, i, i, vp, sz, vp]
             L.wsr_euler2d_w7_run.argtypes = [vp, vp, i, i, d, d, d, d, d, d, i, i, i, C.POINTER(d), C.POINTER(i),
                                              C.POINTER(d), vp, sz, vp]
+            L.wsr_euler2d_w7_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
             L.wsr_euler2d_max_speed.argtypes = [vp, vp, i, i, d, C.POINTER(d), vp, sz, vp]
             L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
                                           C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
@@ -88,7 +89,7 @@ def lib() -> C.CDLL:
 def exported_symbols() -> list[str]:
     return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
             "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_stage_at", "wsr_euler2d_w7_workspace_bytes",
-            "wsr_euler2d_w7_rhs", "wsr_euler2d_w7_run", "wsr_euler2d_max_speed", "wsr_euler2d_run",
+            "wsr_euler2d_w7_rhs", "wsr_euler2d_w7_run", "wsr_euler2d_w7_counters", "wsr_euler2d_max_speed", "wsr_euler2d_run",
             "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops",
             "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
             "wsr_train1d_backward", "wsr_euler3d_workspace_bytes", "wsr_euler3d_stage", "wsr_euler3d_max_speed",

@@ -58,10 +58,10 @@ def vortex_run(n: int, method: str, mlp_params=None, device="cuda", quadrature: 
                         e0.elapsed_time(e1))
 
 
-def vortex7_run(n: int, device="cuda", quadrature: int = 15, method: str = "js") -> VortexResult:
-    """WENO7 (method "js" or "z") with Shu RK4 on the same vortex problem (the WENO7 rows of the reference's
-    convergence table: weno7_point_rk4_shu/point_rk4.py and weno7_point_rk4_z, HLLC, characteristic,
-    [-10, 10]^2, CFL 0.4, t = 2)."""
+def vortex7_run(n: int, device="cuda", quadrature: int = 15, method: str = "js", closure=None) -> VortexResult:
+    """WENO7 (method "js", "z" or "sr_f64" with the WENO7 closure `closure`) with Shu RK4 on the same vortex
+    problem (the WENO7 rows of the reference's convergence table: weno7_point_rk4_shu/point_rk4.py,
+    weno7_point_rk4_z and warp_sod/point_rk4_mlp.py, HLLC, characteristic, [-10, 10]^2, CFL 0.4, t = 2)."""
     from . import euler2d_w7 as E7  # noqa: PLC0415
 
     p = E7.Params(nx=n, ny=n, cfl=CFL, t_end=T_END)
@@ -74,7 +74,7 @@ def vortex7_run(n: int, device="cuda", quadrature: int = 15, method: str = "js")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
     e0.record(stream)
-    res = E7.run(u, p, "periodic", ws=ws, method=method)
+    res = E7.run(u, p, "periodic", ws=ws, method=method, closure=closure)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     err = u.cpu().numpy()[4:-4, 4:-4, 0] - exact[4:-4, 4:-4, 0]

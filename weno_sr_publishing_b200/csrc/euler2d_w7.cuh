@@ -1,4 +1,5 @@
-// 2D Euler WENO7-JS with Shu's fourth-order TVD Runge-Kutta (L and the downwind operator L~), sm_100a.
+// 2D Euler WENO7 (JS, Z or SR weights) with Shu's fourth-order TVD Runge-Kutta (L and the downwind operator L~),
+// sm_100a.
 //
 // Reference: weno7_point_rk4_shu/point_rk4.py:150-538 with the classical WENO7 helpers of
 // weno7_external_clean/warp_weno7_ader4_helpers_classical_only.py:557-855 (betas, face and two-point Gauss
@@ -16,6 +17,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "adv1d.cuh"
 #include "euler2d.cuh"
 
 namespace wsr {
@@ -315,6 +317,242 @@ __global__ void __launch_bounds__(kBlock7, 4) k7_flux(const double* __restrict__
 #pragma unroll
   for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] + f2.v[k];
   store_cell(fout, (size_t)j * nfx + i, o);
+}
+
+// ---------------------------------------------------------------------------------------------
+// WENO7-SR (FP64 closure). Betas come from the reflection-symmetric WENO7 MLP (6 -> 24 -> 16 -> 16 -> 4;
+// features, plateau test and model as in the 1D path), beta = 4 ratio, all ones on a plateau
+// (teacherfree_lab_weno7_rk4_distance_balanced_fast/warp_sod/beta_provider.py:27-33). The lr = 2 face value
+// and the second Gauss point take the betas of the flipped stencil, flipped back (beta_provider.py:164-219).
+// Weights alpha_k = d_k / (beta_k + 1e-12)^2, normalised by max(sum, 1e-300) with divisions
+// (warp_sod/warp_weno7_external_overwrite_fullall.py:67-143).
+//
+// Closure work is compacted per block as in the WENO5-SR kernels: phase A forms every stencil's plateau
+// test and reconstructs plateau stencils at once; the others are queued in shared memory and phase B runs
+// the MLP pair over the queue at full SIMT width. Each block adds its queue length (the closure evaluations
+// it ran) to *counters with one atomic.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ double w7sr_combine(const double s[4], const double d[4], const double b[4]) {
+  double a[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double ib = 1.0 / (b[k] + 1.0e-12);
+    a[k] = d[k] * ib * ib;
+  }
+  const double m = fmax(a[0] + a[1] + a[2] + a[3], 1.0e-300);
+  return a[0] / m * s[0] + a[1] / m * s[1] + a[2] / m * s[2] + a[3] / m * s[3];
+}
+
+// Face value of the stencil q (cells in order) for head lr with betas b.
+__device__ __forceinline__ double w7sr_face(const double q[7], int lr, const double b[4]) {
+  double s[4];
+  const int o = lr == 1 ? 1 : 2;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_face(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  const double d1[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
+  const double d2[4] = {4.0 / 35.0, 18.0 / 35.0, 12.0 / 35.0, 1.0 / 35.0};
+  return w7sr_combine(s, lr == 1 ? d1 : d2, b);
+}
+
+// Gauss-point value (loca 1 or 2) of the stencil q with betas b.
+__device__ __forceinline__ double w7sr_gauss(const double q[7], int loca, const double b[4]) {
+  double s[4];
+  constexpr double s3 = kS3;
+  const double e0 = 59.0 / 880.0, e1 = 5.0 * s3 / 16632.0, f0 = 381.0 / 880.0, f1 = 587.0 * s3 / 194040.0;
+  const double da[4] = {e0 - e1, f0 - f1, f0 + f1, e0 + e1};
+  const double db[4] = {e0 + e1, f0 + f1, f0 - f1, e0 - e1};
+  const int o = loca == 1 ? 1 : 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k] = w7_gauss(o + k, q[k], q[k + 1], q[k + 2], q[k + 3]);
+  return w7sr_combine(s, loca == 1 ? da : db, b);
+}
+
+// Closure betas of the stencil c (already in closure order: flipped for the second side); `flip` maps them
+// back to the stencil's own order.
+__device__ __forceinline__ void w7sr_betas(const double c[7], bool flip, const Mlp7d& P, double b[4]) {
+  double d[4], dmax, qs, f[6], r[4];
+  adv_plateau<7>(c, d, dmax, qs);
+  adv_features<7>(c, d, dmax, qs, f);
+  adv_ratios<7, M_SR64>(f, P, r);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) b[k] = 4.0 * (flip ? r[3 - k] : r[k]);
+}
+
+// Normal reconstruction, one thread per face, same faces and outputs as k7_normal. Stencil n = 2 f + side:
+// characteristic field f; side 0 -> cells 0..6, head lr = 1; side 1 -> cells 1..7, head lr = 2, closure on the
+// flipped cells 7..1.
+template <int DIR>
+__global__ void __launch_bounds__(kBlock7, 3) k7s_normal(const double* __restrict__ u, double* __restrict__ out_l,
+                                                        double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
+                                                        const StepCtl* __restrict__ ctl,
+                                                        unsigned long long* __restrict__ counters,
+                                                        const __grid_constant__ Mlp7d P) {
+  __shared__ double s_ch[4][8][kBlock7];
+  __shared__ double s_val[8][kBlock7];
+  __shared__ unsigned short s_q[8 * kBlock7];
+  __shared__ int s_count;
+  if (ctl->done) return;  // uniform across the launch
+  const int t = threadIdx.x;
+  const int c = DIR == 1 ? blockIdx.x * kBlock7 + t : blockIdx.x * 32 + (t & 31);
+  const int r = DIR == 1 ? blockIdx.y : blockIdx.y * 4 + (t >> 5);
+  const int nxt = nx + 2 * kG;
+  const bool active = DIR == 1 ? (r >= 1 && r < ny + 7 && c <= nx) : (r <= ny && c >= 1 && c < nx + 7);
+  if (t == 0) s_count = 0;
+  RoeJ J;
+  if (active) {
+    auto cell = [&](int k) {
+      const int pj = DIR == 1 ? r : r + k;
+      const int pi = DIR == 1 ? c + k : c;
+      return load_cell(u, nxt, map7(pj, ny, bc), map7(pi, nx, bc));
+    };
+    J = roe_jacobian(cell(3), cell(4), gas);
+    const CharL L = char_left<DIR>(J, gas);
+#pragma unroll 1
+    for (int k = 0; k < 8; ++k) {
+      const d4 qk = cell(k);
+#pragma unroll
+      for (int f = 0; f < 4; ++f) s_ch[f][k][t] = project<DIR>(L, f, qk);
+    }
+  }
+  __syncthreads();
+  // Phase A
+#pragma unroll 1
+  for (int n = 0; n < 8; ++n) {
+    const int f = n >> 1, side = n & 1;
+    bool need = false;
+    if (active) {
+      double q[7], cq[7], d[4], dmax, qs;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][t];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) cq[k] = side ? q[6 - k] : q[k];
+      need = !adv_plateau<7>(cq, d, dmax, qs);
+      if (!need) {
+        const double one[4] = {1.0, 1.0, 1.0, 1.0};
+        s_val[n][t] = w7sr_face(q, side + 1, one);
+      }
+    }
+    queue_push(need, n * kBlock7 + t, s_q, &s_count);
+  }
+  __syncthreads();
+  // Phase B
+  const int count = s_count;
+#pragma unroll 1
+  for (int e = t; e < count; e += kBlock7) {
+    const int id = s_q[e];
+    const int n = id / kBlock7, o = id % kBlock7, f = n >> 1, side = n & 1;
+    double q[7], cq[7], b[4];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][o];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) cq[k] = side ? q[6 - k] : q[k];
+    w7sr_betas(cq, side == 1, P, b);
+    s_val[n][o] = w7sr_face(q, side + 1, b);
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const double cf[4] = {s_val[side][t], s_val[2 + side][t], s_val[4 + side][t], s_val[6 + side][t]};
+      const d4 face = char_to_con<DIR>(cf, J);
+      const size_t idx = DIR == 1 ? (size_t)r * (nx + 2) + c + side : (size_t)(r + side) * (nx + 8) + c;
+      store_cell(side == 0 ? out_r : out_l, idx, face);
+    }
+  }
+  if (t == 0 && count) atomicAdd(counters, (unsigned long long)count);
+}
+
+// Transverse stencil m = 2 comp + side of face (i, j) (side 0: u_L from fr, side 1: u_R from fl), the
+// layout of k7_flux.
+template <int DIR>
+__device__ __forceinline__ void w7_load_transverse(const double* __restrict__ fl, const double* __restrict__ fr,
+                                                   int nx, int i, int j, int m, double q[7]) {
+  const int comp = m >> 1, side = m & 1;
+  const double* src = side == 0 ? fr : fl;
+  if (DIR == 1) {
+    const int ncols = nx + 2, col = side == 0 ? i : i + 1;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) q[k] = __ldg(src + ((size_t)(j + 1 + k) * ncols + col) * 4 + comp);
+  } else {
+    const int ncols = nx + 8, row = side == 0 ? j : j + 1;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) q[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
+  }
+}
+
+// Transverse reconstruction and flux, one thread per face, same faces and outputs as k7_flux. Job
+// n = 2 m + gp: transverse stencil m, Gauss point gp + 1 (the second from the flipped stencil's closure).
+template <int DIR>
+__global__ void __launch_bounds__(kBlock7, 3) k7s_flux(const double* __restrict__ fl, const double* __restrict__ fr,
+                                                      double* __restrict__ fout, int nx, int ny, Gas gas, int reverse,
+                                                      const StepCtl* __restrict__ ctl,
+                                                      unsigned long long* __restrict__ counters,
+                                                      const __grid_constant__ Mlp7d P) {
+  __shared__ double s_g[16][kBlock7];
+  __shared__ unsigned short s_q[16 * kBlock7];
+  __shared__ int s_count;
+  if (ctl->done) return;  // uniform across the launch
+  const int t = threadIdx.x;
+  auto face_i = [&](int th) { return DIR == 1 ? (int)blockIdx.x * 32 + (th & 31) : (int)blockIdx.x * kBlock7 + th; };
+  auto face_j = [&](int th) { return DIR == 1 ? (int)blockIdx.y * 4 + (th >> 5) : (int)blockIdx.y; };
+  const int i = face_i(t), j = face_j(t);
+  const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
+  const bool active = i < nfx && j < nfy;
+  if (t == 0) s_count = 0;
+  __syncthreads();
+  // Phase A
+#pragma unroll 1
+  for (int m = 0; m < 8; ++m) {
+    double q[7];
+    if (active) w7_load_transverse<DIR>(fl, fr, nx, i, j, m, q);
+#pragma unroll 1
+    for (int gp = 0; gp < 2; ++gp) {
+      bool need = false;
+      if (active) {
+        double cq[7], d[4], dmax, qs;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) cq[k] = gp ? q[6 - k] : q[k];
+        need = !adv_plateau<7>(cq, d, dmax, qs);
+        if (!need) {
+          const double one[4] = {1.0, 1.0, 1.0, 1.0};
+          s_g[2 * m + gp][t] = w7sr_gauss(q, gp + 1, one);
+        }
+      }
+      queue_push(need, (2 * m + gp) * kBlock7 + t, s_q, &s_count);
+    }
+  }
+  __syncthreads();
+  // Phase B
+  const int count = s_count;
+#pragma unroll 1
+  for (int e = t; e < count; e += kBlock7) {
+    const int id = s_q[e];
+    const int n = id / kBlock7, o = id % kBlock7, m = n >> 1, gp = n & 1;
+    double q[7], cq[7], b[4];
+    w7_load_transverse<DIR>(fl, fr, nx, face_i(o), face_j(o), m, q);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) cq[k] = gp ? q[6 - k] : q[k];
+    w7sr_betas(cq, gp == 1, P, b);
+    s_g[n][o] = w7sr_gauss(q, gp + 1, b);
+  }
+  __syncthreads();
+  if (active) {
+    d4 l1, l2, r1, r2;
+#pragma unroll
+    for (int comp = 0; comp < 4; ++comp) {
+      l1.v[comp] = s_g[4 * comp + 0][t];
+      l2.v[comp] = s_g[4 * comp + 1][t];
+      r1.v[comp] = s_g[4 * comp + 2][t];
+      r2.v[comp] = s_g[4 * comp + 3][t];
+    }
+    const d4 f1 = reverse ? hllc_flux<DIR>(r1, l1, gas) : hllc_flux<DIR>(l1, r1, gas);
+    const d4 f2 = reverse ? hllc_flux<DIR>(r2, l2, gas) : hllc_flux<DIR>(l2, r2, gas);
+    d4 o;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) o.v[k] = f1.v[k] + f2.v[k];
+    store_cell(fout, (size_t)j * nfx + i, o);
+  }
+  if (t == 0 && count) atomicAdd(counters, (unsigned long long)count);
 }
 
 // rhs[j][i] = -1/2 (f[j][i+1] - f[j][i]) / dx - 1/2 (g[j+1][i] - g[j][i]) / dy (point_rk4.py:290-312).

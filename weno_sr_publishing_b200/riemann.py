@@ -241,9 +241,9 @@ def _run_padded(init: np.ndarray, p: Params, t_end: float, method: str, mlp_para
     return final[3:3 + p.ny, 3:3 + p.nx], res, e0.elapsed_time(e1)
 
 
-def _run_w7(tube: ShockTube, gamma: float, device, method: str = "js") -> tuple:
-    """WENO7 (JS or Z weights) with Shu RK4 on the tube, ghost width 4 (the WENO7 runs of run_sod.py:86-99 and
-    run_shock_tube_benchmark.py:127-177)."""
+def _run_w7(tube: ShockTube, gamma: float, device, method: str = "js", closure=None) -> tuple:
+    """WENO7 (JS, Z or SR-FP64 weights) with Shu RK4 on the tube, ghost width 4 (the WENO7 runs of
+    run_sod.py:86-99 and run_shock_tube_benchmark.py:127-177)."""
     dx = (tube.x_max - tube.x_min) / tube.nx
     p = E7.Params(nx=tube.nx, ny=tube.ny, x_min=tube.x_min, x_max=tube.x_max, y_min=0.0, y_max=tube.ny * dx,
                   gamma=gamma, cfl=tube.cfl, t_end=tube.t_end)
@@ -252,7 +252,7 @@ def _run_w7(tube: ShockTube, gamma: float, device, method: str = "js") -> tuple:
     stream = torch.cuda.current_stream(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    res = E7.run(u, p, "transmissive", method=method)
+    res = E7.run(u, p, "transmissive", method=method, closure=closure)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     return u.cpu().numpy()[4:4 + tube.ny, 4:4 + tube.nx], res, e0.elapsed_time(e1)
@@ -260,11 +260,11 @@ def _run_w7(tube: ShockTube, gamma: float, device, method: str = "js") -> tuple:
 
 def shock_tube_run(tube: ShockTube, method: str, mlp_params=None, device="cuda", gamma: float = 1.4) -> dict:
     """Run the tube on the GPU to t_end and compare the y-averaged solution with the exact cell averages.
-    method: a WENO5 method of the 2D path ("js", "z", "sr_f64", ...), "w7_js" or "w7_z" (WENO7-JS or
-    WENO7-Z, Shu RK4)."""
+    method: a WENO5 method of the 2D path ("js", "z", "sr_f64", ...), "w7_js", "w7_z" or "w7_sr_f64" (WENO7-JS,
+    WENO7-Z or WENO7-SR with the WENO7 closure `mlp_params`, Shu RK4)."""
     p = tube_params(tube, gamma)
-    if method in ("w7_js", "w7_z"):
-        state, res, ms = _run_w7(tube, gamma, device, method[3:])
+    if method in ("w7_js", "w7_z", "w7_sr_f64"):
+        state, res, ms = _run_w7(tube, gamma, device, method[3:], mlp_params)
     else:
         state, res, ms = _run_padded(tube_initial_state(tube, gamma), p, tube.t_end, method, mlp_params, device)
     conserved = state.mean(axis=0)
