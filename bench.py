@@ -59,6 +59,8 @@ def parse():
                     help="euler2d: the headline 2D step; adv1d: 4096 ragged 1D trajectories; train1d: closure "
                          "training steps (B=1024, N=256); euler3d: the 224x88x88 shock-bubble step")
     ap.add_argument("--scheme", type=int, default=5, choices=[5, 7], help="adv1d: WENO5/SSPRK3 or WENO7/Shu RK4")
+    ap.add_argument("--w7-method", default="js", choices=["js", "z", "sr_f64"],
+                    help="euler2d_w7: WENO7-JS, WENO7-Z or WENO7-SR (FP64 closure)")
     return ap.parse_args()
 
 
@@ -681,8 +683,9 @@ def _oracle3d_sample(sb_seed, method, params, budget_s):
 
 
 def bench_w7(args, world, rank, local):
-    """WENO7-JS 2D with Shu RK4 on the periodic isentropic vortex (the reference's point_rk4 path) at
-    args.n^2 (default 1024 when the 2D default 2000 is given), K steps from t = 0."""
+    """WENO7 2D (JS, Z or SR-FP64 weights, --w7-method) with Shu RK4 on the periodic isentropic vortex (the
+    reference's point_rk4 / point_rk4_z / point_rk4_mlp paths) at args.n^2 (default 1024 when the 2D default
+    2000 is given), K steps from t = 0."""
     import torch
     import torch.distributed as dist
 
@@ -690,9 +693,16 @@ def bench_w7(args, world, rank, local):
     from weno_sr_publishing_b200 import euler2d_w7 as E7
     from weno_sr_publishing_b200 import problems as PR
     n = 1024 if args.n == 2000 else args.n
-    metric = f"2D Euler cell-updates/s, WENO7-JS Shu RK4, {n}x{n} isentropic vortex"
+    method = args.w7_method
+    label = {"js": "WENO7-JS", "z": "WENO7-Z", "sr_f64": "WENO7-SR (FP64 closure)"}[method]
+    closure = params = None
+    if method == "sr_f64":
+        from weno_sr_publishing_b200.checkpoint import MODELS_DIR
+        params = {k: v for k, v in np.load(MODELS_DIR / "weno7_sr_fp64_step016750.npz").items() if k != "meta_json"}
+        closure = params
+    metric = f"2D Euler cell-updates/s, {label} Shu RK4, {n}x{n} isentropic vortex"
     cfg = {"workload": f"2D periodic isentropic vortex {n}x{n} on [-10,10]^2 (2x2 Gauss averages), from t=0",
-           "scheme": "WENO7-JS characteristic + two-point Gauss transverse", "flux": "hllc",
+           "scheme": f"{label} characteristic + two-point Gauss transverse", "flux": "hllc",
            "time_integrator": "Shu RK4 (L and L~)", "cfl": 0.4, "state_precision": "fp64",
            "l2_policy": f"state {(n + 8) ** 2 * 32 / 1e6:.0f} MB, workspace {(n * n * 32 * 14) / 1e6:.0f} MB",
            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
@@ -705,7 +715,8 @@ def bench_w7(args, world, rank, local):
         pm = E7.Params(nx=m, ny=m)
         steps, t0 = 0, time.perf_counter()
         while time.perf_counter() - t0 < args.cpu_seconds:
-            _, _, k, _ = O.w7_run(small, m, m, pm.dx, pm.dy, 0.4, 100.0, "periodic", max_steps=1, fast=True)
+            _, _, k, _ = O.w7_run(small, m, m, pm.dx, pm.dy, 0.4, 100.0, "periodic", max_steps=1, fast=True,
+                                  method=method, params=params)
             steps += k
         el = time.perf_counter() - t0
         return {"value": m * m * steps / el, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
@@ -732,7 +743,7 @@ def bench_w7(args, world, rank, local):
     ws = E7.workspace(n, n, dev)
     u = u0.clone()
     if W:
-        E7.run(u, p, "periodic", max_steps=W, ws=ws)
+        E7.run(u, p, "periodic", max_steps=W, ws=ws, method=method, closure=closure)
     u.copy_(u0)
     if world > 1:
         dist.barrier()
@@ -741,10 +752,11 @@ def bench_w7(args, world, rank, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         e0.record(stream)
-        res = E7.run(u, p, "periodic", max_steps=K, ws=ws)
+        res = E7.run(u, p, "periodic", max_steps=K, ws=ws, method=method, closure=closure)
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    counts = E7.closure_counts(ws, p) if method == "sr_f64" else None
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -754,6 +766,8 @@ def bench_w7(args, world, rank, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "clocks": clk.summary(), "gpu_launches": 1 + res.steps * (3 + 6 * 5 + 4),
             "state_finite": bool(torch.isfinite(u).all())}
+    if counts is not None:
+        line["closures_per_step"] = {k: v / max(res.steps, 1) for k, v in counts.items()}
     if not args.skip_extras:
         host = torch.empty(u0.shape, dtype=torch.float64, pin_memory=True)
         host.copy_(u0.cpu())
@@ -761,7 +775,7 @@ def bench_w7(args, world, rank, local):
         t0 = time.perf_counter()
         for _ in range(K):  # each step: pinned state in, one step, state out
             u.copy_(host, non_blocking=True)
-            E7.run(u, p, "periodic", max_steps=1, ws=ws)
+            E7.run(u, p, "periodic", max_steps=1, ws=ws, method=method, closure=closure)
             host.copy_(u, non_blocking=True)
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
