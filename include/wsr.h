@@ -238,6 +238,9 @@ int wsr_euler2d_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, 
 
 /* Measured FMA throughput of this GPU in TFLOP/s (bits = 32 or 64; 2 flops per FMA). */
 int wsr_probe_peak_flops(wsr_ctx *ctx, int bits, double *tflops, void *stream);
+/* The table-driven FP64 exponential of the WENO7-SR closure on n device values (out[i] = exp(x[i]), arguments
+ * clamped to [-700, 700]); for checking it against the CUDA math library. */
+int wsr_probe_exp_tab(wsr_ctx *ctx, const double *x, double *out, int n, void *stream);
 
 /* ---- stage without any allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc (a host that owns all device memory through its own pool,

@@ -166,3 +166,28 @@ def test_sod_and_lax_tables(beta):
     for field, ref in lax.items():
         for got, rv in zip((r[f"{field}_l1_mean"], r[f"{field}_l2"], r[f"{field}_linf"]), ref):
             assert abs(got / rv - 1.0) <= 1e-9, (field, got, rv)
+
+
+def test_table_exponential_against_cuda_exp():
+    """The closure's table-driven exp (Tang's method) against CUDA's exp (torch.exp on the device): within
+    2 ulp over the closure's argument range, exact at 0, monotone across table boundaries."""
+    from weno_sr_publishing_b200.binary_io import ulp_distance
+
+    rng = np.random.default_rng(7)
+    x = np.concatenate([rng.uniform(-40, 40, 200000), rng.uniform(-700, 700, 50000), np.linspace(-1, 1, 20001),
+                        np.arange(-64, 65) * np.log(2) / 32, [0.0, -700.0, 700.0]])
+    xd = torch.as_tensor(x, device=DEV)
+    out = torch.empty_like(xd)
+    ctx = N.context(0)
+    ctx.check(N.lib().wsr_probe_exp_tab(ctx.handle, C.c_void_p(xd.data_ptr()), C.c_void_p(out.data_ptr()), x.size,
+                                        None))
+    torch.cuda.synchronize()
+    got, ref = out.cpu().numpy(), torch.exp(xd).cpu().numpy()
+    assert int(ulp_distance(got, ref).max()) <= 2
+    assert got[x == 0.0][0] == 1.0
+    s = np.sort(x)
+    xs = torch.as_tensor(s, device=DEV)
+    ys = torch.empty_like(xs)
+    ctx.check(N.lib().wsr_probe_exp_tab(ctx.handle, C.c_void_p(xs.data_ptr()), C.c_void_p(ys.data_ptr()), s.size,
+                                        None))
+    assert np.all(np.diff(ys.cpu().numpy()) >= 0)

@@ -82,6 +82,7 @@ def lib() -> C.CDLL:
             L.wsr_profile_read.argtypes = [vp, C.POINTER(d), C.POINTER(C.c_longlong)]
             L.wsr_euler2d_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
             L.wsr_probe_peak_flops.argtypes = [vp, i, C.POINTER(d), vp]
+            L.wsr_probe_exp_tab.argtypes = [vp, vp, vp, i, vp]
             _lib = L
     return _lib
 
@@ -90,7 +91,7 @@ def exported_symbols() -> list[str]:
     return ["wsr_ctx_create", "wsr_ctx_destroy", "wsr_last_error", "wsr_closure_upload",
             "wsr_euler2d_workspace_bytes", "wsr_euler2d_stage", "wsr_euler2d_stage_at", "wsr_euler2d_w7_workspace_bytes",
             "wsr_euler2d_w7_rhs", "wsr_euler2d_w7_run", "wsr_euler2d_w7_counters", "wsr_euler2d_max_speed", "wsr_euler2d_run",
-            "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops",
+            "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops", "wsr_probe_exp_tab",
             "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
             "wsr_train1d_backward", "wsr_euler3d_workspace_bytes", "wsr_euler3d_stage", "wsr_euler3d_max_speed",
             "wsr_euler3d_run", "wsr_euler3d_counters", "wsr_euler2d_stage_noalloc"]

@@ -367,15 +367,122 @@ __device__ __forceinline__ double w7sr_gauss(const double q[7], int loca, const 
   return w7sr_combine(s, loca == 1 ? da : db, b);
 }
 
+// FP64 exponential of the closure's swish and softmax, after Tang's table-driven method (P. T. P. Tang,
+// ACM TOMS 15(2), 1989): x = (32 m + j) ln2/32 + r with |r| <= ln2/64, exp(x) = 2^m 2^(j/32) (1 + p(r)), p the
+// degree-6 Taylor polynomial of e^r - 1 (truncation below 4e-18 on that interval), ln2/32 split in two parts for
+// the reduction. t32[j] = 2^(j/32) rounded to double (kExp2_32, copied to shared memory by each block). Error
+// about 1 ulp; arguments are clamped to [-700, 700], which keeps every result normal (the swish of an argument
+// beyond that range is z or 0 to within 1e-300).
+__constant__ double kExp2_32[32] = {
+    1.0, 1.0218971486541166, 1.0442737824274138, 1.0671404006768237,
+    1.0905077326652577, 1.1143867425958924, 1.1387886347566916, 1.1637248587775775,
+    1.189207115002721, 1.215247359980469, 1.241857812073484, 1.2690509571917332,
+    1.2968395546510096, 1.3252366431597413, 1.3542555469368927, 1.383909881963832,
+    1.4142135623730951, 1.4451808069770467, 1.4768261459394993, 1.5091644275934228,
+    1.5422108254079407, 1.5759808451078865, 1.6104903319492543, 1.645755478153965,
+    1.681792830507429, 1.718619298122478, 1.7562521603732995, 1.7947090750031072,
+    1.8340080864093424, 1.8741676341103, 1.9152065613971474, 1.9571441241754002};
+
+__device__ __forceinline__ double exp_tab(double x, const double* __restrict__ t32) {
+  x = fmin(fmax(x, -700.0), 700.0);
+  constexpr double kShift = 6755399441055744.0;  // 1.5 * 2^52: x 32/ln2 + kShift holds round(x 32/ln2) in its low word
+  constexpr double kInvL = 46.16624130844683, kL1 = 0.02166084939249829, kL2 = 7.247021293269686e-19;
+  const double kd = fma(x, kInvL, kShift);
+  const int n = __double2loint(kd);
+  const double nd = kd - kShift;
+  double r = fma(nd, -kL1, x);
+  r = fma(nd, -kL2, r);
+  double p = fma(r, 1.0 / 720.0, 1.0 / 120.0);
+  p = fma(p, r, 1.0 / 24.0);
+  p = fma(p, r, 1.0 / 6.0);
+  p = fma(p, r, 0.5);
+  p = fma(p, r, 1.0);
+  p = p * r;
+  const double tj = t32[n & 31];
+  const double e = fma(tj, p, tj);
+  return __hiloint2double(__double2hiint(e) + ((n >> 5) << 20), __double2loint(e));
+}
+
+__device__ __forceinline__ double swish_tab(double z, const double* __restrict__ t32) {
+  return z * rcp64(1.0 + exp_tab(-z, t32));
+}
+
+// Dense layer of the WENO7 MLP for the direct (xa) and reflected (xb) inputs together; packed [in][out]
+// weights followed by the biases (the layout of the 1D path).
+template <int NI, int NO>
+__device__ __forceinline__ void w7sr_dense_pair(const double* __restrict__ P, int w, int b, const double* xa,
+                                                const double* xb, double* ya, double* yb, bool act,
+                                                const double* __restrict__ t32) {
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    double za = P[b + o], zb = P[b + o];
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+      za = za + xa[k] * P[w + k * NO + o];
+      zb = zb + xb[k] * P[w + k * NO + o];
+    }
+    ya[o] = act ? swish_tab(za, t32) : za;
+    yb[o] = act ? swish_tab(zb, t32) : zb;
+  }
+}
+
+// MLP 6 -> 24 -> 16 -> 16 -> 4 (swish, swish, swish, 6 tanh(raw/6), softmax; weno7_core.py:311-318) on the
+// direct and reflected features, ratios out.
+__device__ __forceinline__ void w7sr_pair(const double* __restrict__ P, const double* __restrict__ t32,
+                                          const double xa[6], const double xb[6], double ra[4], double rb[4]) {
+  using D = MlpDims<6, 24, 16, 16, 4>;
+  double a1[24], b1[24], a2[16], b2[16], a3[16], b3[16], za[4], zb[4];
+  w7sr_dense_pair<6, 24>(P, D::W1, D::B1, xa, xb, a1, b1, true, t32);
+  w7sr_dense_pair<24, 16>(P, D::W2, D::B2, a1, b1, a2, b2, true, t32);
+  w7sr_dense_pair<16, 16>(P, D::W3, D::B3, a2, b2, a3, b3, true, t32);
+  w7sr_dense_pair<16, 4>(P, D::W4, D::B4, a3, b3, za, zb, false, t32);
+  double ma = -1e30, mb = -1e30;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    za[o] = 6.0 * tanh(div6(za[o]));
+    zb[o] = 6.0 * tanh(div6(zb[o]));
+    ma = za[o] > ma ? za[o] : ma;
+    mb = zb[o] > mb ? zb[o] : mb;
+  }
+  double sa = 0.0, sb = 0.0;
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    za[o] = exp_tab(za[o] - ma, t32);
+    zb[o] = exp_tab(zb[o] - mb, t32);
+    sa = sa + za[o];
+    sb = sb + zb[o];
+  }
+  const double ia = rcp64(sa), ib = rcp64(sb);
+#pragma unroll
+  for (int o = 0; o < 4; ++o) {
+    ra[o] = za[o] * ia;
+    rb[o] = zb[o] * ib;
+  }
+}
+
 // Closure betas of the stencil c (already in closure order: flipped for the second side); `flip` maps them
-// back to the stencil's own order.
-__device__ __forceinline__ void w7sr_betas(const double c[7], bool flip, const Mlp7d& P, double b[4]) {
-  double d[4], dmax, qs, f[6], r[4];
+// back to the stencil's own order. beta = 4 (direct + reflect(reflected)) / 2 (weno7_core.py:320-324).
+__device__ __forceinline__ void w7sr_betas(const double c[7], bool flip, const Mlp7d& P,
+                                           const double* __restrict__ t32, double b[4]) {
+  double d[4], dmax, qs, f[6], ra[4], rb[4];
   adv_plateau<7>(c, d, dmax, qs);
   adv_features<7>(c, d, dmax, qs, f);
-  adv_ratios<7, M_SR64>(f, P, r);
+  const double fr[6] = {f[3], f[2], f[1], f[0], f[4], f[5]};
+  w7sr_pair(P.p, t32, f, fr, ra, rb);
 #pragma unroll
-  for (int k = 0; k < 4; ++k) b[k] = 4.0 * (flip ? r[3 - k] : r[k]);
+  for (int k = 0; k < 4; ++k) {
+    const int o = flip ? 3 - k : k;
+    b[k] = 4.0 * (0.5 * (ra[o] + rb[3 - o]));
+  }
+}
+
+// exp_tab over an array (the probe that checks it against CUDA's exp).
+__global__ void k_probe_exp_tab(const double* __restrict__ x, double* __restrict__ out, int n) {
+  __shared__ double t32[32];
+  if (threadIdx.x < 32) t32[threadIdx.x] = kExp2_32[threadIdx.x];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = exp_tab(x[i], t32);
 }
 
 // Normal reconstruction, one thread per face, same faces and outputs as k7_normal. Stencil n = 2 f + side:
@@ -389,10 +496,12 @@ __global__ void __launch_bounds__(kBlock7, 3) k7s_normal(const double* __restric
                                                         const __grid_constant__ Mlp7d P) {
   __shared__ double s_ch[4][8][kBlock7];
   __shared__ double s_val[8][kBlock7];
+  __shared__ double s_t32[32];
   __shared__ unsigned short s_q[8 * kBlock7];
   __shared__ int s_count;
   if (ctl->done) return;  // uniform across the launch
   const int t = threadIdx.x;
+  if (t < 32) s_t32[t] = kExp2_32[t];
   const int c = DIR == 1 ? blockIdx.x * kBlock7 + t : blockIdx.x * 32 + (t & 31);
   const int r = DIR == 1 ? blockIdx.y : blockIdx.y * 4 + (t >> 5);
   const int nxt = nx + 2 * kG;
@@ -446,7 +555,7 @@ __global__ void __launch_bounds__(kBlock7, 3) k7s_normal(const double* __restric
     for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][o];
 #pragma unroll
     for (int k = 0; k < 7; ++k) cq[k] = side ? q[6 - k] : q[k];
-    w7sr_betas(cq, side == 1, P, b);
+    w7sr_betas(cq, side == 1, P, s_t32, b);
     s_val[n][o] = w7sr_face(q, side + 1, b);
   }
   __syncthreads();
@@ -489,10 +598,12 @@ __global__ void __launch_bounds__(kBlock7, 3) k7s_flux(const double* __restrict_
                                                       unsigned long long* __restrict__ counters,
                                                       const __grid_constant__ Mlp7d P) {
   __shared__ double s_g[16][kBlock7];
+  __shared__ double s_t32[32];
   __shared__ unsigned short s_q[16 * kBlock7];
   __shared__ int s_count;
   if (ctl->done) return;  // uniform across the launch
   const int t = threadIdx.x;
+  if (t < 32) s_t32[t] = kExp2_32[t];
   auto face_i = [&](int th) { return DIR == 1 ? (int)blockIdx.x * 32 + (th & 31) : (int)blockIdx.x * kBlock7 + th; };
   auto face_j = [&](int th) { return DIR == 1 ? (int)blockIdx.y * 4 + (th >> 5) : (int)blockIdx.y; };
   const int i = face_i(t), j = face_j(t);
@@ -532,7 +643,7 @@ __global__ void __launch_bounds__(kBlock7, 3) k7s_flux(const double* __restrict_
     w7_load_transverse<DIR>(fl, fr, nx, face_i(o), face_j(o), m, q);
 #pragma unroll
     for (int k = 0; k < 7; ++k) cq[k] = gp ? q[6 - k] : q[k];
-    w7sr_betas(cq, gp == 1, P, b);
+    w7sr_betas(cq, gp == 1, P, s_t32, b);
     s_g[n][o] = w7sr_gauss(q, gp + 1, b);
   }
   __syncthreads();

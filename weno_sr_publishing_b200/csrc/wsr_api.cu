@@ -976,6 +976,15 @@ extern "C" int wsr_euler2d_w7_counters(wsr_ctx* ctx, void* workspace, size_t wor
   return WSR_OK;
 }
 
+extern "C" int wsr_probe_exp_tab(wsr_ctx* ctx, const double* x, double* out, int n, void* stream) {
+  if (!ctx || !x || !out || n < 0) return WSR_ERR_ARG;
+  if (n == 0) return WSR_OK;
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  w7::k_probe_exp_tab<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(x, out, n);
+  WSR_LAUNCHED(ctx, "k_probe_exp_tab");
+  return WSR_OK;
+}
+
 extern "C" int wsr_probe_peak_flops(wsr_ctx* ctx, int bits, double* tflops, void* stream) {
   if (!ctx || !tflops || (bits != 32 && bits != 64)) return WSR_ERR_ARG;
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
