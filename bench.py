@@ -59,6 +59,10 @@ def parse():
                     help="euler2d: the headline 2D step; adv1d: 4096 ragged 1D trajectories; train1d: closure "
                          "training steps (B=1024, N=256); euler3d: the 224x88x88 shock-bubble step")
     ap.add_argument("--scheme", type=int, default=5, choices=[5, 7], help="adv1d: WENO5/SSPRK3 or WENO7/Shu RK4")
+    ap.add_argument("--decomp", default="auto", choices=["auto", "slabs", "replicas"],
+                    help="euler2d on N ranks: slabs = the one n x n grid cut into y-slabs with a 3-row halo "
+                         "exchange per stage and a MAX all-reduce per step (strong scaling); replicas = N "
+                         "independent copies (weak scaling); auto = slabs when N > 1")
     ap.add_argument("--w7-method", default="js", choices=["js", "z", "sr_f64"],
                     help="euler2d_w7: WENO7-JS, WENO7-Z or WENO7-SR (FP64 closure)")
     return ap.parse_args()
@@ -226,9 +230,13 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
+    slabs = args.decomp == "slabs" or (args.decomp == "auto" and world > 1)
+    if world > 1 or slabs:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev, rank=rank,
+                                world_size=world)
     n, K, W = args.n, args.steps, max(args.warmup, 0)
     p = Params(nx=n, ny=n, x_length=1.0, y_length=1.0, cfl=0.4)
     mlp = None
@@ -264,20 +272,47 @@ def main():
             ms = float(t.item())
         return ms, r
 
+    if slabs:
+        from weno_sr_publishing_b200 import slabs2d as S
+        sp = S.slab_params(p, world, rank)
+        comm = S.DistSlabs()
+
+        def timed_slabs(method, prm, steps, warm):
+            stages = S.CudaStages(method, prm)
+            slab = S.split(start, p, world, rank)
+            if warm:
+                slab = S.run([slab], [sp], 1.0e30, "transmissive", comm, stages, max_steps=warm).slabs[0]
+            dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = S.run([slab], [sp], 1.0e30, "transmissive", comm, stages, max_steps=steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = torch.tensor([e0.elapsed_time(e1)], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item()), r
+
     with ClockSampler(local) as clk:
-        ms, r = timed(args.method, mlp, K, W)
+        ms, r = timed_slabs(args.method, mlp, K, W) if slabs else timed(args.method, mlp, K, W)
     clocks = clk.summary()
-    value = world * n * n * K / (ms * 1e-3)
+    units = n * n if slabs else world * n * n  # slabs: the one grid's cell updates (strong scaling)
+    value = units * K / (ms * 1e-3)
+    cfg = workload_config(args, world)
+    if slabs:
+        cfg["parallelism"] = (f"y-slabs x{world}: rank r owns rows of the one {n}x{n} grid, 3-row halo exchange "
+                              f"per stage (NCCL send/recv), MAX all-reduce of the wave speed per step")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": workload_config(args, world), "clocks": clocks}
-    # per step: dt kernels (2), 3 stages x 5 kernels, t/steps update (1); plus init and max-speed per run
-    line["gpu_launches"] = 2 + K * (3 + 3 * 5)
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong" if slabs else "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg, "clocks": clocks}
+    # device loop, per step: dt kernels (2), 3 stages x 5 kernels, t/steps update (1); plus init and max speed.
+    # slabs, per step: max speed (1), 3 stages x (control init + 5 kernels)
+    line["gpu_launches"] = K * (1 + 3 * 6) if slabs else 2 + K * (3 + 3 * 5)
 
     if not args.skip_extras:
         # WENO5-JS on the same state and steps: the cost ratio of the learned closure
-        ms_js, _ = timed("js", None, K, W)
-        line["js"] = {"value": world * n * n * K / (ms_js * 1e-3), "ms_per_step": ms_js / K,
+        ms_js, _ = timed_slabs("js", None, K, W) if slabs else timed("js", None, K, W)
+        line["js"] = {"value": units * K / (ms_js * 1e-3), "ms_per_step": ms_js / K,
                       "sr_over_js_cost": (ms / K) / (ms_js / K)}
 
     # per-kernel device time (CUDA events around each launch) and closure tallies for the roofline
@@ -324,12 +359,44 @@ def main():
             wk = R.kernel_work(k, args.method, n, n, mlp_n / 3.0, plat_n / 3.0)
             for key in step_work:
                 step_work[key] += 3 * wk[key]
+    if slabs:  # each rank does its slab's share of the grid's work in the job's step time
+        step_work = {k: v / world for k, v in step_work.items()}
     line["roofline_step"] = R.bound(step_work, ms / K * 1e-3, peak32, peak64, hbm["gbs"])
     line["kernels"] = {k: {kk: v[kk] for kk in ("ms_per_launch", "launches", "share", "bound", "frac")}
                        for k, v in per_kernel.items()}
     line["closure_tally_per_step"] = {k: {"mlp": v[0], "plateau": v[1]} for k, v in tallies.items()}
 
-    if not args.skip_extras:
+    if not args.skip_extras and slabs:
+        # end to end per rank: pinned host slab -> device, one step of the decomposed grid, device -> host
+        stages = S.CudaStages(args.method, mlp)
+        host = torch.empty(sp.padded_shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(S.split(start, p, world, rank).cpu())
+        slab = torch.empty(sp.padded_shape, dtype=torch.float64, device=dev)
+
+        def e2e_step():
+            slab.copy_(host, non_blocking=True)
+            out = S.run([slab], [sp], 1.0e30, "transmissive", comm, stages, max_steps=1).slabs[0]
+            host.copy_(out, non_blocking=True)
+
+        for _ in range(max(W, 1)):
+            e2e_step()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        nbytes = int(np.prod(sp.padded_shape)) * 8
+        line["e2e"] = {"value": units * K / (float(t.item()) * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                       "d2h_bytes_per_step": nbytes,
+                       "api": "weno_sr_publishing_b200.slabs2d.run (pinned host slab per rank, 1 step per call)"}
+        if rank == 0:
+            line["matched_l1"] = matched_l1_block(args.method, mlp, dev)
+    elif not args.skip_extras:
         # end to end: pinned host state -> device, one step, device -> pinned host, K times
         host = torch.empty(p.padded_shape, dtype=torch.float64, pin_memory=True)
         host.copy_(start.cpu())
@@ -356,7 +423,7 @@ def main():
                                               args.cpu_seconds)
         if rank == 0:
             line["matched_l1"] = matched_l1_block(args.method, mlp, dev)
-    if world > 1:
+    if world > 1 or slabs:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:

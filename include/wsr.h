@@ -48,6 +48,10 @@ extern "C" {
 #define WSR_BC_PERIODIC 1
 #define WSR_BC_DOUBLE_MACH 2 /* Mach-10 double-Mach reflection on [0, nx dx] x [0, ny dy] (time dependent;
                                  weno5_hllc_refsym.py:26-124); 2D stage and run functions only */
+#define WSR_BC_Y_HALO 16     /* flag, OR-ed with WSR_BC_TRANSMISSIVE or WSR_BC_PERIODIC in wsr_euler2d_stage(_at):
+                                the 3 ghost rows below and above the interior are read from the stage state as
+                                stored (a slab of a y-decomposed grid whose halo the caller has exchanged); x ghosts
+                                are derived from the base boundary as usual. wsr_euler2d_run rejects it. */
 
 /* interface fluxes */
 #define WSR_FLUX_HLLC 0

@@ -37,6 +37,9 @@
 
 enum { OR_METHOD_JS = 0, OR_METHOD_SR64 = 1, OR_METHOD_SR32 = 2, OR_METHOD_SRBF16 = 3, OR_METHOD_Z = 4 };
 enum { OR_BC_TRANSMISSIVE = 0, OR_BC_PERIODIC = 1, OR_BC_DOUBLE_MACH = 2 };
+/* flag OR-ed into the boundary of a stage: the y ghost rows of u_stage are kept as given (a slab of a
+ * y-decomposed grid whose halo has been exchanged); x ghosts follow the base boundary */
+#define OR_BC_Y_HALO 16
 enum { OR_FLUX_HLLC = 0, OR_FLUX_FORCE = 1 };
 
 typedef struct { double v[4]; } vec4;
@@ -477,6 +480,7 @@ typedef struct {
     const double *P64;
     const float *P32;
     double bt; /* boundary time of the stage (double-Mach only) */
+    int y_halo; /* y ghost rows taken as stored (OR_BC_Y_HALO) */
 } or_cfg;
 
 static inline vec4 load4(const double *a, int nxt, int j, int i) {
@@ -543,6 +547,7 @@ static void apply_bc(const double *src, double *dst, const or_cfg *c) {
                 if (i < GC) si = i + c->nx; else if (i >= c->nx + GC) si = i - c->nx;
                 if (j < GC) sj = j + c->ny; else if (j >= c->ny + GC) sj = j - c->ny;
             }
+            if (c->y_halo) sj = j;
             store4(dst, nxt, j, i, load4(src, nxt, sj, si));
         }
     }
@@ -708,7 +713,8 @@ static void free_stage(or_stage_buf *b) {
 int or_euler2d_stage_at(const double *u_stage, const double *u0, double *u_out, int nx, int ny, double dx,
                         double dy, double gamma, double dt, int rk, int method, int bc, int flux,
                         const double *P64, const float *P32, double boundary_time) {
-    or_cfg c = {nx, ny, method, bc, flux, dx, dy, gamma, P64, P32, boundary_time};
+    or_cfg c = {nx, ny, method, bc & ~OR_BC_Y_HALO, flux, dx, dy, gamma, P64, P32, boundary_time,
+                (bc & OR_BC_Y_HALO) != 0};
     or_stage_buf b;
     if (alloc_stage(&b, padded_len(nx, ny))) { free_stage(&b); return -1; }
     stage(u_stage, u0, u_out, dt, rk, &c, &b);

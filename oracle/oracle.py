@@ -146,14 +146,19 @@ def max_speed(u: np.ndarray, nx: int, ny: int, gamma: float = 1.4) -> float:
     return float(_lib().or_euler2d_max_speed(np.ascontiguousarray(u, dtype=np.float64), nx, ny, gamma))
 
 
+Y_HALO = 16
+
+
 def euler2d_stage(u_stage, u0, u_out, nx, ny, dx, dy, dt, rk, method, bc="transmissive", flux="hllc",
-                  params=None, gamma=1.4, boundary_time=0.0) -> np.ndarray:
-    """One SSPRK3 stage; returns a copy of u_out with its interior overwritten."""
+                  params=None, gamma=1.4, boundary_time=0.0, y_halo=False) -> np.ndarray:
+    """One SSPRK3 stage; returns a copy of u_out with its interior overwritten. y_halo: the y ghost rows of
+    u_stage are used as given (a slab of a y-decomposed grid), x ghosts follow `bc`."""
     out = np.array(u_out, dtype=np.float64, copy=True)
     p64, p32 = _params(params)
     rc = _lib().or_euler2d_stage_at(np.ascontiguousarray(u_stage, dtype=np.float64),
                                     np.ascontiguousarray(u0, dtype=np.float64), out, nx, ny, dx, dy, gamma, dt, rk,
-                                    METHOD[method], BC[bc], FLUX[flux], p64, p32, float(boundary_time))
+                                    METHOD[method], BC[bc] | (Y_HALO if y_halo else 0), FLUX[flux], p64, p32,
+                                    float(boundary_time))
     if rc != 0:
         raise MemoryError("oracle stage allocation failed")
     return out

@@ -19,6 +19,7 @@ METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3, "z": 4}
 # methods whose weights come from an uploaded MLP closure
 SR_METHODS = ("sr_f64", "sr_f32", "sr_bf16")
 BC = {"transmissive": 0, "periodic": 1, "double-mach": 2}
+BC_Y_HALO = 16  # flag: y ghost rows read as stored (slabs of a y-decomposed grid)
 FLUX = {"hllc": 0, "force": 1}
 FLUX3 = {"evilin": 0, "hllc": 1}
 OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT = 1, 2, 4

@@ -30,9 +30,12 @@ enum Bc { BC_TRANSMISSIVE = 0, BC_PERIODIC = 1, BC_DOUBLE_MACH = 2 };
 // Boundary of one stage. The double-Mach boundary is time dependent: it is evaluated at
 // ctl->t + t_off * ctl->dt (the SSPRK3 stages use t, t + dt and t + dt/2, REFSYM:462-527), on the cell
 // centres ((i - 3 + 1/2) dx, (j - 3 + 1/2) dy) of the padded grid.
+// y_ext: the y ghost rows of the stage state are stored in the array (filled from neighbouring slabs of a
+// y-decomposed grid, or by the caller) and read as they are; x ghosts are still derived from `kind`.
 struct StageBc {
   int kind;
   double dx, dy, t_off;
+  int y_ext;
 };
 enum Flux { FLUX_HLLC = 0, FLUX_FORCE = 1 };
 
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
       const int pi = DIR == 1 ? c + k : c;
       if (bc.kind == BC_DOUBLE_MACH && (pj < kGhost || pj >= ny + kGhost || pi < kGhost || pi >= nx + kGhost))
         return double_mach_ghost(u, nx, ny, pj, pi, bc, bt, gas.g);
-      return load_cell(u, nxt, map_index(pj, ny, bc.kind), map_index(pi, nx, bc.kind));
+      return load_cell(u, nxt, bc.y_ext ? pj : map_index(pj, ny, bc.kind), map_index(pi, nx, bc.kind));
     };
     J = roe_jacobian(cell(2), cell(3), gas);
     const CharL L = char_left<DIR>(J, gas);

@@ -72,8 +72,11 @@ int check_2d(wsr_ctx* ctx, int nx, int ny, int method, int bc, int flux, void* w
   if ((long long)(nx + 6) * (ny + 6) > (1ll << 31) / 4)
     return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
   if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
-  if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC && bc != WSR_BC_DOUBLE_MACH)
+  const int base = bc & ~WSR_BC_Y_HALO;
+  if (base != WSR_BC_TRANSMISSIVE && base != WSR_BC_PERIODIC && base != WSR_BC_DOUBLE_MACH)
     return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
+  if ((bc & WSR_BC_Y_HALO) && base == WSR_BC_DOUBLE_MACH)
+    return fail(ctx, WSR_ERR_ARG, "WSR_BC_Y_HALO combines with WSR_BC_TRANSMISSIVE or WSR_BC_PERIODIC only");
   if (flux != WSR_FLUX_HLLC && flux != WSR_FLUX_FORCE) return fail(ctx, WSR_ERR_ARG, "bad flux %d", flux);
   if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && !ctx->have_closure)
     return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before wsr_closure_upload");
@@ -124,7 +127,9 @@ struct StageArgs {
 };
 
 // One stage = 5 launches. dt/dx and dt/dy are read from ws.ctl on the device.
-inline StageBc stage_bc(const StageArgs& a) { return StageBc{a.bc, a.dx, a.dy, a.t_off}; }
+inline StageBc stage_bc(const StageArgs& a) {
+  return StageBc{a.bc & ~WSR_BC_Y_HALO, a.dx, a.dy, a.t_off, (a.bc & WSR_BC_Y_HALO) ? 1 : 0};
+}
 
 // Kernel parameters of a method: the uploaded closure, or for WENO-Z the per-direction eps = h^2.
 template <int M>
@@ -358,6 +363,8 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
                     int* fallbacks_out, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
   if (rc) return rc;
+  if (bc & WSR_BC_Y_HALO)
+    return fail(ctx, WSR_ERR_ARG, "WSR_BC_Y_HALO needs ghost rows refreshed between stages: use wsr_euler2d_stage");
   if (!u || !u[0] || !u[1] || !u[2] || !u[3]) return fail(ctx, WSR_ERR_ARG, "null state buffer");
   if (misaligned(u[0]) || misaligned(u[1]) || misaligned(u[2]) || misaligned(u[3]))
     return fail(ctx, WSR_ERR_ARG, "state arrays must be 16-byte aligned");

@@ -69,9 +69,10 @@ def prepare_closure(method: str, mlp_params, dev: int) -> N.Context:
 
 def stage(u_stage: torch.Tensor, u0: torch.Tensor, u_out: torch.Tensor, params: Params, dt: float, rk: int,
           method: str, boundary: str, mlp_params=None, flux: str = "hllc", opts: int = 0,
-          ws: Workspace | None = None, boundary_time: float = 0.0) -> None:
+          ws: Workspace | None = None, boundary_time: float = 0.0, y_halo: bool = False) -> None:
     """One SSPRK3 stage into the interior of u_out (launch_stage of the reference adapters); the
-    double-Mach boundary is evaluated at boundary_time."""
+    double-Mach boundary is evaluated at boundary_time. y_halo: the y ghost rows of u_stage are read as stored
+    (a slab of a y-decomposed grid, WSR_BC_Y_HALO)."""
     for t in (u_stage, u0, u_out):
         _check_state(t, params)
     if boundary not in N.BC:
@@ -82,7 +83,8 @@ def stage(u_stage: torch.Tensor, u0: torch.Tensor, u_out: torch.Tensor, params: 
     ctx.check(N.lib().wsr_euler2d_stage_at(
         ctx.handle, C.c_void_p(u_stage.data_ptr()), C.c_void_p(u0.data_ptr()), C.c_void_p(u_out.data_ptr()),
         params.nx, params.ny, params.dx, params.dy, params.gamma, float(dt), int(rk), N.METHOD[method],
-        N.BC[boundary], N.FLUX[flux], int(opts), float(boundary_time), C.c_void_p(ws.ptr), ws.nbytes,
+        N.BC[boundary] | (N.BC_Y_HALO if y_halo else 0), N.FLUX[flux], int(opts), float(boundary_time),
+        C.c_void_p(ws.ptr), ws.nbytes,
         _stream_ptr(dev)))
 
 
