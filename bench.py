@@ -273,7 +273,7 @@ def main():
         return ms, r
 
     if slabs:
-        from weno_sr_publishing_b200 import slabs2d as S
+        from weno_sr_publishing_b200 import slabs as S
         sp = S.slab_params(p, world, rank)
         comm = S.DistSlabs()
 
@@ -393,7 +393,7 @@ def main():
         nbytes = int(np.prod(sp.padded_shape)) * 8
         line["e2e"] = {"value": units * K / (float(t.item()) * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                        "d2h_bytes_per_step": nbytes,
-                       "api": "weno_sr_publishing_b200.slabs2d.run (pinned host slab per rank, 1 step per call)"}
+                       "api": "weno_sr_publishing_b200.slabs.run (pinned host slab per rank, 1 step per call)"}
         if rank == 0:
             line["matched_l1"] = matched_l1_block(args.method, mlp, dev)
     elif not args.skip_extras:

@@ -61,6 +61,9 @@ extern "C" {
 #define WSR_OPT_ENO_CUTOFF 1  /* the reference's eno_cutoff flag (4e-7), off in all paper runs */
 #define WSR_OPT_JS_FALLBACK 2 /* per-stencil WENO5-JS weights when the closure is non-finite, and per
                                  face when an SR face state has rho <= 0 or p <= 0 */
+#define WSR_OPT_Z_HALO 8      /* wsr_euler3d_stage: the 3 z ghost planes below and above are filled by the caller
+                                 (a slab of a z-decomposed grid) and not overwritten; x and y ghosts are filled as
+                                 usual. wsr_euler3d_run rejects it. */
 
 typedef struct wsr_ctx wsr_ctx;
 

@@ -240,6 +240,7 @@ typedef struct {
     const double *P64;
     const float *P32;
     const double *inflow;  /* 5 conserved values for the x-low ghosts, or NULL (transmissive) */
+    int z_halo;            /* z ghost planes given by the caller (a slab of a z-decomposed grid): not filled */
 } o3_cfg;
 
 typedef struct {
@@ -283,6 +284,7 @@ static void boundary(double *q, const o3_cfg *c) {
                 st(q, at(c, k, c->ny + 3 + g, i), b);
             }
         }
+    if (c->z_halo) return;
     for (int j = 0; j < py; ++j)
         for (int i = 0; i < px; ++i) {
             v5 a = ld(q, at(c, 3, j, i)), b = ld(q, at(c, c->nz + 2, j, i));
@@ -506,6 +508,22 @@ int or_euler3d_run(double *q, int nx, int ny, int nz, double dx, double dy, doub
     }
     free_buf(&b);
     return taken;
+}
+
+/* One RK stage in place (rk_stage) with the stage-start copy in the caller's q0 (padded, kept between the
+ * three stages); z_halo: the z ghost planes of q are taken as given. Returns 0, or -1 on allocation failure. */
+int or_euler3d_stage(double *q, double *q0, int nx, int ny, int nz, double dx, double dy, double dz, double dt,
+                     int stage, int method, int flux, const double *P64, const float *P32, const double *inflow,
+                     int z_halo) {
+    o3_cfg c = {nx, ny, nz, method, flux, dx, dy, dz, P64, P32, inflow, z_halo};
+    o3_buf b;
+    if (alloc_buf(&b, &c)) { free_buf(&b); return -1; }
+    double *own = b.q0;
+    b.q0 = q0;
+    rk_stage(q, stage, dt, &c, &b);
+    b.q0 = own;
+    free_buf(&b);
+    return 0;
 }
 
 /* Flat wrappers for the flux tests: n interfaces of 5 conserved values each. */

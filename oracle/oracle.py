@@ -55,6 +55,9 @@ def _lib(fast: bool = False) -> C.CDLL:
         lib.or_euler3d_run.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _fp,
                                        _vp, _dp, C.c_int]
+        lib.or_euler3d_stage.restype = C.c_int
+        lib.or_euler3d_stage.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, C.c_int, C.c_int, _dp, _fp, C.c_void_p, C.c_int]
         lib.or_euler3d_max_speed.restype = C.c_double
         lib.or_euler3d_max_speed.argtypes = [_dp, C.c_int, C.c_int, C.c_int]
         lib.or_hllc5_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, _dp]
@@ -201,6 +204,20 @@ def euler3d_run(q, nx, ny, nz, dx, dy, dz, cfl, steps, method, flux="evilin", pa
     if taken < 0:
         raise MemoryError("oracle allocation failed")
     return out, dts[:taken]
+
+
+def euler3d_stage(q, q0, nx, ny, nz, dx, dy, dz, dt, stage, method, flux="evilin", params=None, inflow=None,
+                  z_halo=False) -> None:
+    """One RK stage of the 3D oracle on q in place (numpy, padded), q0 the caller's stage-start copy (written at
+    stage 1, read at 2 and 3); z_halo: the z ghost planes of q are used as given."""
+    p64, p32 = _params(params)
+    keep = None if inflow is None else np.ascontiguousarray(inflow, dtype=np.float64)
+    if not (q.flags.c_contiguous and q0.flags.c_contiguous and q.dtype == q0.dtype == np.float64):
+        raise ValueError("q and q0 must be C-contiguous float64 arrays")
+    rc = _lib().or_euler3d_stage(q, q0, nx, ny, nz, dx, dy, dz, dt, stage, METHOD[method], FLUX3[flux], p64, p32,
+                                 None if keep is None else keep.ctypes.data_as(C.c_void_p), int(bool(z_halo)))
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
 
 
 def euler3d_max_speed(q, nx, ny, nz) -> float:

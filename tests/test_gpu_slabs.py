@@ -15,7 +15,7 @@ import torch
 from weno_sr_publishing_b200 import _native as N
 from weno_sr_publishing_b200 import euler2d as E
 from weno_sr_publishing_b200 import problems
-from weno_sr_publishing_b200 import slabs2d as S
+from weno_sr_publishing_b200 import slabs as S
 from weno_sr_publishing_b200.checkpoint import MODELS_DIR
 from weno_sr_publishing_b200.params import Params
 
@@ -103,3 +103,42 @@ def test_one_rank_nccl_group(boundary):
         np.testing.assert_array_equal(S.gather_interior(res.slabs), ref)
     finally:
         dist.destroy_process_group()
+
+
+def _initial3(nx, ny, nz, seed=1):
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(*[(np.arange(n) + 0.5) / n for n in (nz, ny, nx)], indexing="ij")
+    rho = 1.0 + 0.4 * (x + 0.6 * y + 0.3 * z > 0.8) + 0.05 * rng.uniform(size=x.shape)
+    p = 1.0 + 1.5 * (z < 0.4) + 0.05 * rng.uniform(size=x.shape)
+    u, v, w = 0.3 * rng.uniform(-1, 1, x.shape), 0.2 * rng.uniform(-1, 1, x.shape), 0.25 * np.sin(6 * x)
+    inner = np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], axis=-1)
+    return np.ascontiguousarray(np.pad(inner, ((3, 3), (3, 3), (3, 3), (0, 0)), mode="edge"))
+
+
+@pytest.mark.parametrize("world", [2, 4])
+@pytest.mark.parametrize("method,flux,inflow", [("js", "evilin", None), ("sr_f32", "hllc", None),
+                                                ("sr_f64", "hllc", (1.2, 0.4, 0.0, 0.0, 3.0))])
+def test_3d_slabs_equal_single_domain(world, method, flux, inflow):
+    from weno_sr_publishing_b200 import euler3d as E3
+
+    nx, ny, nz = 24, 17, 30
+    d = (0.05, 0.06, 0.04)
+    q0 = _initial3(nx, ny, nz)
+    q = torch.as_tensor(q0, device=DEV).clone()
+    rres = E3.run(q, nx, ny, nz, *d, 0.4, method, flux, mlp_params=_closure(method), inflow=inflow, steps=4)
+    ref = q.cpu().numpy()[3:-3, 3:-3, 3:-3]
+    g = torch.as_tensor(q0, device=DEV)
+    slabs = [S.split3(g, nz, world, r) for r in range(world)]
+    grids = [S.slab_grid3(nx, ny, nz, *d, world, r) for r in range(world)]
+    res = S.run3(slabs, grids, 0.4, S.LocalSlabs(world), S.CudaStages3(method, flux, _closure(method), inflow),
+                 steps=4)
+    assert res.steps == rres.steps and res.dts == list(rres.dts)
+    np.testing.assert_array_equal(S.gather_interior3(res.slabs), ref)
+
+
+def test_3d_run_rejects_the_halo_option():
+    from weno_sr_publishing_b200 import euler3d as E3
+
+    q = torch.as_tensor(_initial3(8, 8, 8), device=DEV)
+    with pytest.raises(ValueError, match="WSR_OPT_Z_HALO"):
+        E3.run(q, 8, 8, 8, 0.1, 0.1, 0.1, 0.4, steps=1, opts=N.OPT_Z_HALO)

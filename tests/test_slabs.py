@@ -14,7 +14,7 @@ import torch.multiprocessing as mp
 
 from oracle import oracle as O
 from weno_sr_publishing_b200 import problems
-from weno_sr_publishing_b200 import slabs2d as S
+from weno_sr_publishing_b200 import slabs as S
 from weno_sr_publishing_b200.params import Params
 
 NX, NY = 17, 14
@@ -167,3 +167,76 @@ def test_three_gloo_ranks_periodic():
     ref, _, rsteps, _ = O.euler2d_run(_initial(), NX, NY, p.dx, p.dy, p.cfl, 0.02, "js", "periodic")
     np.testing.assert_array_equal(np.concatenate([out[r][0] for r in range(world)], axis=0), ref[3:-3, 3:-3])
     assert all(out[r][1] == rsteps for r in range(world))
+
+
+# ------------------------------------------------------------------------------------------------
+# 3D z-slabs
+# ------------------------------------------------------------------------------------------------
+NX3, NY3, NZ3 = 7, 6, 13
+
+
+class OracleStages3:
+    """The 3D oracle's stage (z-halo mode) and wave speed, on numpy slabs; q0 per slab."""
+
+    def __init__(self, method="js", flux="evilin", params=None, inflow=None):
+        self.method, self.flux, self.params, self.inflow = method, flux, params, inflow
+        self.q0 = {}
+
+    def max_speed(self, q, g):
+        return O.euler3d_max_speed(q, g.nx, g.ny, g.nz)
+
+    def stage(self, q, g, dt, st):
+        q0 = self.q0.setdefault(id(q), np.zeros_like(q))
+        O.euler3d_stage(q, q0, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, dt, st, self.method, self.flux, self.params,
+                        self.inflow, z_halo=True)
+
+
+def _initial3(seed=1):
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(*[(np.arange(n) + 0.5) / n for n in (NZ3, NY3, NX3)], indexing="ij")
+    rho = 1.0 + 0.4 * (x + 0.6 * y + 0.3 * z > 0.8) + 0.05 * rng.uniform(size=x.shape)
+    p = 1.0 + 1.5 * (z < 0.4) + 0.05 * rng.uniform(size=x.shape)
+    u, v, w = 0.3 * rng.uniform(-1, 1, x.shape), 0.2 * rng.uniform(-1, 1, x.shape), 0.25 * np.sin(6 * x)
+    inner = np.stack([rho, rho * u, rho * v, rho * w, p / 0.4 + 0.5 * rho * (u * u + v * v + w * w)], axis=-1)
+    return np.ascontiguousarray(np.pad(inner, ((3, 3), (3, 3), (3, 3), (0, 0)), mode="edge"))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("method,flux,inflow", [("js", "evilin", None), ("js", "hllc", None),
+                                                ("sr_f64", "hllc", (1.2, 0.4, 0.0, 0.0, 3.0))])
+def test_decomposed_3d_oracle_run_equals_single_domain(world, method, flux, inflow):
+    params = None
+    if method != "js":
+        from weno_sr_publishing_b200.checkpoint import MODELS_DIR
+        params = dict(np.load(MODELS_DIR / "weno5_sr_fp64_step012250.npz"))
+    q = _initial3()
+    d = (0.1, 0.11, 0.09)
+    ref, rdts = O.euler3d_run(q, NX3, NY3, NZ3, *d, 0.4, 3, method, flux, params=params, inflow=inflow)[:2]
+    grids = [S.slab_grid3(NX3, NY3, NZ3, *d, world, r) for r in range(world)]
+    slabs = [S.split3(q, NZ3, world, r) for r in range(world)]
+    res = S.run3(slabs, grids, 0.4, S.LocalSlabs(world), OracleStages3(method, flux, params, inflow), steps=3)
+    assert res.steps == 3 and res.dts == list(rdts)
+    np.testing.assert_array_equal(S.gather_interior3(res.slabs), ref[3:-3, 3:-3, 3:-3])
+
+
+def _worker3(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        d = (0.1, 0.11, 0.09)
+        res = S.run3([S.split3(_initial3(), NZ3, world, rank)], [S.slab_grid3(NX3, NY3, NZ3, *d, world, rank)], 0.4,
+                     S.DistSlabs(), OracleStages3("js", "hllc"), t_end=0.05)
+        out[rank] = (S.gather_interior3(res.slabs), res.steps, res.t)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_3d_equal_single_domain():
+    world = 2
+    manager = mp.Manager()
+    out = manager.dict()
+    mp.spawn(_worker3, args=(world, _free_port(), out), nprocs=world, join=True)
+    ref, rdts = O.euler3d_run(_initial3(), NX3, NY3, NZ3, 0.1, 0.11, 0.09, 0.4, 100, "js", "hllc", t_end=0.05)[:2]
+    assert out[0][1] == out[1][1] == len(rdts) and out[0][2] == out[1][2]
+    np.testing.assert_array_equal(np.concatenate([out[r][0] for r in range(world)], axis=0), ref[3:-3, 3:-3, 3:-3])

@@ -22,7 +22,7 @@ BC = {"transmissive": 0, "periodic": 1, "double-mach": 2}
 BC_Y_HALO = 16  # flag: y ghost rows read as stored (slabs of a y-decomposed grid)
 FLUX = {"hllc": 0, "force": 1}
 FLUX3 = {"evilin": 0, "hllc": 1}
-OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT = 1, 2, 4
+OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT, OPT_Z_HALO = 1, 2, 4, 8
 PROF_KINDS = ("normal_x", "normal_y", "flux_x", "flux_y", "update", "control")
 N_PARAMS5 = 189
 PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")

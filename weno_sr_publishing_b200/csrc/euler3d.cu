@@ -654,7 +654,8 @@ int stage3(wsr_ctx* ctx, const Run3& r, const Ws3& w, int stage, cudaStream_t st
   const Dims3& d = r.d;
   k3_bc<1><<<dim3((d.py + kT3 - 1) / kT3, d.pz), kT3, 0, st>>>(r.q, d, r.in, w.ctl);
   k3_bc<2><<<dim3((d.px + kT3 - 1) / kT3, d.pz), kT3, 0, st>>>(r.q, d, r.in, w.ctl);
-  k3_bc<3><<<dim3((d.px + kT3 - 1) / kT3, d.py), kT3, 0, st>>>(r.q, d, r.in, w.ctl);
+  // WSR_OPT_Z_HALO: the z ghost planes were filled by the caller (a slab of a z-decomposed grid)
+  if (!(r.opts & WSR_OPT_Z_HALO)) k3_bc<3><<<dim3((d.px + kT3 - 1) / kT3, d.py), kT3, 0, st>>>(r.q, d, r.in, w.ctl);
   WSR_LAUNCHED(ctx, "k3_bc");
   int rc;
   if ((rc = sweep3<M, 1, FLUX>(ctx, r, w, r.dx, st))) return rc;
@@ -784,6 +785,8 @@ extern "C" int wsr_euler3d_run(wsr_ctx* ctx, double* q, int nx, int ny, int nz, 
   int rc = check3(ctx, q, nx, ny, nz, dx, dy, dz, method, flux, workspace, workspace_bytes);
   if (rc) return rc;
   if (max_steps < 1) return fail(ctx, WSR_ERR_ARG, "max_steps must be >= 1");
+  if (opts & WSR_OPT_Z_HALO)
+    return fail(ctx, WSR_ERR_ARG, "WSR_OPT_Z_HALO needs ghost planes refreshed between stages: use wsr_euler3d_stage");
   if (!(cfl > 0.0)) return fail(ctx, WSR_ERR_ARG, "cfl must be positive");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));

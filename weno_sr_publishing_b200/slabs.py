@@ -1,6 +1,7 @@
-"""Y-slab decomposition of the 2D Euler WENO5 step over ranks (one process per GPU).
+"""Slab decompositions of the 2D and 3D Euler WENO5 steps over ranks (one process per GPU): y-slabs in 2D,
+z-slabs in 3D -- in both layouts the leading array axis, so the halo blocks are contiguous.
 
-The global grid (nx x ny interior cells, ghost width 3) is cut into slabs of whole rows; rank r owns rows
+2D. The global grid (nx x ny interior cells, ghost width 3) is cut into slabs of whole rows; rank r owns rows
 [y0_r, y1_r) in the reference's padded layout [(ny_r + 6), (nx + 6), 4] with its own 3 ghost rows below and
 above. Before every SSPRK3 stage the slabs exchange 3 interior rows with each neighbour -- one contiguous
 3 x (nx + 6) x 4 block per side, sent upward in one phase and downward in the next (torch.distributed
@@ -12,6 +13,11 @@ dt and stop rules (wsr_euler2d_run, warp_weno5_helpers.py:189-207, weno5_hllc_re
 decomposed run equals the single-domain run bit for bit.
 
 The double-Mach boundary (time-dependent y boundaries) is not decomposed.
+
+3D. The grid [nz+6][ny+6][nx+6][5] is cut into z-slabs the same way; before every RK stage 3 z-planes are
+exchanged with each neighbour (the global z ends copy their edge plane: the solver's outflow boundary), and
+the stage fills the x and y ghosts of every plane itself, halo planes included, and leaves the z ghost
+planes as given (WSR_OPT_Z_HALO). The loop applies the 3D solver's dt and stop rules (solver.py:303-329).
 """
 from __future__ import annotations
 
@@ -23,6 +29,7 @@ import torch
 
 from . import _native as N
 from . import euler2d as E
+from . import euler3d as E3
 from .params import Params
 
 GHOST = 3
@@ -230,4 +237,102 @@ def gather_interior(slabs: list) -> np.ndarray:
     for u in slabs:
         a = u.detach().cpu().numpy() if isinstance(u, torch.Tensor) else np.asarray(u)
         parts.append(a[GHOST:a.shape[0] - GHOST, GHOST:a.shape[1] - GHOST])
+    return np.concatenate(parts, axis=0)
+
+
+# ------------------------------------------------------------------------------------------------
+# 3D z-slabs
+# ------------------------------------------------------------------------------------------------
+@dataclass(frozen=True)
+class Grid3:
+    """One z-slab of a 3D grid: its interior size, the spacings of the global grid, its first global plane."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dy: float
+    dz: float
+    z0: int = 0
+
+    @property
+    def padded_shape(self) -> tuple[int, int, int, int]:
+        return (self.nz + 2 * GHOST, self.ny + 2 * GHOST, self.nx + 2 * GHOST, 5)
+
+
+def slab_grid3(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float, world: int, rank: int) -> Grid3:
+    z0, z1 = slab_rows(nz, world, rank)
+    return Grid3(nx, ny, z1 - z0, dx, dy, dz, z0)
+
+
+def split3(q_global, nz: int, world: int, rank: int):
+    """The padded z-slab `rank` of a padded global 3D state, ghost planes included (copied)."""
+    return split(q_global, Params(nx=1, ny=nz), world, rank)
+
+
+class CudaStages3:
+    """The 3D z-slab stages (in place, stage-start copy in the slab's workspace) and wave speeds through
+    libwsr.so (WSR_OPT_Z_HALO)."""
+
+    def __init__(self, method: str = "js", flux: str = "evilin", mlp_params=None, inflow=None, opts: int = 0):
+        self.method, self.flux, self.mlp_params, self.inflow, self.opts = method, flux, mlp_params, inflow, opts
+        self._ws: dict = {}
+
+    def _workspace(self, q: torch.Tensor, g: Grid3):
+        key = (q.data_ptr(), g.nx, g.ny, g.nz)
+        if key not in self._ws:
+            self._ws[key] = E3.workspace(g.nx, g.ny, g.nz, q.device)
+        return self._ws[key]
+
+    def max_speed(self, q: torch.Tensor, g: Grid3) -> float:
+        return E3.max_speed(q, g.nx, g.ny, g.nz, self._workspace(q, g))
+
+    def stage(self, q: torch.Tensor, g: Grid3, dt: float, stage: int) -> None:
+        E3.stage(q, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, dt, stage, self.method, self.flux, self.mlp_params,
+                 self.inflow, self.opts | N.OPT_Z_HALO, ws=self._workspace(q, g))
+
+
+@dataclass
+class SlabRun3:
+    slabs: list
+    grids: list
+    dts: list = field(default_factory=list)
+    steps: int = 0
+    t: float = 0.0
+
+
+def run3(slabs: list, grids: list, cfl: float, comm, stages, t_end: float | None = None, steps: int | None = None,
+         t_start: float = 0.0) -> SlabRun3:
+    """Advance the local 3D z-slabs in place: to t_end, or exactly `steps` steps when t_end is None
+    (Weno5Rk3Solver.advance, solver.py:303-329: dt = cfl min(dx, dy, dz) / max speed, 1e10 below 1e-15,
+    clipped to t_end; stop when t == t_end)."""
+    if t_end is None and steps is None:
+        raise ValueError("give t_end or steps")
+    g0 = grids[0]
+    hmin = min(g0.dx, g0.dy, g0.dz)
+    t_stop = 1.0e300 if t_end is None else float(t_end)
+    cap = steps if steps is not None else 1_000_000
+    t, taken, dts = float(t_start), 0, []
+    for _ in range(cap):
+        if t == t_stop:
+            break
+        m = comm.max(max(stages.max_speed(q, g) for q, g in zip(slabs, grids)))
+        dt = 1.0e10 if m < 1.0e-15 else cfl * hmin / m
+        if t + dt > t_stop:
+            dt = t_stop - t
+        t = t + dt
+        for st in (1, 2, 3):
+            comm.exchange(slabs, False)
+            for q, g in zip(slabs, grids):
+                stages.stage(q, g, dt, st)
+        taken += 1
+        dts.append(dt)
+    return SlabRun3(slabs, list(grids), dts, taken, t)
+
+
+def gather_interior3(slabs: list) -> np.ndarray:
+    """Interior cells of the 3D slabs in order, as one [nz][ny][nx][5] host array."""
+    parts = []
+    for q in slabs:
+        a = q.detach().cpu().numpy() if isinstance(q, torch.Tensor) else np.asarray(q)
+        parts.append(a[GHOST:-GHOST, GHOST:-GHOST, GHOST:-GHOST])
     return np.concatenate(parts, axis=0)
