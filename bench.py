@@ -875,6 +875,10 @@ def bench_3d(args, world, rank, local):
            "time_integrator": "SSPRK3", "state_precision": "fp64",
            "l2_policy": "state 81 MB, workspace 0.8 GB per step: larger than L2",
            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+    slabs = args.decomp == "slabs" or (args.decomp == "auto" and world > 1)
+    if slabs:
+        cfg["parallelism"] = (f"z-slabs x{world}: rank r owns planes of the one 224x88x88 grid, 3-plane halo "
+                              f"exchange per stage (NCCL send/recv), MAX all-reduce of the wave speed per step")
     sb = PR.ShockBubble.seeded(0)
     if args.impl == "reference":
         if rank != 0:
@@ -889,14 +893,20 @@ def bench_3d(args, world, rank, local):
         return
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
+    if world > 1 or slabs:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29534")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev, rank=rank,
+                                world_size=world)
     stream = torch.cuda.current_stream(dev)
     q0 = torch.as_tensor(sb.state(), device=dev).contiguous()
     dx, dy, dz = sb.spacing
     ws = E3.workspace(sb.nx, sb.ny, sb.nz, dev)
     K, W = args.steps, max(args.warmup, 0)
+    if slabs:
+        _bench_3d_slabs(args, world, rank, local, sb, q0, method, params, metric, cfg, K, W)
+        return
     q = q0.clone()
     if W:
         E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=W, ws=ws)
@@ -949,6 +959,65 @@ def bench_3d(args, world, rank, local):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _bench_3d_slabs(args, world, rank, local, sb, q0, method, params, metric, cfg, K, W):
+    """The 3D step on z-slabs of the one shock-bubble grid (strong scaling), timed as the max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    from weno_sr_publishing_b200 import slabs as S
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    dx, dy, dz = sb.spacing
+    grid = S.slab_grid3(sb.nx, sb.ny, sb.nz, dx, dy, dz, world, rank)
+    comm = S.DistSlabs()
+    stages = S.CudaStages3(method, "hllc", params, sb.inflow())
+    if W:
+        S.run3([S.split3(q0, sb.nz, world, rank)], [grid], 0.4, comm, stages, steps=W)
+    slab = S.split3(q0, sb.nz, world, rank)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        res = S.run3([slab], [grid], 0.4, comm, stages, steps=K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    cells = sb.nx * sb.ny * sb.nz
+    ok = torch.tensor([float(torch.isfinite(slab).all())], device=dev)
+    dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+    line = {"metric": metric, "value": cells * K / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": cfg, "clocks": clk.summary(),
+            # per step: max speed (1), 3 stages x (control init + 2 boundary passes + 3 sweeps x 3 + update)
+            "gpu_launches": K * (1 + 3 * 13), "t_reached": res.t, "state_finite": bool(ok.item()),
+            "shock": {"mach": sb.mach, "density_ratio": sb.density_ratio}}
+    if not args.skip_extras:
+        # end to end: this rank's padded slab from pinned host memory, K steps, and back
+        host = torch.empty(grid.padded_shape, dtype=torch.float64, pin_memory=True)
+        host.copy_(S.split3(q0, sb.nz, world, rank).cpu())
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        slab.copy_(host, non_blocking=True)
+        S.run3([slab], [grid], 0.4, comm, stages, steps=K)
+        host.copy_(slab, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        nbytes = int(np.prod(grid.padded_shape)) * 8
+        line["e2e"] = {"value": cells * K / (float(t.item()) * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes / K,
+                       "d2h_bytes_per_step": nbytes / K,
+                       "api": "weno_sr_publishing_b200.slabs.run3 on a slab copied from / to pinned host memory"}
+    dist.barrier()
+    dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
