@@ -407,6 +407,7 @@ def main():
         e0.record(stream)
         for _ in range(K):
             E.advance_host(host, p, 1, args.method, "transmissive", mlp_params=mlp, bufs=bufs, ws=ws, device=dev)
+        E.host_copies_done(dev)  # the last read-back is inside the timed region
         e1.record(stream)
         torch.cuda.synchronize()
         ms_e2e = e0.elapsed_time(e1)

@@ -152,15 +152,64 @@ def run(bufs: list, params: Params, t_end: float, method: str, boundary: str, ml
     return RunResult(slot.value, [float(x) for x in dts[:steps.value]], steps.value, t.value, fb.value)
 
 
+_COPY_BANDS = 8
+_copy_pipes: dict = {}
+
+
+class _CopyPipe:
+    """Copy streams of one host buffer: the state goes in and out in row bands, host -> device on one stream
+    and device -> host on another, and band b of a call's input waits only for band b of the previous call's
+    output (the same pinned rows), so one call's read-back and the next call's upload share the two copy
+    directions instead of following each other."""
+
+    def __init__(self, dev: torch.device, rows: int):
+        self.h2d = torch.cuda.Stream(dev)
+        self.d2h = torch.cuda.Stream(dev)
+        edges = np.linspace(0, rows, min(_COPY_BANDS, rows) + 1).astype(int)
+        self.bands = [(int(a), int(b)) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+        self.out_done = [torch.cuda.Event() for _ in self.bands]
+        self.pending = False
+
+
 def advance_host(u_host: np.ndarray, params: Params, steps: int, method: str, boundary: str, mlp_params=None,
                  bufs: list | None = None, ws: Workspace | None = None, device="cuda") -> np.ndarray:
     """Host-buffer entry: copy the padded state to the device, run `steps` full CFL steps, copy it back
-    into u_host (in place). Pinned host memory makes both copies asynchronous DMA."""
+    into u_host (in place). With pinned host memory both copies are asynchronous DMA in row bands on two copy
+    streams: the read-back is complete once the device is synchronised or host_copies_done() has ordered the
+    current stream after it; the next call's upload of the same rows waits for it band by band."""
     dev = torch.device(device)
     if bufs is None:
         bufs = [torch.empty(params.padded_shape, dtype=torch.float64, device=dev) for _ in range(4)]
     host = torch.from_numpy(u_host) if isinstance(u_host, np.ndarray) else u_host
-    bufs[0].copy_(host, non_blocking=True)
+    key = (dev.index if dev.index is not None else torch.cuda.current_device(), host.data_ptr(), tuple(host.shape))
+    pipe = _copy_pipes.get(key)
+    if pipe is None:
+        pipe = _copy_pipes[key] = _CopyPipe(dev, int(host.shape[0]))
+    cur = torch.cuda.current_stream(dev)
+    pipe.h2d.wait_stream(cur)  # earlier work on bufs[0] is done before it is overwritten
+    with torch.cuda.stream(pipe.h2d):
+        for k, (r0, r1) in enumerate(pipe.bands):
+            if pipe.pending:
+                pipe.h2d.wait_event(pipe.out_done[k])
+            bufs[0][r0:r1].copy_(host[r0:r1], non_blocking=True)
+    cur.wait_stream(pipe.h2d)
     res = run(bufs, params, 1.0e300, method, boundary, mlp_params=mlp_params, fixed_steps=steps, ws=ws)
-    host.copy_(bufs[res.final_slot], non_blocking=True)
+    out = bufs[res.final_slot]
+    pipe.d2h.wait_stream(cur)
+    with torch.cuda.stream(pipe.d2h):
+        for k, (r0, r1) in enumerate(pipe.bands):
+            host[r0:r1].copy_(out[r0:r1], non_blocking=True)
+            pipe.out_done[k].record(pipe.d2h)
+    pipe.pending = True
     return u_host
+
+
+def host_copies_done(device="cuda") -> None:
+    """Make the current stream wait for every read-back advance_host has issued on `device` (work or events
+    recorded on the current stream afterwards come after them)."""
+    dev = torch.device(device)
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    cur = torch.cuda.current_stream(dev)
+    for key, pipe in _copy_pipes.items():
+        if key[0] == idx:
+            cur.wait_stream(pipe.d2h)
