@@ -552,6 +552,9 @@ def bench_1d(args, world, rank, local):
                "method": method, "loss": "mean L1 to exact cell averages at every completed step",
                "l2_policy": "inputs larger than L2 for the long distances (checkpoints + stage scratch)"}
     cfg["parallelism"] = f"replicas x{world}" if world > 1 else "single GPU"
+    if args.workload == "adv1d" and world > 1:
+        cfg["parallelism"] = (f"sharded x{world}: 4096 x {world} seeded trajectories, each rank its cost-balanced "
+                              f"share (cells x steps, longest first), no data-path collective")
     if args.workload == "train1d" and world > 1:
         cfg["parallelism"] = f"data parallel x{world}: each rank its own 1024 trajectories, gradient all-reduce"
     if args.impl == "reference":
@@ -592,7 +595,10 @@ def bench_1d(args, world, rank, local):
             "config": cfg}
     if args.workload == "adv1d":
         from weno_sr_publishing_b200 import adv1d as A1
-        states, vel, ns, steps = adv1d_batch()
+        states, vel, ns, steps = adv1d_batch(B=4096 * world)
+        if world > 1:  # this rank's cost-balanced share of the 4096 x world trajectories
+            mine = A1.shard_by_cost(ns * steps, world, rank)
+            states, vel, ns, steps = [states[b] for b in mine], vel[mine], ns[mine], steps[mine]
         closure = _closure(args.scheme, method)
         cl = A1.as_closure(closure)
         ctx = N.context(local)
@@ -641,7 +647,12 @@ def bench_1d(args, world, rank, local):
                 ms += e0.elapsed_time(e1)
         ms = max_over_ranks(ms)
         work = float(np.sum(ns * steps))
-        line.update({"value": world * work * K / (ms * 1e-3), "ms_per_step": ms / K, "clocks": clk.summary(),
+        total = work
+        if world > 1:  # the cell-steps of all shards
+            t = torch.tensor([work], dtype=torch.float64, device=dev)
+            dist.all_reduce(t)
+            total = float(t.item())
+        line.update({"value": total * K / (ms * 1e-3), "ms_per_step": ms / K, "clocks": clk.summary(),
                      "gpu_launches": K})
         flat.copy_(flat0)
         launch(N.OPT_COUNT, cnt)
@@ -659,7 +670,8 @@ def bench_1d(args, world, rank, local):
             host = [o.cpu() for o in outs]
         el = time.perf_counter() - t0
         nbytes = int(np.sum(ns)) * 8
-        line["e2e"] = {"value": world * work * K / el, "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+        el = max_over_ranks(el * 1e3) * 1e-3
+        line["e2e"] = {"value": total * K / el, "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
                        "d2h_bytes_per_step": nbytes, "api": "weno_sr_publishing_b200.adv1d.run_batched (host arrays)"}
         peak = ctx.peak_tflops(32 if method in ("sr_f32", "sr_bf16") else 64, C_stream(stream))
         line["roofline"] = _roofline_1d(args.scheme, method, work, mlp_n, plat_n, ms / K, peak, ctx, stream)

@@ -59,3 +59,19 @@ def test_gste_weno5_js_oracle_matches_reference_final_state():
     dt = 10.0 / steps
     out = A.run(g["initial"], 1.0, dx, [dt] * steps, 5, None, "ssprk3")
     assert np.abs(out - g["weno5_js_final"]).max() <= 1e-12
+
+
+def test_shard_by_cost_partitions_and_balances():
+    from weno_sr_publishing_b200 import adv1d as A1
+
+    rng = np.random.default_rng(4)
+    cost = rng.integers(100, 1001, 4096 * 3) * 2 * rng.choice([2, 8, 64, 128, 256, 512, 1024], 4096 * 3)
+    for world in (1, 2, 3, 8):
+        parts = [A1.shard_by_cost(cost, world, r) for r in range(world)]
+        allidx = np.sort(np.concatenate(parts))
+        np.testing.assert_array_equal(allidx, np.arange(cost.size))
+        loads = np.array([cost[p].sum() for p in parts])
+        assert loads.max() - loads.min() <= cost.max()
+        np.testing.assert_array_equal(parts[0], A1.shard_by_cost(cost, world, 0))  # deterministic
+    with pytest.raises(ValueError):
+        A1.shard_by_cost(cost, 2, 2)

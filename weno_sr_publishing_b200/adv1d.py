@@ -142,6 +142,23 @@ def run_batched(states, velocities, dx, n_full, dt_full, dt_last=None, *, scheme
     return outs, {"fallbacks": fb.value, "mlp": int(cnt[0]), "plateau": int(cnt[1])}
 
 
+def shard_by_cost(cost, world: int, rank: int) -> np.ndarray:
+    """Trajectories of `rank` when a batch is sharded over `world` ranks by cost (cells x steps of each
+    trajectory): longest first, each to the rank with the least load so far (ties to the lower rank). Every
+    trajectory lands on exactly one rank, every rank ends within one trajectory's cost of the mean, and every
+    rank computes the same partition without communicating. Returns sorted indices."""
+    cost = np.asarray(cost, dtype=np.float64).reshape(-1)
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"bad rank {rank} of {world}")
+    load = np.zeros(world)
+    owner = np.empty(cost.size, dtype=np.int64)
+    for b in np.argsort(-cost, kind="stable"):
+        r = int(np.argmin(load))
+        owner[b] = r
+        load[r] += cost[b]
+    return np.flatnonzero(owner == rank)
+
+
 def _rows(state):
     t = torch.as_tensor(state, dtype=torch.float64)
     if t.ndim != 2:
