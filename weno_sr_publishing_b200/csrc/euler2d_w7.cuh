@@ -25,6 +25,10 @@ namespace w7 {
 
 constexpr int kG = 4;  // ghost width
 constexpr int kBlock7 = 128;
+// Resident blocks per SM the WENO7-SR kernels' register budget targets (the FP64 MLP pair is register heavy).
+#ifndef WSR_W7SR_MIN_BLOCKS
+#define WSR_W7SR_MIN_BLOCKS 4
+#endif
 
 __device__ __forceinline__ int map7(int p, int n, int bc) {
   if (bc == BC_TRANSMISSIVE) return p < kG ? kG : (p >= n + kG ? n + kG - 1 : p);
@@ -489,7 +493,7 @@ __global__ void k_probe_exp_tab(const double* __restrict__ x, double* __restrict
 // characteristic field f; side 0 -> cells 0..6, head lr = 1; side 1 -> cells 1..7, head lr = 2, closure on the
 // flipped cells 7..1.
 template <int DIR>
-__global__ void __launch_bounds__(kBlock7, 3) k7s_normal(const double* __restrict__ u, double* __restrict__ out_l,
+__global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_normal(const double* __restrict__ u, double* __restrict__ out_l,
                                                         double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
                                                         const StepCtl* __restrict__ ctl,
                                                         unsigned long long* __restrict__ counters,
@@ -592,7 +596,7 @@ __device__ __forceinline__ void w7_load_transverse(const double* __restrict__ fl
 // Transverse reconstruction and flux, one thread per face, same faces and outputs as k7_flux. Job
 // n = 2 m + gp: transverse stencil m, Gauss point gp + 1 (the second from the flipped stencil's closure).
 template <int DIR>
-__global__ void __launch_bounds__(kBlock7, 3) k7s_flux(const double* __restrict__ fl, const double* __restrict__ fr,
+__global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_flux(const double* __restrict__ fl, const double* __restrict__ fr,
                                                       double* __restrict__ fout, int nx, int ny, Gas gas, int reverse,
                                                       const StepCtl* __restrict__ ctl,
                                                       unsigned long long* __restrict__ counters,
