@@ -21,11 +21,6 @@ namespace wsr {
 
 constexpr int kAdvThreads = 256;
 constexpr int kAdvNmax = 2048;
-// Resident blocks per SM the register budget targets: the FP64 closure kernels otherwise take 255 registers
-// (one block per SM); 2 blocks measured 4% faster on the WENO7 Shu RK4 batch. The FP32 and JS kernels are
-// left to the compiler (a 3-block bound on the FP32 WENO5 batch measured no change).
-template <int M>
-constexpr int adv_min_blocks() { return M == M_SR64 ? 2 : 1; }
 
 // ---------------------------------------------------------------------------------------------
 // Generic MLP I -> H1 -> H2 -> H3 -> O (swish, swish, swish, 6 tanh(raw/6), softmax), packed
@@ -428,7 +423,7 @@ __device__ __forceinline__ double adv_rhs(const double* fl, const double* fr, co
 }
 
 template <int SCHEME, int M, int INTEG>
-__global__ void __launch_bounds__(kAdvThreads, adv_min_blocks<M>()) k_adv1d(double* __restrict__ u, const long long* __restrict__ offsets,
+__global__ void __launch_bounds__(kAdvThreads) k_adv1d(double* __restrict__ u, const long long* __restrict__ offsets,
                                                         const int* __restrict__ order, const double* __restrict__ vel,
                                                         const double* __restrict__ dxs, const int* __restrict__ nfull,
                                                         const double* __restrict__ dtf, const double* __restrict__ dtl,
