@@ -848,6 +848,17 @@ def bench_w7(args, world, rank, local):
             "state_finite": bool(torch.isfinite(u).all())}
     if counts is not None:
         line["closures_per_step"] = {k: v / max(res.steps, 1) for k, v in counts.items()}
+        # the closure kernels are FP64-bound: algorithmic work = the MLP pair's multiply-adds per closure
+        # evaluation (2 passes x (6x24 + 24x16 + 16x16 + 16x4) FMA = 3392 flop), device-counted evaluations
+        from weno_sr_publishing_b200 import _native as N
+        ctx = N.context(local)
+        peak64 = ctx.peak_tflops(64, C_stream(stream))
+        flop = 3392.0 * sum(counts.values())
+        achieved = flop / (ms * 1e-3) / 1e12
+        line["roofline"] = {"kernel": "k7s_normal + k7s_flux (the step's closure kernels)", "bound": "fp64",
+                            "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                            "traffic": None, "work": "MLP multiply-adds only (exp, rcp, features not counted)",
+                            "peak_source": f"measured FMA probe {peak64:.1f}"}
     if not args.skip_extras:
         host = torch.empty(u0.shape, dtype=torch.float64, pin_memory=True)
         host.copy_(u0.cpu())
