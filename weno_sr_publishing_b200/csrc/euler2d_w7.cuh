@@ -413,6 +413,10 @@ __device__ __forceinline__ double swish_tab(double z, const double* __restrict__
 
 // Dense layer of the WENO7 MLP for the direct (xa) and reflected (xb) inputs together; packed [in][out]
 // weights followed by the biases (the layout of the 1D path).
+// The multiply-adds are unrolled (the weights stay constant-bank operands); the activations run in a rolled loop
+// per layer, so the exp/reciprocal sequence is in the code once per layer instead of once per neuron: with 112
+// inlined copies per closure, instruction fetch was the kernels' first stall (63.5 against 79.6 ms per 1024^2
+// step).
 template <int NI, int NO>
 __device__ __forceinline__ void w7sr_dense_pair(const double* __restrict__ P, int w, int b, const double* xa,
                                                 const double* xb, double* ya, double* yb, bool act,
@@ -425,8 +429,15 @@ __device__ __forceinline__ void w7sr_dense_pair(const double* __restrict__ P, in
       za = za + xa[k] * P[w + k * NO + o];
       zb = zb + xb[k] * P[w + k * NO + o];
     }
-    ya[o] = act ? swish_tab(za, t32) : za;
-    yb[o] = act ? swish_tab(zb, t32) : zb;
+    ya[o] = za;
+    yb[o] = zb;
+  }
+  if (act) {
+#pragma unroll 1
+    for (int o = 0; o < NO; ++o) {
+      ya[o] = swish_tab(ya[o], t32);
+      yb[o] = swish_tab(yb[o], t32);
+    }
   }
 }
 
