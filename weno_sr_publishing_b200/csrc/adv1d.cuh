@@ -43,7 +43,7 @@ __device__ __forceinline__ void dense_pair(const T* __restrict__ P, int w, int b
       za = za + xa[k] * P[w + k * NO + o];
       zb = zb + xb[k] * P[w + k * NO + o];
     }
-    if (act) {
+    if (act && !kRollActAlways<T>) {
       za = swish<T>(za);
       zb = swish<T>(zb);
       if (BF16) {
@@ -54,6 +54,7 @@ __device__ __forceinline__ void dense_pair(const T* __restrict__ P, int w, int b
     ya[o] = za;
     yb[o] = zb;
   }
+  if (act) swish_rolled<T, kRollActAlways<T>>(ya, yb, NO);
 }
 
 template <typename T, bool BF16, int I, int H1, int H2, int H3, int O>

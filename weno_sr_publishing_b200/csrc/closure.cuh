@@ -260,7 +260,32 @@ __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__floa
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
 
-template <typename T, bool BF16>
+// FP64 activations in a rolled loop per layer after the layer's unrolled multiply-adds: inlined once per neuron,
+// the FP64 exp/reciprocal sequences can make a closure kernel's code large enough that instruction fetch stalls
+// it. Measured per kernel family: the 3D kernels run 37% faster rolled (64.5 -> 41.0 ms per shock-bubble SR-FP64
+// step) and the 1D batch 10% (dense_pair, adv1d.cuh); the 2D WENO5 kernels, with their smaller MLP, 3% slower,
+// so the choice is made per translation unit (WSR_ROLL_FP64_ACT, off by default). Single precision stays fully
+// unrolled (its exp and reciprocal are single hardware instructions).
+#ifndef WSR_ROLL_FP64_ACT
+#define WSR_ROLL_FP64_ACT 0
+#endif
+template <typename T>
+constexpr bool kRollAct = WSR_ROLL_FP64_ACT && sizeof(T) == 8;
+template <typename T>
+constexpr bool kRollActAlways = sizeof(T) == 8;
+
+template <typename T, bool ROLL = kRollAct<T>>
+__device__ __forceinline__ void swish_rolled(T* a, T* b, int n) {
+  if constexpr (ROLL) {
+#pragma unroll 1
+    for (int o = 0; o < n; ++o) {
+      a[o] = swish<T>(a[o]);
+      b[o] = swish<T>(b[o]);
+    }
+  }
+}
+
+template <typename T, bool BF16, bool ROLL = kRollAct<T>>
 __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5], const T xb[5], T ra[3], T rb[3]) {
   T ha[10], hb[10];
 #pragma unroll
@@ -271,13 +296,14 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
       za = fma_t(xa[k], P[kW1 + k * 10 + o], za);
       zb = fma_t(xb[k], P[kW1 + k * 10 + o], zb);
     }
-    ha[o] = swish<T>(za);
-    hb[o] = swish<T>(zb);
+    ha[o] = ROLL ? za : swish<T>(za);
+    hb[o] = ROLL ? zb : swish<T>(zb);
     if (BF16) {
       ha[o] = bf16r(ha[o]);
       hb[o] = bf16r(hb[o]);
     }
   }
+  swish_rolled<T, ROLL>(ha, hb, 10);
   T ga[6], gb[6];
 #pragma unroll
   for (int o = 0; o < 6; ++o) {
@@ -287,13 +313,14 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
       za = fma_t(ha[k], P[kW2 + k * 6 + o], za);
       zb = fma_t(hb[k], P[kW2 + k * 6 + o], zb);
     }
-    ga[o] = swish<T>(za);
-    gb[o] = swish<T>(zb);
+    ga[o] = ROLL ? za : swish<T>(za);
+    gb[o] = ROLL ? zb : swish<T>(zb);
     if (BF16) {
       ga[o] = bf16r(ga[o]);
       gb[o] = bf16r(gb[o]);
     }
   }
+  swish_rolled<T, ROLL>(ga, gb, 6);
   T ka[6], kb[6];
 #pragma unroll
   for (int o = 0; o < 6; ++o) {
@@ -303,13 +330,14 @@ __device__ __forceinline__ void mlp_pair(const T* __restrict__ P, const T xa[5],
       za = fma_t(ga[k], P[kW3 + k * 6 + o], za);
       zb = fma_t(gb[k], P[kW3 + k * 6 + o], zb);
     }
-    ka[o] = swish<T>(za);
-    kb[o] = swish<T>(zb);
+    ka[o] = ROLL ? za : swish<T>(za);
+    kb[o] = ROLL ? zb : swish<T>(zb);
     if (BF16) {
       ka[o] = bf16r(ka[o]);
       kb[o] = bf16r(kb[o]);
     }
   }
+  swish_rolled<T, ROLL>(ka, kb, 6);
   T ba[3], bb[3];
 #pragma unroll
   for (int o = 0; o < 3; ++o) {

@@ -27,6 +27,8 @@
 
 #include <cstring>
 
+// the 3D closure kernels apply the FP64 activations in rolled loops (closure.cuh)
+#define WSR_ROLL_FP64_ACT 1
 #include "closure.cuh"
 #include "wsr_ctx.cuh"
 
