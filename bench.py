@@ -84,34 +84,46 @@ def initial_state(n):
     return problems.make_quadrant_state(n, n, problems.seeded_quadrant_states(0), quadrature=1)
 
 
-def crop(state, n_crop):
-    """Centre n_crop x n_crop window of a padded state, re-padded (ghosts are refilled by the BC)."""
-    n = state.shape[0] - 6
-    a = (n - n_crop) // 2
-    out = np.zeros((n_crop + 6, n_crop + 6, 4))
-    out[3:3 + n_crop, 3:3 + n_crop] = state[3 + a:3 + a + n_crop, 3 + a:3 + a + n_crop]
-    return out
+CPU_SAMPLE_N = 256
 
 
-def cpu_sample(state, method, params, budget_s, fast=True):
-    """Time the CPU oracle (all host threads) on a centre crop of the benchmark state."""
+def cpu_sample_state(t0):
+    """The CPU-feasible sample of the benchmark workload: the same seeded quadrant problem on a 256 x 256 grid
+    of the whole unit square, advanced (untimed) to t0 with the oracle's WENO5-JS, so that it holds the same
+    waves as the 2000^2 state at t0 (a 2000^2 state at t0 takes thousands of 2000^2 steps, out of reach of
+    the CPU)."""
     from oracle import oracle as O
-    n_crop = 256
-    sub = crop(state, n_crop)
-    dx = 1.0 / params["n"]
-    prm = params["mlp"]
-    O.euler2d_run(sub, n_crop, n_crop, dx, dx, 0.4, 1.0, method, "transmissive", params=prm, fixed_steps=1, fast=fast)
-    steps, t0 = 0, time.perf_counter()
-    while True:
-        O.euler2d_run(sub, n_crop, n_crop, dx, dx, 0.4, 1.0, method, "transmissive", params=prm, fixed_steps=1,
-                      fast=fast)
+    from weno_sr_publishing_b200 import problems
+    m = CPU_SAMPLE_N
+    init = problems.make_quadrant_state(m, m, problems.seeded_quadrant_states(0), quadrature=1)
+    state, _, _, _ = O.euler2d_run(init, m, m, 1.0 / m, 1.0 / m, 0.4, t0, "js", "transmissive", fast=True)
+    return state
+
+
+def cpu_steps(state, method, mlp, steps):
+    """Wall time of `steps` full SSPRK3 steps of the C oracle (OpenMP, all host threads) on the sample state."""
+    from oracle import oracle as O
+    m = CPU_SAMPLE_N
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.euler2d_run(state, m, m, 1.0 / m, 1.0 / m, 0.4, 1.0, method, "transmissive", params=mlp, fixed_steps=1,
+                      fast=True)
+    return time.perf_counter() - t0
+
+
+def cpu_sample(method, mlp, t0, budget_s):
+    """The repo arm's CPU baseline: the reference arm's sample and timing, for as many steps as fit the budget."""
+    from oracle import oracle as O
+    m = CPU_SAMPLE_N
+    state = cpu_sample_state(t0)
+    cpu_steps(state, method, mlp, 1)
+    steps, el = 0, 0.0
+    while el < budget_s and steps < 200:
+        el += cpu_steps(state, method, mlp, 1)
         steps += 1
-        el = time.perf_counter() - t0
-        if el >= budget_s or steps >= 50:
-            break
-    return {"value": n_crop * n_crop * steps / el, "unit": UNIT, "cores": O.num_threads(fast),
-            "kind": "port", "sample": f"{steps} step(s) of a {n_crop}x{n_crop} centre crop of the benchmark state, "
-                                      f"{el:.1f} s, C oracle (OpenMP, -O3)"}
+    return {"value": m * m * steps / el, "unit": UNIT, "cores": O.num_threads(True), "kind": "port",
+            "sample": f"{steps} step(s) of the same seeded problem on a {m}x{m} grid of the whole unit square at "
+                      f"t0={t0} (C oracle, OpenMP, -O3), {el:.1f} s; the sample bench.py --impl reference times"}
 
 
 class ClockSampler:
@@ -163,40 +175,37 @@ class ClockSampler:
 
 
 def run_reference(args, rank):
-    """The reference has no CPU path for 2D Euler (Warp GPU kernels only); its CPU counterpart here is the
-    C restatement of those kernels in oracle/ (a port), timed on all host threads. The 2000^2 state at t0
-    is out of reach on the CPU, so the sample is the same problem on a 256^2 grid of the whole square,
-    advanced (untimed) to the same t0 with the oracle's WENO5-JS: the same physical mix of plateau and
-    wave regions per cell."""
+    """The reference's CPU counterpart of the 2D step: the reference has no CPU path for 2D Euler (its Warp
+    GPU kernels only, and warp-lang is not installed), so its algorithm runs as the C restatement in oracle/
+    (a port), timed on all host threads. A step is one full SSPRK3 step of the CPU-feasible sample of the
+    benchmark workload (cpu_sample_state: the same problem on a 256^2 grid at t0), W untimed and K timed; the
+    line's config names that grid, and ms_per_step is the measured time of one sample step."""
     if rank != 0:
         return
     from oracle import oracle as O
-    from weno_sr_publishing_b200 import problems
     from weno_sr_publishing_b200.checkpoint import MODELS_DIR
     mlp = None
     if args.method != "js":
         name = "weno5_sr_fp64_step012250.npz" if args.method == "sr_f64" else "weno5_sr_fp32_step016500.npz"
         mlp = {k: v for k, v in np.load(MODELS_DIR / name).items() if k != "meta_json"}
-    m = 256
-    init = problems.make_quadrant_state(m, m, problems.seeded_quadrant_states(0), quadrature=1)
-    state, _, _, _ = O.euler2d_run(init, m, m, 1.0 / m, 1.0 / m, 0.4, args.t0, "js", "transmissive", fast=True)
-    dx = 1.0 / m
-    for _ in range(args.warmup):
-        O.euler2d_run(state, m, m, dx, dx, 0.4, 1.0, args.method, "transmissive", params=mlp, fixed_steps=1,
-                      fast=True)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        O.euler2d_run(state, m, m, dx, dx, 0.4, 1.0, args.method, "transmissive", params=mlp, fixed_steps=1,
-                      fast=True)
-    el = time.perf_counter() - t0
+    m = CPU_SAMPLE_N
+    state = cpu_sample_state(args.t0)
+    cpu_steps(state, args.method, mlp, max(args.warmup, 0))
+    el = cpu_steps(state, args.method, mlp, args.steps)
     v = m * m * args.steps / el
+    cfg = workload_config(args, args.gpus)
+    cfg["workload"] = (f"2D Euler quadrant Riemann problem, seed 0, on a {m}x{m} grid of the unit square at "
+                       f"t0={args.t0}: the CPU-feasible sample of the {args.n}x{args.n} workload")
+    cfg["grid"] = [m, m]
+    cfg["sample_of"] = workload_config(args, args.gpus)["workload"]
+    cfg["l2_policy"] = "CPU run: state 4 x 2.1 MB"
     base = {"value": v, "unit": UNIT, "cores": O.num_threads(True), "kind": "port",
-            "sample": f"{args.steps} steps of the same problem on a {m}x{m} grid at t0={args.t0} "
-                      f"(C oracle, OpenMP), {el:.1f} s"}
+            "sample": f"{args.steps} steps (after {args.warmup} untimed) of the same problem on a {m}x{m} grid at "
+                      f"t0={args.t0} (C oracle, OpenMP, -O3), {el:.1f} s"}
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * args.n * args.n / v, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(args, args.gpus), "impl": "reference", "cpu_baseline": base,
+            "config": cfg, "impl": "reference", "cpu_baseline": base,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -365,6 +374,8 @@ def main():
     line["kernels"] = {k: {kk: v[kk] for kk in ("ms_per_launch", "launches", "share", "bound", "frac")}
                        for k, v in per_kernel.items()}
     line["closure_tally_per_step"] = {k: {"mlp": v[0], "plateau": v[1]} for k, v in tallies.items()}
+    if not args.skip_extras and not slabs and args.method != "js":
+        line["precision_l1"] = precision_block(bufs, start, p, mlp, K, ws)
 
     if not args.skip_extras and slabs:
         # end to end per rank: pinned host slab -> device, one step of the decomposed grid, device -> host
@@ -401,12 +412,14 @@ def main():
         host = torch.empty(p.padded_shape, dtype=torch.float64, pin_memory=True)
         host.copy_(start.cpu())
         for _ in range(max(W, 1)):
-            E.advance_host(host, p, 1, args.method, "transmissive", mlp_params=mlp, bufs=bufs, ws=ws, device=dev)
+            E.advance_host(host, p, 1, args.method, "transmissive", mlp_params=mlp, bufs=bufs, ws=ws, device=dev,
+                           async_readback=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(K):
-            E.advance_host(host, p, 1, args.method, "transmissive", mlp_params=mlp, bufs=bufs, ws=ws, device=dev)
+            E.advance_host(host, p, 1, args.method, "transmissive", mlp_params=mlp, bufs=bufs, ws=ws, device=dev,
+                           async_readback=True)
         E.host_copies_done(dev)  # the last read-back is inside the timed region
         e1.record(stream)
         torch.cuda.synchronize()
@@ -418,10 +431,10 @@ def main():
         nbytes = int(np.prod(p.padded_shape)) * 8
         line["e2e"] = {"value": world * n * n * K / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                        "d2h_bytes_per_step": nbytes,
-                       "api": "weno_sr_publishing_b200.euler2d.advance_host (pinned host buffer, 1 step per call)"}
+                       "api": "weno_sr_publishing_b200.euler2d.advance_host (pinned host buffer, 1 step per call, "
+                              "async_readback=True; the last read-back completes inside the timed region)"}
         if rank == 0 and world == 1:
-            line["cpu_baseline"] = cpu_sample(start.cpu().numpy(), args.method, {"n": n, "mlp": mlp},
-                                              args.cpu_seconds)
+            line["cpu_baseline"] = cpu_sample(args.method, mlp, args.t0, args.cpu_seconds)
         if rank == 0:
             line["matched_l1"] = matched_l1_block(args.method, mlp, dev)
     if world > 1 or slabs:
@@ -429,6 +442,21 @@ def main():
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def precision_block(bufs, start, p, mlp, steps, ws):
+    """Density L1 distance (sum |rho_a - rho_b| dx dy) after the timed steps from the benchmark state between
+    the closure evaluated in FP64 and in FP32 / BF16, with the same checkpoint's weights."""
+    from weno_sr_publishing_b200 import euler2d as E
+    rho = {}
+    for m in ("sr_f64", "sr_f32", "sr_bf16"):
+        bufs[0].copy_(start)
+        r = E.run(bufs, p, 1.0, m, "transmissive", mlp_params=mlp, fixed_steps=steps, ws=ws)
+        rho[m] = bufs[r.final_slot][3:3 + p.ny, 3:3 + p.nx, 0].double().cpu().numpy()
+    l1 = {m: float(np.abs(rho[m] - rho["sr_f64"]).sum() * p.dx * p.dy) for m in ("sr_f32", "sr_bf16")}
+    return {"against": "the same steps with the closure in FP64 (same checkpoint)", "steps": steps,
+            "rho_l1": l1, "bound": {"sr_f32": 1e-8, "sr_bf16": 5e-4},
+            "within_bound": {"sr_f32": l1["sr_f32"] <= 1e-8, "sr_bf16": l1["sr_bf16"] <= 5e-4}}
 
 
 def matched_l1_block(method, mlp, dev):

@@ -251,14 +251,19 @@ int wsr_probe_exp_tab(wsr_ctx *ctx, const double *x, double *out, int n, void *s
 
 /* ---- stage without any allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc (a host that owns all device memory through its own pool,
- * or a step that must not pay cudaMalloc's implicit synchronisation). Same result as
- * wsr_euler2d_stage, but the scratch lives in a static device array of WSR_NOALLOC_SCRATCH_BYTES
- * (32 MiB, enough for grids up to 400 x 400) that every GPU loading the library holds until exit.
- * No context: `closure_params` is a HOST array of the 189 packed parameters (NULL for WSR_METHOD_JS).
- * Runs on the calling thread's current device; `stream` must belong to it. The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress) and must come before any stream capture
- * on that device. Grids whose workspace exceeds the array return WSR_ERR_SCRATCH_LIMIT. All calls on
- * a device share the array: calls that overlap on the GPU race and must be serialised by the caller.
+ * or a step that must not pay cudaMalloc's implicit synchronisation). One SSPRK3 stage like
+ * wsr_euler2d_stage, with its scratch in a static device array of WSR_NOALLOC_SCRATCH_BYTES (32 MiB,
+ * enough for grids up to 400 x 400) that every GPU loading the library holds until exit.
+ * Supported: method WSR_METHOD_JS, WSR_METHOD_Z, WSR_METHOD_SR_F64, WSR_METHOD_SR_F32 or WSR_METHOD_SR_BF16;
+ * bc WSR_BC_TRANSMISSIVE or WSR_BC_PERIODIC (no double-Mach boundary, no WSR_BC_Y_HALO); flux WSR_FLUX_HLLC or
+ * WSR_FLUX_FORCE. Anything else returns WSR_ERR_ARG.
+ * No context: `closure_params` is a HOST array of the 189 packed parameters (NULL for WSR_METHOD_JS and
+ * WSR_METHOD_Z). Runs on the calling thread's current device; `stream` must belong to it. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and must come before any stream capture on
+ * that device; the address is cached for the process and is not valid after cudaDeviceReset. On entry the
+ * call clears this thread's pending CUDA launch error (cudaGetLastError), so that WSR_ERR_CUDA reports its own
+ * launches. Grids whose workspace exceeds the array return WSR_ERR_SCRATCH_LIMIT. All calls on a device share
+ * the array: calls that overlap on the GPU race and must be serialised by the caller.
  * Returns status codes only (no message). */
 #define WSR_ERR_SCRATCH_LIMIT 4
 #define WSR_NOALLOC_SCRATCH_BYTES (32u << 20)

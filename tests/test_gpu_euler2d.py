@@ -198,3 +198,45 @@ def test_invalid_arguments_raise():
         E.stage(u, u, u, p, 1e-3, 1, "js", "reflective")
     with pytest.raises(ValueError):
         E.stage(u, u, u, p, 1e-3, 1, "sr_f64", "transmissive", mlp_params=None)
+
+
+# FORCE flux (warp_weno5_helpers.py:401-435): the oracle's FORCE is bit-identical to the reference's; the CUDA
+# path's FORCE stage and runs are held to the HLLC stage tolerances.
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32"])
+@pytest.mark.parametrize("rk", [1, 2, 3])
+def test_force_stage_matches_oracle(case, method, rk):
+    e = np.load(G / f"euler2d_{case}.npz")
+    nx, ny, bc = int(e["nx"]), int(e["ny"]), str(e["bc"])
+    p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4)
+    u0 = e["initial"]
+    rng = np.random.default_rng(10 + rk)
+    u_stage = u0 * (1.0 + 0.01 * rng.uniform(-1, 1, u0.shape)) if rk > 1 else u0
+    dt = 0.3 * min(p.dx, p.dy) / O.max_speed(u0, nx, ny)
+    ref = O.euler2d_stage(u_stage, u0, np.zeros_like(u0), nx, ny, p.dx, p.dy, dt, rk, method, bc, flux="force",
+                          params=PARAMS[method])
+    out = torch.zeros(p.padded_shape, dtype=torch.float64, device=DEV)
+    E.stage(_t(u_stage), _t(u0), out, p, dt, rk, method, bc, mlp_params=PARAMS[method], flux="force")
+    err = _rel(_interior(out.cpu().numpy(), nx, ny), _interior(ref, nx, ny))
+    assert err <= STAGE_TOL[method], err
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("method,tol", [("js", 1e-11), ("sr_f64", 1e-11), ("sr_f32", 1e-5)])
+def test_force_ten_step_run_matches_oracle(case, method, tol):
+    e = np.load(G / f"euler2d_{case}.npz")
+    nx, ny, bc = int(e["nx"]), int(e["ny"]), str(e["bc"])
+    init = e["initial"]
+    p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4, t_end=1.0)
+    ref, rdts, rsteps, _ = O.euler2d_run(init, nx, ny, p.dx, p.dy, 0.4, 1.0, method, bc, flux="force",
+                                         params=PARAMS[method], fixed_steps=10)
+    bufs = [_t(init)] + [torch.zeros_like(_t(init)) for _ in range(3)]
+    res = E.run(bufs, p, 1.0, method, bc, mlp_params=PARAMS[method], flux="force", fixed_steps=10)
+    assert res.steps == rsteps == 10
+    got = bufs[res.final_slot].cpu().numpy()
+    assert _rel(_interior(got, nx, ny), _interior(ref, nx, ny)) <= tol
+    np.testing.assert_allclose(res.dts, rdts, rtol=100 * tol)
+    # FORCE is a different scheme: the run must not coincide with the HLLC run
+    bufs2 = [_t(init)] + [torch.zeros_like(_t(init)) for _ in range(3)]
+    res2 = E.run(bufs2, p, 1.0, method, bc, mlp_params=PARAMS[method], fixed_steps=10)
+    assert _rel(_interior(bufs2[res2.final_slot].cpu().numpy(), nx, ny), _interior(got, nx, ny)) > 1e-8

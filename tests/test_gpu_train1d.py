@@ -110,6 +110,57 @@ def test_gradients_match_oracle_multi_segment(prec):
     assert _nrel(gu0.cpu().numpy(), guo) <= 5e-2
 
 
+LONG = dict(n=64, B=4, steps=2048, every=32)  # 1024 cells of propagation at CFL 0.5, 64 checkpoint segments
+
+
+def _long_case(prec):
+    rng = np.random.default_rng(31)
+    n, B, steps = LONG["n"], LONG["B"], LONG["steps"]
+    desc, _ = P.make_profiles(rng, B, n)
+    vel = T.balanced_velocities(B)
+    src = "weno5_sr_fp64_step012250.npz" if prec == "f64" else "weno5_sr_fp32_step016500.npz"
+    p = np.concatenate([np.load(M / src)[k].reshape(-1).astype(np.float64) for k in T.PARAM_NAMES])
+    u0 = P.cell_averages(desc, n, 0.0)
+    return desc, vel, p, u0
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_gradients_match_oracle_at_1024_cells_of_propagation(prec):
+    """The unroll length of the training workload's longest distance: B = 4 mixed families, N = 64,
+    2048 SSPRK3 steps (1024 cells at CFL 0.5) with a checkpoint every 32 steps, so the adjoint recomputes 64
+    segments; the parameter gradient is compared element-wise with autograd through the whole unroll."""
+    desc, vel, p, u0 = _long_case(prec)
+    n, steps = LONG["n"], LONG["steps"]
+    targets = np.stack([P.cell_averages(desc, n, vel * (k * 0.5 / n)) for k in range(1, steps + 1)], axis=1)
+    lo, go, guo, fo = O.loss_and_grads(p, u0, targets, vel, 0.5 / n, float(n), prec)
+    loss, grad, gu0, fin = T.loss_and_grads(p, _batch(desc, vel, n, steps, u0, every=LONG["every"]), prec,
+                                            want_u0=True)
+    assert abs(float(loss) - lo) <= (1e-10 if prec == "f64" else 1e-5) * lo
+    assert _rel(fin.cpu().numpy(), fo) <= (1e-10 if prec == "f64" else 1e-5)
+    assert _rel(grad.cpu().numpy(), go) <= GTOL[prec], _rel(grad.cpu().numpy(), go)
+    assert _nrel(gu0.cpu().numpy(), guo) <= 5e-2
+
+
+def test_directional_finite_differences_at_1024_cells_of_propagation():
+    """Central differences of the FP64 loss over the full 2048-step unroll along random parameter directions."""
+    desc, vel, p, u0 = _long_case("f64")
+    n, steps = LONG["n"], LONG["steps"]
+    _, grad, _, _ = T.loss_and_grads(p, _batch(desc, vel, n, steps, u0, every=LONG["every"]), "f64")
+    grad = grad.cpu().numpy()
+    rng = np.random.default_rng(37)
+
+    def L(pp):
+        return float(T.loss_and_grads(pp, _batch(desc, vel, n, steps, u0, every=LONG["every"]), "f64")[0])
+
+    errs = []
+    for _ in range(4):
+        v = rng.standard_normal(p.size)
+        h = 1e-6
+        fd = (L(p + h * v) - L(p - h * v)) / (2 * h)
+        errs.append(abs(fd - grad @ v) / max(abs(grad @ v), 1e-12))
+    assert np.median(errs) <= 1e-4, errs
+
+
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_initial_state_gradient_matches_oracle_on_smooth_profiles(prec):
     """Without near-plateau stencils the state adjoint is well conditioned and agrees tightly."""
@@ -217,12 +268,13 @@ def test_invalid_arguments_raise():
         T.loss_and_grads(p, _batch(desc, [1.0, -1.0], 2048, 2), "f64")  # n > 1024
 
 
-def test_training_from_initialisation_beats_js(tmp_path):
-    """300 Adam steps from the reference's initialisation (FP32 closure, N = 96, B = 256, distances 2, 8,
-    64 cells) give a closure whose error under the reference's evaluation protocol (rk3_advection.py:533-560,
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_training_from_initialisation_beats_js(tmp_path, precision):
+    """300 Adam steps from the reference's initialisation (FP32 or FP64 closure, N = 96, B = 256, distances 2,
+    8, 64 cells) give a closure whose error under the reference's evaluation protocol (rk3_advection.py:533-560,
     distance 20 cells, N = 96, balanced velocities) is below WENO5-JS for every profile family."""
     cfg = T.TrainConfig(out_dir=tmp_path / "run", steps=300, grid=96, batch=256, distances=(2, 8, 64),
-                        precision="f32", lr=1e-3, lr_final=2e-4, log_interval=50, checkpoint_interval=1000,
+                        precision=precision, lr=1e-3, lr_final=2e-4, log_interval=50, checkpoint_interval=1000,
                         state_interval=1000, device=DEV)
     out = T.train(cfg)
     assert out["skipped"] == 0
@@ -238,7 +290,7 @@ def test_training_from_initialisation_beats_js(tmp_path):
     assert float(np.mean(ratios)) < 0.7, ratios
     # the written checkpoint is a reference-format closure
     last = tmp_path / "run" / "checkpoints" / "model_step_000300.npz"
-    m = T.ClosureMLP.from_checkpoint(last, torch.float32)
+    m = T.ClosureMLP.from_checkpoint(last, torch.float32 if precision == "f32" else torch.float64)
     assert torch.equal(m.packed(), out["model"].packed().detach().cpu())
 
 

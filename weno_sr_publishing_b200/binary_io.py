@@ -1,51 +1,60 @@
 """Step files of the 3D solver and their comparison (warp_weno5_3d_rk3/binary_io.py).
 
-Format (the C++ code's, little-endian native packing): a 20-byte header ``uint32 nz, ny, nx; float64 time``
-followed by ``float64 primitive[nz][ny][nx][5]`` with components (rho, u, v, w, p) of the interior cells.
-``read_step`` raises ValueError on a truncated header or payload and on trailing bytes, as the reference does.
+Format (an interface, kept as the reference's C++ code writes it): a packed 20-byte header
+``uint32 nz, ny, nx; float64 time`` followed by ``float64 primitive[nz][ny][nx][5]`` with components
+(rho, u, v, w, p) of the interior cells, all little-endian. ``read_step`` raises ValueError on a truncated
+header or payload and on trailing bytes, the reference's error type for those cases.
 """
 from __future__ import annotations
 
 import hashlib
 import json
-import struct
 from pathlib import Path
 
 import numpy as np
 import torch
 
-HEADER = struct.Struct("=IIId")
+# The 20-byte header as one packed little-endian record (the C++ writer's native packing on x86).
+STEP_HEADER = np.dtype([("nz", "<u4"), ("ny", "<u4"), ("nx", "<u4"), ("time", "<f8")])
 COMPONENT_NAMES = ("rho", "u", "v", "w", "p")
 GHOST = 3
 
 
+def _payload_shape(head) -> tuple[int, int, int, int]:
+    return int(head["nz"]), int(head["ny"]), int(head["nx"]), len(COMPONENT_NAMES)
+
+
 def read_step(path: str | Path) -> tuple[float, np.ndarray]:
+    """(time, primitive[nz][ny][nx][5]) of a step file. The file size is checked against the size the header
+    implies before any payload is read: a short header, a short payload or trailing bytes raise ValueError."""
     path = Path(path)
-    with path.open("rb") as stream:
-        head = stream.read(HEADER.size)
-        if len(head) != HEADER.size:
-            raise ValueError(f"truncated step header: {path}")
-        nz, ny, nx, time = HEADER.unpack(head)
-        count = int(nz) * int(ny) * int(nx) * 5
-        values = np.fromfile(stream, dtype=np.float64, count=count)
-        extra = stream.read(1)
-    if values.size != count:
-        raise ValueError(f"truncated payload: expected {count}, got {values.size}")
-    if extra:
-        raise ValueError(f"unexpected trailing bytes in {path}")
-    return float(time), values.reshape((nz, ny, nx, 5))
+    size = path.stat().st_size
+    if size < STEP_HEADER.itemsize:
+        raise ValueError(f"{path}: {size} bytes, shorter than the {STEP_HEADER.itemsize}-byte step header")
+    head = np.fromfile(path, dtype=STEP_HEADER, count=1)[0]
+    shape = _payload_shape(head)
+    expected = STEP_HEADER.itemsize + 8 * int(np.prod(shape, dtype=np.int64))
+    if size != expected:
+        what = "truncated payload" if size < expected else "trailing bytes after the payload"
+        raise ValueError(f"{path}: {what}: header {shape[:3]} implies {expected} bytes, file has {size}")
+    values = np.fromfile(path, dtype="<f8", offset=STEP_HEADER.itemsize).reshape(shape)
+    return float(head["time"]), values
 
 
 def write_step(path: str | Path, time: float, primitive: np.ndarray) -> None:
-    primitive = np.ascontiguousarray(primitive, dtype=np.float64)
-    if primitive.ndim != 4 or primitive.shape[-1] != 5:
-        raise ValueError("primitive must have shape (nz, ny, nx, 5)")
-    nz, ny, nx, _ = primitive.shape
+    """Write one step file: the header record, then the primitive array as little-endian float64."""
+    prim = np.asarray(primitive)
+    if prim.ndim != 4 or prim.shape[-1] != len(COMPONENT_NAMES):
+        raise ValueError(f"primitive must have shape (nz, ny, nx, 5), got {prim.shape}")
+    head = np.zeros((), dtype=STEP_HEADER)
+    head["nz"], head["ny"], head["nx"] = prim.shape[:3]
+    head["time"] = time
     path = Path(path)
     path.parent.mkdir(parents=True, exist_ok=True)
-    with path.open("wb") as stream:
-        stream.write(HEADER.pack(nz, ny, nx, float(time)))
-        primitive.tofile(stream)
+    body = np.ascontiguousarray(prim, dtype="<f8")
+    with path.open("wb") as out:
+        out.write(head.tobytes())
+        out.write(memoryview(body).cast("B"))
 
 
 def primitive_interior(q, nx: int, ny: int, nz: int) -> np.ndarray:
@@ -103,7 +112,7 @@ def compare_steps(candidate: str | Path, reference: str | Path) -> dict:
         "file_bitwise_identical": Path(candidate).read_bytes() == Path(reference).read_bytes(),
         "array_bitwise_identical": bool(np.all(same)),
         "header": {"shape_equal": True, "candidate_time": tc, "reference_time": tr,
-                   "time_bitwise_equal": struct.pack("=d", tc) == struct.pack("=d", tr)},
+                   "time_bitwise_equal": np.float64(tc).tobytes() == np.float64(tr).tobytes()},
         "unequal_count": int(np.count_nonzero(~same)),
         "finite_pair_count": int(np.count_nonzero(np.isfinite(uc) & np.isfinite(ur))),
         "normalized_l1": float(np.sum(err)) / denom if denom else (0.0 if not np.any(err) else float("inf")),

@@ -13,7 +13,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libwsr.so"
-SOURCES = [CSRC / "wsr_api.cu", CSRC / "euler3d.cu"]
+SOURCES = [CSRC / "wsr_api.cu", CSRC / "wsr_api_1d.cu", CSRC / "wsr_api_w7.cu", CSRC / "euler3d.cu"]
 # euler3d.cu reproduces the reference's 3D Warp module, which is compiled without contraction
 EXTRA_FLAGS = {"euler3d.cu": ["-fmad=false"]}
 HEADERS = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "wsr.h"]

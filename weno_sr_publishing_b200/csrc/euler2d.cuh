@@ -80,7 +80,7 @@ __device__ __forceinline__ void store_cell(double* __restrict__ u, size_t idx, c
 
 // Double-Mach reflection (REFSYM:26-124): a Mach-10 shock through (1/6, 0) at 60 degrees to the wall.
 // Exact pre/post-shock state at (x, y) and time t, with round-to-nearest operations in the reference's order.
-__device__ __noinline__ d4 double_mach_state(double x, double y, double t, double g) {
+static __device__ __noinline__ d4 double_mach_state(double x, double y, double t, double g) {
   const double r3 = __dsqrt_rn(3.0);
   const double shock_x = __dadd_rn(__dadd_rn(1.0 / 6.0, __ddiv_rn(y, r3)), __ddiv_rn(__dmul_rn(20.0, t), r3));
   double rho = 1.4, u = 0.0, v = 0.0, p = 1.0;
@@ -99,7 +99,7 @@ __device__ __noinline__ d4 double_mach_state(double x, double y, double t, doubl
 // (all columns), the left columns and the bottom rows left of x = 1/6 (there at y = 0); a reflection of the
 // interior (v negated, column clamped to the interior) on the bottom rows right of it; a copy of the last
 // interior column on the right.
-__device__ __noinline__ d4 double_mach_ghost(const double* __restrict__ u, int nx, int ny, int pj, int pi,
+static __device__ __noinline__ d4 double_mach_ghost(const double* __restrict__ u, int nx, int ny, int pj, int pi,
                                              const StageBc& bc, double t, double g) {
   const int nxt = nx + 2 * kGhost;
   const double x = __dmul_rn((double)(pi - kGhost) + 0.5, bc.dx);
@@ -450,7 +450,7 @@ __device__ __forceinline__ void block_max_to(unsigned long long v, unsigned long
 
 // SSPRK3 update of the interior (DEPLOY:1027-1056) and, on stage 3, the max wave speed of the new
 // state plus the health flags that the reference reads back on the host.
-__global__ void __launch_bounds__(256) k_update(const double* __restrict__ u_stage, const double* __restrict__ u0,
+static __global__ void __launch_bounds__(256) k_update(const double* __restrict__ u_stage, const double* __restrict__ u0,
                                                 double* __restrict__ u_out, const double* __restrict__ fx,
                                                 const double* __restrict__ fy, int nx, int ny, int rk, double g,
                                                 StepCtl* __restrict__ ctl) {
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ u_sta
   }
 }
 
-__global__ void __launch_bounds__(256) k_max_speed(const double* __restrict__ u, int nx, int ny, double g,
+static __global__ void __launch_bounds__(256) k_max_speed(const double* __restrict__ u, int nx, int ny, double g,
                                                    unsigned long long* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(256) k_max_speed(const double* __restrict__ u,
 
 // dt for the next step (REFSYM:477-483, wh:189-207), on one thread. Also resets the max-speed slot
 // that the coming stage-3 update accumulates into. `dts` records each step's dt.
-__global__ void k_step_begin(StepCtl* ctl, double* dts) {
+static __global__ void k_step_begin(StepCtl* ctl, double* dts) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (ctl->done) return;
   if (ctl->check_health && ctl->health_bad &&
@@ -529,14 +529,14 @@ __global__ void k_step_begin(StepCtl* ctl, double* dts) {
   dts[ctl->steps] = dt;
 }
 
-__global__ void k_set_dt_ratios(StepCtl* ctl, double dx, double dy) {
+static __global__ void k_set_dt_ratios(StepCtl* ctl, double dx, double dy) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (ctl->done) return;
   ctl->dt_dx = ctl->dt / dx;
   ctl->dt_dy = ctl->dt / dy;
 }
 
-__global__ void k_step_end(StepCtl* ctl) {
+static __global__ void k_step_end(StepCtl* ctl) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (ctl->done) return;
   ctl->t = ctl->t + ctl->dt;

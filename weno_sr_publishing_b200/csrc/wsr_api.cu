@@ -1,4 +1,5 @@
-// extern "C" entry points of libwsr.so (declared in include/wsr.h).
+// extern "C" entry points of libwsr.so for the 2D WENO5 path, the throughput probes and the no-allocation
+// stage (declared in include/wsr.h); the 1D/training and WENO7 entry points are in wsr_api_1d.cu and wsr_api_w7.cu.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -9,10 +10,7 @@
 #include <new>
 
 #include "../../include/wsr.h"
-#include "adv1d.cuh"
 #include "euler2d.cuh"
-#include "euler2d_w7.cuh"
-#include "train1d.cuh"
 #include "wsr_ctx.cuh"
 
 using namespace wsr;
@@ -28,8 +26,6 @@ struct Ws2d {
   double* dts;  // ring of kDtsRing
   double *xl, *xr, *yl, *yr, *fx, *fy;
 };
-
-size_t cells_bytes(size_t n) { return align_up(n * 4 * sizeof(double)); }
 
 size_t ws_bytes(int nx, int ny) {
   size_t b = align_up(sizeof(StepCtl)) + align_up(sizeof(int)) + align_up(8 * sizeof(unsigned long long)) +
@@ -481,246 +477,6 @@ int wsr_euler2d_counters(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, 
 
 }  // extern "C"
 
-// ---------------------------------------------------------------------------------------------
-// Batched 1D advection
-// ---------------------------------------------------------------------------------------------
-namespace {
-
-template <int SCHEME, int M>
-const typename AdvParams<SCHEME, M>::type& adv_params_of(const wsr_ctx* ctx);
-template <>
-const NoParams& adv_params_of<5, M_JS>(const wsr_ctx*) {
-  static const NoParams np{};
-  return np;
-}
-template <>
-const NoParams& adv_params_of<7, M_JS>(const wsr_ctx*) {
-  static const NoParams np{};
-  return np;
-}
-template <>
-const Mlp5d& adv_params_of<5, M_SR64>(const wsr_ctx* c) { return c->p64; }
-template <>
-const Mlp5f& adv_params_of<5, M_SR32>(const wsr_ctx* c) { return c->p32; }
-template <>
-const Mlp5f& adv_params_of<5, M_SRBF16>(const wsr_ctx* c) { return c->pbf16; }
-template <>
-const Mlp7d& adv_params_of<7, M_SR64>(const wsr_ctx* c) { return c->q64; }
-template <>
-const Mlp7f& adv_params_of<7, M_SR32>(const wsr_ctx* c) { return c->q32; }
-template <>
-const Mlp7f& adv_params_of<7, M_SRBF16>(const wsr_ctx* c) { return c->qbf16; }
-
-struct AdvArgs {
-  double* u;
-  const long long* offsets;
-  const int* order;
-  const double *vel, *dx;
-  const int* nfull;
-  const double *dtf, *dtl;
-  int B, nmax, opts;
-  int *fallbacks, *errors;
-  unsigned long long* counters;
-};
-
-template <int SCHEME, int M, int INTEG>
-int adv_launch(wsr_ctx* ctx, const AdvArgs& a, cudaStream_t st) {
-  const size_t smem = adv_smem_bytes<INTEG>(a.nmax);
-  auto kern = k_adv1d<SCHEME, M, INTEG>;
-  WSR_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<a.B, kAdvThreads, smem, st>>>(a.u, a.offsets, a.order, a.vel, a.dx, a.nfull, a.dtf, a.dtl, a.B, a.nmax,
-                                        a.opts, a.fallbacks, a.errors, a.counters, adv_params_of<SCHEME, M>(ctx));
-  WSR_LAUNCHED(ctx, "k_adv1d");
-  return WSR_OK;
-}
-
-template <int SCHEME, int INTEG>
-int adv_dispatch_m(wsr_ctx* ctx, int method, const AdvArgs& a, cudaStream_t st) {
-  switch (method) {
-    case WSR_METHOD_JS:
-      return adv_launch<SCHEME, M_JS, INTEG>(ctx, a, st);
-    case WSR_METHOD_SR_F64:
-      return adv_launch<SCHEME, M_SR64, INTEG>(ctx, a, st);
-    case WSR_METHOD_SR_F32:
-      return adv_launch<SCHEME, M_SR32, INTEG>(ctx, a, st);
-    default:
-      return adv_launch<SCHEME, M_SRBF16, INTEG>(ctx, a, st);
-  }
-}
-
-}  // namespace
-
-extern "C" size_t wsr_adv1d_workspace_bytes(void) { return 256; }
-
-extern "C" int wsr_adv1d_run(wsr_ctx* ctx, double* u, const long long* offsets, const int* order,
-                             const double* velocity, const double* dx, const int* n_full, const double* dt_full,
-                             const double* dt_last, int B, int nmax, int scheme, int method, int integrator, int opts,
-                             int* fallbacks_out, int* errors_out, unsigned long long* counters_out, void* workspace,
-                             size_t workspace_bytes, void* stream) {
-  if (!ctx) return WSR_ERR_ARG;
-  if (B < 1) return fail(ctx, WSR_ERR_ARG, "B must be >= 1");
-  if (scheme != 5 && scheme != 7) return fail(ctx, WSR_ERR_ARG, "scheme must be 5 or 7 (got %d)", scheme);
-  if (integrator != WSR_INTEG_SSPRK3 && integrator != WSR_INTEG_SHU_RK4)
-    return fail(ctx, WSR_ERR_ARG, "bad integrator %d", integrator);
-  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
-  if (nmax < (scheme == 5 ? 5 : 7) || nmax > kAdvNmax)
-    return fail(ctx, WSR_ERR_ARG, "nmax must be in [%d, %d] (got %d)", scheme == 5 ? 5 : 7, kAdvNmax, nmax);
-  if (method != WSR_METHOD_JS && !(scheme == 5 ? ctx->have_closure : ctx->have_closure7))
-    return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before uploading a WENO%d closure", scheme);
-  if (!u || !offsets || !velocity || !dx || !n_full || !dt_full || !dt_last)
-    return fail(ctx, WSR_ERR_ARG, "null array argument");
-  if (!workspace || workspace_bytes < wsr_adv1d_workspace_bytes())
-    return fail(ctx, WSR_ERR_ARG, "workspace too small");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  int* fb = static_cast<int*>(workspace);
-  int* err = fb + 1;
-  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(static_cast<char*>(workspace) + 16);
-  WSR_CUDA(ctx, cudaMemsetAsync(workspace, 0, 32, st));
-  AdvArgs a{u, offsets, order, velocity, dx, n_full, dt_full, dt_last, B, nmax, opts, fb, err, cnt};
-  int rc;
-  if (scheme == 5)
-    rc = integrator == WSR_INTEG_SSPRK3 ? adv_dispatch_m<5, 0>(ctx, method, a, st) : adv_dispatch_m<5, 1>(ctx, method, a, st);
-  else
-    rc = integrator == WSR_INTEG_SSPRK3 ? adv_dispatch_m<7, 0>(ctx, method, a, st) : adv_dispatch_m<7, 1>(ctx, method, a, st);
-  if (rc) return rc;
-  if (fallbacks_out || errors_out || counters_out) {
-    int host[4];
-    unsigned long long hc[2];
-    WSR_CUDA(ctx, cudaMemcpyAsync(host, workspace, 16, cudaMemcpyDeviceToHost, st));
-    WSR_CUDA(ctx, cudaMemcpyAsync(hc, cnt, 16, cudaMemcpyDeviceToHost, st));
-    WSR_CUDA(ctx, cudaStreamSynchronize(st));
-    if (fallbacks_out) *fallbacks_out = host[0];
-    if (errors_out) *errors_out = host[1];
-    if (counters_out) {
-      counters_out[0] = hc[0];
-      counters_out[1] = hc[1];
-    }
-    if (host[1]) return fail(ctx, WSR_ERR_ARG, "%d trajectories had fewer cells than the stencil or more than nmax", host[1]);
-  }
-  return WSR_OK;
-}
-
-namespace {
-
-struct WsTrain {
-  double* ck;         // B x K x n checkpoint states (every ckpt_every-th step)
-  double* seg;        // B x min(every, steps) x 3 x n stage states of the segment being reversed
-  unsigned* signs;    // B x steps x ceil(n/32) x 2 ballot words of sign(u - e)
-  double* loss_part;  // B
-  double* grad_part;  // B x 189
-};
-
-size_t train_ws_bytes(int B, int n, int steps, int every) {
-  const size_t K = (size_t)(steps + every - 1) / every, seg = (size_t)(every < steps ? every : steps);
-  const size_t words = (size_t)(n + 31) / 32;
-  return align_up((size_t)B * K * n * sizeof(double)) + align_up((size_t)B * seg * 3 * n * sizeof(double)) +
-         align_up((size_t)B * steps * words * 2 * sizeof(unsigned)) + align_up((size_t)B * sizeof(double)) +
-         align_up((size_t)B * kP5 * sizeof(double));
-}
-
-WsTrain carve_train(void* base, int B, int n, int steps, int every) {
-  const size_t K = (size_t)(steps + every - 1) / every, seg = (size_t)(every < steps ? every : steps);
-  const size_t words = (size_t)(n + 31) / 32;
-  char* p = static_cast<char*>(base);
-  WsTrain w;
-  w.ck = reinterpret_cast<double*>(p);
-  p += align_up((size_t)B * K * n * sizeof(double));
-  w.seg = reinterpret_cast<double*>(p);
-  p += align_up((size_t)B * seg * 3 * n * sizeof(double));
-  w.signs = reinterpret_cast<unsigned*>(p);
-  p += align_up((size_t)B * steps * words * 2 * sizeof(unsigned));
-  w.loss_part = reinterpret_cast<double*>(p);
-  p += align_up((size_t)B * sizeof(double));
-  w.grad_part = reinterpret_cast<double*>(p);
-  return w;
-}
-
-int check_train(wsr_ctx* ctx, const double* velocity, int B, int n, double dx, double dt, int steps, int every,
-                int method, void* ws, size_t wsb) {
-  if (!ctx) return WSR_ERR_ARG;
-  if (B < 1) return fail(ctx, WSR_ERR_ARG, "B must be >= 1");
-  if (n < 5 || n > kTrainNmax) return fail(ctx, WSR_ERR_ARG, "n must be in [5, %d] (got %d)", kTrainNmax, n);
-  if (steps < 1 || every < 1) return fail(ctx, WSR_ERR_ARG, "steps and ckpt_every must be >= 1");
-  if (!(dx > 0.0) || !(dt > 0.0)) return fail(ctx, WSR_ERR_ARG, "dx and dt must be positive");
-  if (method != WSR_METHOD_SR_F64 && method != WSR_METHOD_SR_F32)
-    return fail(ctx, WSR_ERR_ARG, "training needs WSR_METHOD_SR_F64 or WSR_METHOD_SR_F32 (got %d)", method);
-  if (!ctx->have_closure) return fail(ctx, WSR_ERR_NO_CLOSURE, "training called before wsr_closure_upload");
-  if (!velocity) return fail(ctx, WSR_ERR_ARG, "null velocity array");
-  if (!ws) return fail(ctx, WSR_ERR_ARG, "workspace is NULL");
-  if (reinterpret_cast<uintptr_t>(ws) % kAlign) return fail(ctx, WSR_ERR_ARG, "workspace must be 256-byte aligned");
-  if (wsb < train_ws_bytes(B, n, steps, every))
-    return fail(ctx, WSR_ERR_ARG, "workspace too small: %zu < %zu bytes", wsb, train_ws_bytes(B, n, steps, every));
-  return WSR_OK;
-}
-
-template <int M>
-int train_fwd_launch(wsr_ctx* ctx, const double* u0, const double* desc, const double* vel, int B, int n, double dx,
-                     double dt, int steps, int every, double* loss_out, double* u_final, const WsTrain& w,
-                     cudaStream_t st) {
-  const size_t smem = train_fwd_smem(n);
-  auto kern = k_train_fwd<M>;
-  WSR_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<B, kTrainThreads, smem, st>>>(u0, desc, vel, n, dx, dt, steps, every, w.ck, w.signs, w.loss_part, u_final,
-                                       params_of<M>(ctx));
-  WSR_LAUNCHED(ctx, "k_train_fwd");
-  k_train_reduce<<<1, 256, 0, st>>>(w.loss_part, nullptr, B, 1.0 / ((double)B * (double)steps * (double)n),
-                                    loss_out, nullptr);
-  WSR_LAUNCHED(ctx, "k_train_reduce");
-  return WSR_OK;
-}
-
-template <int M>
-int train_bwd_launch(wsr_ctx* ctx, const double* vel, int B, int n, double dx, double dt, int steps, int every,
-                     double* grad_out, double* grad_u0, const WsTrain& w, cudaStream_t st) {
-  const size_t smem = train_bwd_smem<M>(n);
-  auto kern = k_train_bwd<M>;
-  WSR_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const double gscale = 1.0 / ((double)B * (double)steps * (double)n);
-  kern<<<B, kTrainThreads, smem, st>>>(w.ck, w.signs, vel, n, dx, dt, steps, every, gscale, w.seg, w.grad_part,
-                                       grad_u0, params_of<M>(ctx));
-  WSR_LAUNCHED(ctx, "k_train_bwd");
-  k_train_reduce<<<1, 256, 0, st>>>(nullptr, w.grad_part, B, 0.0, nullptr, grad_out);
-  WSR_LAUNCHED(ctx, "k_train_reduce");
-  return WSR_OK;
-}
-
-}  // namespace
-
-extern "C" size_t wsr_train1d_workspace_bytes(int B, int n, int steps, int ckpt_every) {
-  if (B < 1 || n < 1 || steps < 1 || ckpt_every < 1) return 0;
-  return train_ws_bytes(B, n, steps, ckpt_every);
-}
-
-extern "C" int wsr_train1d_forward(wsr_ctx* ctx, const double* u0, const double* desc, const double* velocity, int B,
-                                   int n, double dx, double dt, int steps, int ckpt_every, int method,
-                                   double* loss_out, double* u_final, void* workspace, size_t workspace_bytes,
-                                   void* stream) {
-  const int rc = check_train(ctx, velocity, B, n, dx, dt, steps, ckpt_every, method, workspace, workspace_bytes);
-  if (rc) return rc;
-  if (!desc || !loss_out) return fail(ctx, WSR_ERR_ARG, "null desc or loss_out");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  const WsTrain w = carve_train(workspace, B, n, steps, ckpt_every);
-  return method == WSR_METHOD_SR_F64
-             ? train_fwd_launch<M_SR64>(ctx, u0, desc, velocity, B, n, dx, dt, steps, ckpt_every, loss_out, u_final, w, st)
-             : train_fwd_launch<M_SR32>(ctx, u0, desc, velocity, B, n, dx, dt, steps, ckpt_every, loss_out, u_final, w, st);
-}
-
-extern "C" int wsr_train1d_backward(wsr_ctx* ctx, const double* velocity, int B, int n, double dx, double dt,
-                                    int steps, int ckpt_every, int method, double* grad_out, double* grad_u0,
-                                    void* workspace, size_t workspace_bytes, void* stream) {
-  const int rc = check_train(ctx, velocity, B, n, dx, dt, steps, ckpt_every, method, workspace, workspace_bytes);
-  if (rc) return rc;
-  if (!grad_out) return fail(ctx, WSR_ERR_ARG, "null grad_out");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  const WsTrain w = carve_train(workspace, B, n, steps, ckpt_every);
-  return method == WSR_METHOD_SR_F64
-             ? train_bwd_launch<M_SR64>(ctx, velocity, B, n, dx, dt, steps, ckpt_every, grad_out, grad_u0, w, st)
-             : train_bwd_launch<M_SR32>(ctx, velocity, B, n, dx, dt, steps, ckpt_every, grad_out, grad_u0, w, st);
-}
-
 namespace {
 // Independent FMA chains for the peak-throughput probe (8 per thread).
 template <typename T>
@@ -737,260 +493,6 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T a, T b) 
   if (s == T(-12345.678)) out[blockIdx.x] = s;  // keeps the chains live
 }
 }  // namespace
-
-// ---------------------------------------------------------------------------------------------
-// 2D Euler WENO7 (JS, Z, SR-FP64) with Shu RK4 (weno7_point_rk4_shu/point_rk4.py, weno7_point_rk4_z.py,
-// teacherfree_lab_weno7_rk4_distance_balanced_fast/warp_sod/point_rk4_mlp.py).
-// ---------------------------------------------------------------------------------------------
-namespace {
-
-struct Ws7 {
-  StepCtl* ctl;
-  double* dts;                     // ring of kDtsRing
-  unsigned long long* counters;    // SR closure evaluations: normal x, normal y, flux x, flux y
-  double *xl, *xr, *yl, *yr, *fx, *fy;
-  double *u1, *u2, *u3;
-  double* rhs[6];  // rhs0, rhs_t0, rhs1, rhs_t1, rhs2, rhs3 (interior)
-};
-
-size_t ws7_bytes(int nx, int ny) {
-  const size_t np = (size_t)(nx + 8) * (ny + 8), ni = (size_t)nx * ny;
-  return align_up(sizeof(StepCtl)) + align_up(kDtsRing * sizeof(double)) + align_up(4 * sizeof(unsigned long long)) +
-         2 * cells_bytes((size_t)(ny + 8) * (nx + 2)) + 2 * cells_bytes((size_t)(ny + 2) * (nx + 8)) +
-         cells_bytes((size_t)ny * (nx + 1)) + cells_bytes((size_t)(ny + 1) * nx) + 3 * cells_bytes(np) +
-         6 * cells_bytes(ni);
-}
-
-Ws7 carve7(void* base, int nx, int ny) {
-  char* p = static_cast<char*>(base);
-  auto take = [&](size_t bytes) {
-    char* q = p;
-    p += bytes;
-    return reinterpret_cast<double*>(q);
-  };
-  Ws7 w;
-  w.ctl = reinterpret_cast<StepCtl*>(take(align_up(sizeof(StepCtl))));
-  w.dts = take(align_up(kDtsRing * sizeof(double)));
-  w.counters = reinterpret_cast<unsigned long long*>(take(align_up(4 * sizeof(unsigned long long))));
-  w.xl = take(cells_bytes((size_t)(ny + 8) * (nx + 2)));
-  w.xr = take(cells_bytes((size_t)(ny + 8) * (nx + 2)));
-  w.yl = take(cells_bytes((size_t)(ny + 2) * (nx + 8)));
-  w.yr = take(cells_bytes((size_t)(ny + 2) * (nx + 8)));
-  w.fx = take(cells_bytes((size_t)ny * (nx + 1)));
-  w.fy = take(cells_bytes((size_t)(ny + 1) * nx));
-  const size_t np = (size_t)(nx + 8) * (ny + 8);
-  w.u1 = take(cells_bytes(np));
-  w.u2 = take(cells_bytes(np));
-  w.u3 = take(cells_bytes(np));
-  for (int k = 0; k < 6; ++k) w.rhs[k] = take(cells_bytes((size_t)nx * ny));
-  return w;
-}
-
-int check7(wsr_ctx* ctx, int nx, int ny, int bc, int method, void* ws, size_t wsb) {
-  if (!ctx) return WSR_ERR_ARG;
-  if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && method != WSR_METHOD_SR_F64)
-    return fail(ctx, WSR_ERR_ARG, "WENO7 2D method must be WSR_METHOD_JS, WSR_METHOD_Z or WSR_METHOD_SR_F64 (got %d)",
-                method);
-  if (method == WSR_METHOD_SR_F64 && !ctx->have_closure7)
-    return fail(ctx, WSR_ERR_NO_CLOSURE, "WSR_METHOD_SR_F64 needs the WENO7 closure (wsr_closure_upload, scheme 7)");
-  if (nx < 4 || ny < 4) return fail(ctx, WSR_ERR_ARG, "nx and ny must be >= 4 (got %d, %d)", nx, ny);
-  if ((long long)(nx + 8) * (ny + 8) > (1ll << 31) / 4)
-    return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
-  if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC) return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
-  if (!ws) return fail(ctx, WSR_ERR_ARG, "workspace is NULL");
-  if (reinterpret_cast<uintptr_t>(ws) % kAlign) return fail(ctx, WSR_ERR_ARG, "workspace must be 256-byte aligned");
-  if (wsb < ws7_bytes(nx, ny))
-    return fail(ctx, WSR_ERR_ARG, "workspace too small: %zu < %zu bytes", wsb, ws7_bytes(nx, ny));
-  return WSR_OK;
-}
-
-// One right-hand side L(src) (reverse = 0) or L~(src) (reverse = 1) into rhs: 5 launches. z: WENO-Z
-// weights with eps = dx^3 along x and dy^3 along y.
-template <bool Z>
-int launch_rhs7_t(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g,
-                  int bc, int reverse, const Ws7& w, cudaStream_t st) {
-  const Gas gas = make_gas(g);
-  const double ex = dx * dx * dx, ey = dy * dy * dy;
-  w7::k7_normal<1, Z><<<dim3((nx + 1 + 127) / 128, ny + 7), 128, 0, st>>>(src, w.xl, w.xr, nx, ny, bc, gas, ex, w.ctl);
-  WSR_LAUNCHED(ctx, "k7_normal<x>");
-  w7::k7_normal<2, Z><<<dim3((nx + 7 + 31) / 32, (ny + 1 + 3) / 4), 128, 0, st>>>(src, w.yl, w.yr, nx, ny, bc, gas, ey,
-                                                                                w.ctl);
-  WSR_LAUNCHED(ctx, "k7_normal<y>");
-  w7::k7_flux<1, Z><<<dim3((nx + 1 + 31) / 32, (ny + 3) / 4), 128, 0, st>>>(w.xl, w.xr, w.fx, nx, ny, gas, reverse,
-                                                                           ey, w.ctl);
-  WSR_LAUNCHED(ctx, "k7_flux<x>");
-  w7::k7_flux<2, Z><<<dim3((nx + 127) / 128, ny + 1), 128, 0, st>>>(w.yl, w.yr, w.fy, nx, ny, gas, reverse, ex, w.ctl);
-  WSR_LAUNCHED(ctx, "k7_flux<y>");
-  w7::k7_rhs<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(w.fx, w.fy, rhs, nx, ny, 1.0 / dx, 1.0 / dy, w.ctl);
-  WSR_LAUNCHED(ctx, "k7_rhs");
-  return WSR_OK;
-}
-
-// The same right-hand side with the FP64 WENO7 closure.
-int launch_rhs7_sr(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g,
-                   int bc, int reverse, const Ws7& w, cudaStream_t st) {
-  const Gas gas = make_gas(g);
-  const Mlp7d& P = ctx->q64;
-  w7::k7s_normal<1><<<dim3((nx + 1 + 127) / 128, ny + 7), 128, 0, st>>>(src, w.xl, w.xr, nx, ny, bc, gas, w.ctl,
-                                                                       w.counters + 0, P);
-  WSR_LAUNCHED(ctx, "k7s_normal<x>");
-  w7::k7s_normal<2><<<dim3((nx + 7 + 31) / 32, (ny + 1 + 3) / 4), 128, 0, st>>>(src, w.yl, w.yr, nx, ny, bc, gas,
-                                                                               w.ctl, w.counters + 1, P);
-  WSR_LAUNCHED(ctx, "k7s_normal<y>");
-  w7::k7s_flux<1><<<dim3((nx + 1 + 31) / 32, (ny + 3) / 4), 128, 0, st>>>(w.xl, w.xr, w.fx, nx, ny, gas, reverse,
-                                                                         w.ctl, w.counters + 2, P);
-  WSR_LAUNCHED(ctx, "k7s_flux<x>");
-  w7::k7s_flux<2><<<dim3((nx + 127) / 128, ny + 1), 128, 0, st>>>(w.yl, w.yr, w.fy, nx, ny, gas, reverse, w.ctl,
-                                                                 w.counters + 3, P);
-  WSR_LAUNCHED(ctx, "k7s_flux<y>");
-  w7::k7_rhs<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(w.fx, w.fy, rhs, nx, ny, 1.0 / dx, 1.0 / dy, w.ctl);
-  WSR_LAUNCHED(ctx, "k7_rhs");
-  return WSR_OK;
-}
-
-int launch_rhs7(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g, int bc,
-                int reverse, int method, const Ws7& w, cudaStream_t st) {
-  if (method == WSR_METHOD_SR_F64) return launch_rhs7_sr(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st);
-  return method == WSR_METHOD_Z ? launch_rhs7_t<true>(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st)
-                                : launch_rhs7_t<false>(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st);
-}
-
-template <int S>
-int launch_shu7(wsr_ctx* ctx, const w7::ShuArgs& a, int nx, int ny, const Ws7& w, cudaStream_t st) {
-  w7::k7_shu<S><<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(a, nx, ny, w.ctl);
-  WSR_LAUNCHED(ctx, "k7_shu");
-  return WSR_OK;
-}
-
-// One Shu RK4 step of u (in place): L(u), L~(u), L(u1), L~(u1), L(u2), L(u3) and four combinations
-// (point_rk4.py:514-538).
-int shu_step7(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double g, int bc, int method, const Ws7& w,
-              cudaStream_t st) {
-  int rc;
-  double* const* R = w.rhs;
-  w7::ShuArgs a{u, w.u1, w.u2, w.u3, R[0], R[1], R[2], R[3], R[4], R[5], nullptr};
-  if ((rc = launch_rhs7(ctx, u, R[0], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
-  a.out = w.u1;
-  if ((rc = launch_shu7<1>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, u, R[1], nx, ny, dx, dy, g, bc, 1, method, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u1, R[2], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
-  a.out = w.u2;
-  if ((rc = launch_shu7<2>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u1, R[3], nx, ny, dx, dy, g, bc, 1, method, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u2, R[4], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
-  a.out = w.u3;
-  if ((rc = launch_shu7<3>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u3, R[5], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
-  a.out = u;
-  return launch_shu7<4>(ctx, a, nx, ny, w, st);
-}
-
-__global__ void k7_init(StepCtl* ctl, unsigned long long* counters, double t_start, double t_end, double cfl,
-                        double hmin, int max_steps) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int k = 0; k < 4; ++k) counters[k] = 0ull;
-  ctl->t = t_start;
-  ctl->t_end = t_end;
-  ctl->dt = 0.0;
-  ctl->max_speed_bits = 0ull;
-  ctl->steps = 0;
-  ctl->done = 0;
-  ctl->health_bad = 0;
-  ctl->fallbacks = 0;
-  ctl->check_health = 0;
-  ctl->check_interval = 0;
-  ctl->max_steps = max_steps;
-  ctl->cfl = cfl;
-  ctl->hmin = hmin;
-}
-
-}  // namespace
-
-extern "C" size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny) {
-  if (nx < 4 || ny < 4) return 0;
-  return ws7_bytes(nx, ny);
-}
-
-extern "C" int wsr_euler2d_w7_rhs(wsr_ctx* ctx, const double* u, double* rhs, int nx, int ny, double dx, double dy,
-                                  double gamma, int bc, int method, int reverse, void* workspace,
-                                  size_t workspace_bytes, void* stream) {
-  int rc = check7(ctx, nx, ny, bc, method, workspace, workspace_bytes);
-  if (rc) return rc;
-  if (!u || !rhs) return fail(ctx, WSR_ERR_ARG, "null pointer");
-  if (misaligned(u) || misaligned(rhs)) return fail(ctx, WSR_ERR_ARG, "arrays must be 16-byte aligned");
-  if (!(dx > 0.0) || !(dy > 0.0)) return fail(ctx, WSR_ERR_ARG, "dx, dy must be positive");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  Ws7 w = carve7(workspace, nx, ny);
-  k7_init<<<1, 1, 0, st>>>(w.ctl, w.counters, 0.0, 1.0, 0.0, 0.0, 1);
-  WSR_LAUNCHED(ctx, "k7_init");
-  return launch_rhs7(ctx, u, rhs, nx, ny, dx, dy, gamma, bc, reverse != 0, method, w, st);
-}
-
-extern "C" int wsr_euler2d_w7_run(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double gamma,
-                                  double cfl, double t_start, double t_end, int bc, int method, int max_steps,
-                                  double* dts_host, int* steps_out, double* t_out, void* workspace,
-                                  size_t workspace_bytes, void* stream) {
-  int rc = check7(ctx, nx, ny, bc, method, workspace, workspace_bytes);
-  if (rc) return rc;
-  if (!u) return fail(ctx, WSR_ERR_ARG, "null state");
-  if (misaligned(u)) return fail(ctx, WSR_ERR_ARG, "state must be 16-byte aligned");
-  if (max_steps < 1) return fail(ctx, WSR_ERR_ARG, "max_steps must be >= 1");
-  if (!(cfl > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return fail(ctx, WSR_ERR_ARG, "cfl, dx, dy must be positive");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  Ws7 w = carve7(workspace, nx, ny);
-  k7_init<<<1, 1, 0, st>>>(w.ctl, w.counters, t_start, t_end, cfl, dx < dy ? dx : dy, max_steps);
-  WSR_LAUNCHED(ctx, "k7_init");
-  const int batch = 16;  // steps launched between host polls (<= kDtsRing)
-  int host_steps = 0, seen = 0, done = 0;
-  StepCtl snap;
-  std::memset(&snap, 0, sizeof(snap));
-  while (!done) {
-    const int nb = max_steps - host_steps < batch ? max_steps - host_steps : batch;
-    if (nb <= 0) break;
-    for (int b = 0; b < nb; ++b) {
-      w7::k7_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, w.ctl);
-      w7::k7_step_begin<<<1, 1, 0, st>>>(w.ctl, w.dts, kDtsRing);
-      WSR_LAUNCHED(ctx, "k7_step_begin");
-      if ((rc = shu_step7(ctx, u, nx, ny, dx, dy, gamma, bc, method, w, st))) return rc;
-      k_step_end<<<1, 1, 0, st>>>(w.ctl);
-      WSR_LAUNCHED(ctx, "k_step_end");
-    }
-    host_steps += nb;
-    WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, w.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
-    WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned + 128, w.dts, kDtsRing * sizeof(double), cudaMemcpyDeviceToHost, st));
-    WSR_CUDA(ctx, cudaStreamSynchronize(st));
-    std::memcpy(&snap, ctx->host_pinned, sizeof(StepCtl));
-    for (int s = seen; s < snap.steps; ++s)
-      if (dts_host && s < max_steps) dts_host[s] = ctx->host_pinned[128 + (s % kDtsRing)];
-    seen = snap.steps;
-    done = snap.done;
-  }
-  if (steps_out) *steps_out = snap.steps;
-  if (t_out) *t_out = snap.t;
-  return WSR_OK;
-}
-
-extern "C" int wsr_euler2d_w7_counters(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, int nx, int ny,
-                                       unsigned long long* out_host) {
-  if (!ctx || !workspace || !out_host) return WSR_ERR_ARG;
-  if (nx < 4 || ny < 4 || workspace_bytes < ws7_bytes(nx, ny))
-    return fail(ctx, WSR_ERR_ARG, "workspace does not hold a %d x %d WENO7 grid", nx, ny);
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  Ws7 w = carve7(workspace, nx, ny);
-  WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-  return WSR_OK;
-}
-
-extern "C" int wsr_probe_exp_tab(wsr_ctx* ctx, const double* x, double* out, int n, void* stream) {
-  if (!ctx || !x || !out || n < 0) return WSR_ERR_ARG;
-  if (n == 0) return WSR_OK;
-  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
-  w7::k_probe_exp_tab<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(x, out, n);
-  WSR_LAUNCHED(ctx, "k_probe_exp_tab");
-  return WSR_OK;
-}
 
 extern "C" int wsr_probe_peak_flops(wsr_ctx* ctx, int bits, double* tflops, void* stream) {
   if (!ctx || !tflops || (bits != 32 && bits != 64)) return WSR_ERR_ARG;
@@ -1039,7 +541,8 @@ extern "C" int wsr_probe_peak_flops(wsr_ctx* ctx, int bits, double* tflops, void
 // it keeps the previous call's contents: the control block and counters are re-initialised by every
 // call, and every face/flux value a call reads is written earlier in the same call, so nothing
 // carries over; but calls that overlap on the GPU (e.g. on two streams at once) race on the array
-// and must be serialised by the caller.
+// and must be serialised by the caller. The device address of the array is looked up once per device and
+// cached for the life of the process; it does not survive cudaDeviceReset on that device.
 // ---------------------------------------------------------------------------------------------
 static __device__ __align__(256) unsigned char g_noalloc_scratch[WSR_NOALLOC_SCRATCH_BYTES];
 
@@ -1076,7 +579,8 @@ int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a,
       w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P);
   k_update<<<dim3((a.nx + 255) / 256, a.ny), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk,
                                                           a.g, w.ctl);
-  return cudaGetLastError() == cudaSuccess ? WSR_OK : WSR_ERR_CUDA;
+  // the error state was drained on entry, so an error here comes from these launches
+  return cudaPeekAtLastError() == cudaSuccess ? WSR_OK : WSR_ERR_CUDA;
 }
 
 }  // namespace
@@ -1086,12 +590,15 @@ extern "C" int wsr_euler2d_stage_noalloc(const double* u_stage, const double* u0
                                          int flux, int opts, const double* closure_params, void* stream) {
   if (nx < 3 || ny < 3) return WSR_ERR_ARG;
   if (ws_bytes(nx, ny) > (size_t)WSR_NOALLOC_SCRATCH_BYTES) return WSR_ERR_SCRATCH_LIMIT;
-  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return WSR_ERR_ARG;
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return WSR_ERR_ARG;
   if (bc != WSR_BC_TRANSMISSIVE && bc != WSR_BC_PERIODIC) return WSR_ERR_ARG;
   if (flux != WSR_FLUX_HLLC && flux != WSR_FLUX_FORCE) return WSR_ERR_ARG;
   if (rk < 1 || rk > 3 || !(dt > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return WSR_ERR_ARG;
   if (!u_stage || !u0 || !u_out || misaligned(u_stage) || misaligned(u0) || misaligned(u_out)) return WSR_ERR_ARG;
-  if (method != WSR_METHOD_JS && !closure_params) return WSR_ERR_NO_CLOSURE;
+  if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && !closure_params) return WSR_ERR_NO_CLOSURE;
+  // Drain a launch error left in this thread's error state by earlier, unrelated work, so that the checks below
+  // report only this call's launches (an error that made the context unusable is sticky and still reported).
+  (void)cudaGetLastError();
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return WSR_ERR_CUDA;
   void* scratch = nullptr;
@@ -1100,11 +607,13 @@ extern "C" int wsr_euler2d_stage_noalloc(const double* u_stage, const double* u0
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   Ws2d w = carve(scratch, nx, ny);
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
-  if (cudaGetLastError() != cudaSuccess) return WSR_ERR_CUDA;
+  if (cudaPeekAtLastError() != cudaSuccess) return WSR_ERR_CUDA;
   StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma, 0.0};
   switch (method) {
     case WSR_METHOD_JS:
       return noalloc_launch<M_JS>(NoParams{}, a, w, st);
+    case WSR_METHOD_Z:
+      return noalloc_launch<M_Z>(ZEps{dx * dx, dy * dy}, a, w, st);
     case WSR_METHOD_SR_F64: {
       Mlp5d P;
       for (int k = 0; k < kParams5; ++k) P.p[k] = closure_params[k];

@@ -67,6 +67,9 @@ constexpr int kDtsRing = 64;  // dt records kept on the device between host poll
 
 inline size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
+// bytes of an array of n cells of 4 FP64 values, padded to the workspace alignment
+inline size_t cells_bytes(size_t n) { return align_up(n * 4 * sizeof(double)); }
+
 inline bool misaligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) != 0; }
 
 

@@ -153,6 +153,7 @@ def run(bufs: list, params: Params, t_end: float, method: str, boundary: str, ml
 
 
 _COPY_BANDS = 8
+_MAX_PIPES = 8  # copy pipes kept per process (one per host buffer in use); the oldest is retired beyond this
 _copy_pipes: dict = {}
 
 
@@ -171,21 +172,42 @@ class _CopyPipe:
         self.pending = False
 
 
+def _pipe_for(key, dev: torch.device, rows: int) -> _CopyPipe:
+    pipe = _copy_pipes.get(key)
+    if pipe is None:
+        if len(_copy_pipes) >= _MAX_PIPES:
+            old_key = next(iter(_copy_pipes))
+            old = _copy_pipes.pop(old_key)
+            if old.pending:  # its read-back stays ordered before later work of this process
+                torch.cuda.current_stream(old.d2h.device).wait_stream(old.d2h)
+        pipe = _copy_pipes[key] = _CopyPipe(dev, rows)
+    return pipe
+
+
 def advance_host(u_host: np.ndarray, params: Params, steps: int, method: str, boundary: str, mlp_params=None,
-                 bufs: list | None = None, ws: Workspace | None = None, device="cuda") -> np.ndarray:
+                 bufs: list | None = None, ws: Workspace | None = None, device="cuda",
+                 async_readback: bool = False) -> np.ndarray:
     """Host-buffer entry: copy the padded state to the device, run `steps` full CFL steps, copy it back
-    into u_host (in place). With pinned host memory both copies are asynchronous DMA in row bands on two copy
-    streams: the read-back is complete once the device is synchronised or host_copies_done() has ordered the
-    current stream after it; the next call's upload of the same rows waits for it band by band."""
+    into u_host (in place), and return u_host.
+
+    By default the call returns after the read-back has completed, so u_host holds the result. With
+    async_readback=True and pinned host memory, the read-back is asynchronous DMA in row bands on a copy stream
+    and the call returns as soon as it is queued: u_host is complete only after host_copies_done() (which orders
+    the current stream after it) and a synchronisation, or after the device is synchronised. The next call's
+    upload of the same rows waits for the previous read-back band by band, so consecutive calls overlap their
+    two copy directions. Work on the device buffers `bufs` waits for every read-back still in flight on the
+    device, whichever host buffer it targets, before it overwrites them."""
     dev = torch.device(device)
     if bufs is None:
         bufs = [torch.empty(params.padded_shape, dtype=torch.float64, device=dev) for _ in range(4)]
     host = torch.from_numpy(u_host) if isinstance(u_host, np.ndarray) else u_host
-    key = (dev.index if dev.index is not None else torch.cuda.current_device(), host.data_ptr(), tuple(host.shape))
-    pipe = _copy_pipes.get(key)
-    if pipe is None:
-        pipe = _copy_pipes[key] = _CopyPipe(dev, int(host.shape[0]))
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    key = (idx, host.data_ptr(), tuple(host.shape))
     cur = torch.cuda.current_stream(dev)
+    pipe = _pipe_for(key, dev, int(host.shape[0]))
+    for other_key, other in _copy_pipes.items():  # read-backs of other host buffers may still read from bufs
+        if other is not pipe and other.pending and other_key[0] == idx:
+            cur.wait_stream(other.d2h)
     pipe.h2d.wait_stream(cur)  # earlier work on bufs[0] is done before it is overwritten
     with torch.cuda.stream(pipe.h2d):
         for k, (r0, r1) in enumerate(pipe.bands):
@@ -200,13 +222,17 @@ def advance_host(u_host: np.ndarray, params: Params, steps: int, method: str, bo
         for k, (r0, r1) in enumerate(pipe.bands):
             host[r0:r1].copy_(out[r0:r1], non_blocking=True)
             pipe.out_done[k].record(pipe.d2h)
-    pipe.pending = True
+    if async_readback:
+        pipe.pending = True
+    else:
+        pipe.d2h.synchronize()
+        pipe.pending = False
     return u_host
 
 
 def host_copies_done(device="cuda") -> None:
-    """Make the current stream wait for every read-back advance_host has issued on `device` (work or events
-    recorded on the current stream afterwards come after them)."""
+    """Make the current stream wait for every read-back advance_host(async_readback=True) has issued on
+    `device` (work or events recorded on the current stream afterwards come after them)."""
     dev = torch.device(device)
     idx = dev.index if dev.index is not None else torch.cuda.current_device()
     cur = torch.cuda.current_stream(dev)
