@@ -865,6 +865,8 @@ def bench_w7(args, world, rank, local):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     counts = E7.closure_counts(ws, p) if method == "sr_f64" else None
+    if counts is not None:
+        counts.pop("fallbacks")
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -989,7 +991,8 @@ def bench_3d(args, world, rank, local):
     q.copy_(q0)
     E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=K, ws=ws,
            opts=4)
-    line["closure_tally_per_step"] = {k: {"mlp": v[0] / K, "plateau": v[1] / K} for k, v in E3.counters(ws).items()}
+    line["closure_tally_per_step"] = {k: {"mlp": v[0] / K, "plateau": v[1] / K} for k, v in E3.counters(ws).items()
+                                      if k != "fallbacks"}
     if not args.skip_extras:
         # end to end: the padded state from pinned host memory, K steps, and back
         host = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True)

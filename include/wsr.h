@@ -91,19 +91,22 @@ size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny);
  * WSR_METHOD_SR_F64 (betas of the FP64 WENO7 closure uploaded with wsr_closure_upload(ctx, 7, ...), the lr = 2
  * face and the second Gauss point from the flipped stencil; compute_rhs_mlp of
  * teacherfree_lab_weno7_rk4_distance_balanced_fast/warp_sod/point_rk4_mlp.py:198-277 with eno_cutoff off).
- * WSR_METHOD_SR_F64 without an uploaded WENO7 closure returns WSR_ERR_NO_CLOSURE. */
+ * WSR_METHOD_SR_F64 without an uploaded WENO7 closure returns WSR_ERR_NO_CLOSURE.
+ * opts: 0, or WSR_OPT_JS_FALLBACK with WSR_METHOD_SR_F64 (an addition; the reference stops the run instead): a
+ * stencil whose closure betas are not finite takes WENO7-JS weights, and a normal face state with rho <= 0 or
+ * p <= 0 is recomputed with WENO7-JS weights; both are counted (wsr_euler2d_w7_counters, out_host[4]). */
 int wsr_euler2d_w7_rhs(wsr_ctx *ctx, const double *u, double *rhs, int nx, int ny, double dx, double dy,
-                       double gamma, int bc, int method, int reverse, void *workspace, size_t workspace_bytes,
-                       void *stream);
+                       double gamma, int bc, int method, int reverse, int opts, void *workspace,
+                       size_t workspace_bytes, void *stream);
 /* Time loop of run_from_initial (point_rk4.py:568-600) on u in place from time t_start: dt = cfl min(dx, dy)
  * / max speed, the loop runs while t < t_end, a step that would pass t_end is shortened to reach it; at most
  * max_steps steps. dts_host (capacity max_steps) receives each step's dt. */
 int wsr_euler2d_w7_run(wsr_ctx *ctx, double *u, int nx, int ny, double dx, double dy, double gamma, double cfl,
-                       double t_start, double t_end, int bc, int method, int max_steps, double *dts_host,
+                       double t_start, double t_end, int bc, int method, int opts, int max_steps, double *dts_host,
                        int *steps_out, double *t_out, void *workspace, size_t workspace_bytes, void *stream);
 /* WSR_METHOD_SR_F64 closure evaluations (stencils that ran the MLP pair) since the last wsr_euler2d_w7_rhs /
- * wsr_euler2d_w7_run on this workspace: out_host[4] = normal x, normal y, transverse x, transverse y.
- * Synchronous. */
+ * wsr_euler2d_w7_run on this workspace: out_host[0..3] = normal x, normal y, transverse x, transverse y;
+ * out_host[4] = JS fallbacks taken under WSR_OPT_JS_FALLBACK (out_host holds 5 values). Synchronous. */
 int wsr_euler2d_w7_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny,
                             unsigned long long *out_host);
 
@@ -212,8 +215,11 @@ int wsr_euler3d_run(wsr_ctx *ctx, double *q, int nx, int ny, int nz, double dx, 
                     double t_start, double t_end, int max_steps, int method, int flux, int opts, const double *inflow,
                     double *dts_host, int *steps_out, double *t_out, void *workspace, size_t workspace_bytes,
                     void *stream);
-/* Closure tallies of the last 3D stage/run made with WSR_OPT_COUNT: out_host[6] = (MLP, plateau) stencils
- * of the normal, first transverse and second transverse (flux) kernels. */
+/* Closure tallies of the last 3D stage/run made with WSR_OPT_COUNT: out_host[0..5] = (MLP, plateau) stencils
+ * of the normal, first transverse and second transverse (flux) kernels; out_host[6] = JS fallbacks taken under
+ * WSR_OPT_JS_FALLBACK (stencils whose closure output is not finite, and normal face states with rho <= 0 or
+ * p <= 0 recomputed with WENO5-JS weights; an addition without a counterpart in the reference). out_host holds
+ * 7 values. */
 int wsr_euler3d_counters(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny, int nz,
                          unsigned long long *out_host);
 

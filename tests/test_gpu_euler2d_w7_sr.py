@@ -129,7 +129,7 @@ def test_sr_without_closure_is_an_error():
         u = torch.zeros(p.padded_shape, dtype=torch.float64, device=DEV)
         out = torch.zeros((8, 8, 4), dtype=torch.float64, device=DEV)
         rc = lib.wsr_euler2d_w7_rhs(h, C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()), 8, 8, 0.1, 0.1, 1.4, 1,
-                                    1, 0, C.c_void_p(ws.ptr), ws.nbytes, None)
+                                    1, 0, 0, C.c_void_p(ws.ptr), ws.nbytes, None)
         assert rc == 3 and b"closure" in lib.wsr_last_error(h)
     finally:
         lib.wsr_ctx_destroy(h)
@@ -191,3 +191,30 @@ def test_table_exponential_against_cuda_exp():
     ctx.check(N.lib().wsr_probe_exp_tab(ctx.handle, C.c_void_p(xs.data_ptr()), C.c_void_p(ys.data_ptr()), s.size,
                                         None))
     assert np.all(np.diff(ys.cpu().numpy()) >= 0)
+
+
+def test_js_fallback_when_closure_is_not_finite():
+    """WSR_OPT_JS_FALLBACK: with NaN output biases every closure evaluation is non-finite, so every stencil that
+    runs the closure takes WENO7-JS weights and the run equals WENO7-JS (plateau stencils take unit betas, which
+    give the linear weights that JS gives there to rounding); without the option the NaN reaches the state."""
+    nx, ny = 20, 16
+    p = E7.Params(nx=nx, ny=ny, cfl=0.4, t_end=0.3)
+    init = problems.vortex_point_rk4(nx, ny, 0.0, 3)
+    bad = {k: np.array(v, dtype=np.float64, copy=True) for k, v in np.load(CKPT).items() if k != "meta_json"}
+    bad["b4"][:] = np.nan
+    ws = E7.workspace(nx, ny, DEV)
+    u_js = torch.as_tensor(init, device=DEV).contiguous()
+    E7.run(u_js, p, "periodic", ws=ws, max_steps=3)
+    u_fb = torch.as_tensor(init, device=DEV).contiguous()
+    E7.run(u_fb, p, "periodic", ws=ws, max_steps=3, method="sr_f64", closure=bad, js_fallback=True)
+    counts = E7.closure_counts(ws, p)
+    evaluated = counts["normal_x"] + counts["normal_y"] + counts["flux_x"] + counts["flux_y"]
+    assert evaluated > 0 and counts["fallbacks"] >= evaluated  # every closure evaluation fell back
+    # the SR and JS kernels round their projections differently and the unnormalised WENO7 betas cancel on smooth
+    # data, so the two kernel families agree to the run tolerance of the vortex (measured 2e-12), not to 1e-13
+    assert _rel(u_fb.cpu().numpy()[4:-4, 4:-4], u_js.cpu().numpy()[4:-4, 4:-4]) <= RUN_TOL["vortex"]
+    u_nan = torch.as_tensor(init, device=DEV).contiguous()
+    E7.run(u_nan, p, "periodic", ws=ws, max_steps=1, method="sr_f64", closure=bad)
+    assert not bool(torch.isfinite(u_nan).all())
+    with pytest.raises(ValueError):
+        E7.run(u_js, p, "periodic", ws=ws, max_steps=1, js_fallback=True)  # WENO7-JS has no closure to replace

@@ -154,3 +154,24 @@ def test_step_file_of_device_state(tmp_path):
     t, prim = B.read_step(tmp_path / "step.bin")
     assert t == res.t and prim.shape == (nz, ny, nx, 5)
     np.testing.assert_array_equal(prim, B.primitive_interior(ref, nx, ny, nz))
+
+
+def test_js_fallback_when_closure_is_not_finite():
+    """WSR_OPT_JS_FALLBACK in 3D: with NaN output biases every non-plateau stencil takes WENO5-JS weights, so a
+    step equals the WENO5-JS step up to the rounding of the two JS evaluations (reciprocals vs IEEE divisions);
+    the fallbacks are counted. Without the option the NaN reaches the state."""
+    nx, ny, nz = 12, 10, 8
+    q0 = _random_state(nx, ny, nz, 4)
+    dx = dy = dz = 1.0 / nx
+    bad = {k: np.array(v, copy=True) for k, v in P64.items()}
+    bad["b4"][:] = np.nan
+    q_js = torch.as_tensor(q0, device=DEV).contiguous()
+    E3.run(q_js, nx, ny, nz, dx, dy, dz, 0.4, "js", "hllc", steps=2)
+    q_fb = torch.as_tensor(q0, device=DEV).contiguous()
+    ws = E3.workspace(nx, ny, nz, DEV)
+    E3.run(q_fb, nx, ny, nz, dx, dy, dz, 0.4, "sr_f64", "hllc", bad, steps=2, opts=2, ws=ws)  # OPT_JS_FALLBACK
+    assert E3.counters(ws)["fallbacks"] > 0
+    assert _rel(q_fb.cpu().numpy(), q_js.cpu().numpy()) <= 1e-12
+    q_nan = torch.as_tensor(q0, device=DEV).contiguous()
+    E3.run(q_nan, nx, ny, nz, dx, dy, dz, 0.4, "sr_f64", "hllc", bad, steps=1)
+    assert not bool(torch.isfinite(q_nan[INNER]).all())

@@ -56,8 +56,8 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_stage_at.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, d, vp, sz, vp]
             L.wsr_euler2d_w7_workspace_bytes.restype = sz
             L.wsr_euler2d_w7_workspace_bytes.argtypes = [i, i]
-            L.wsr_euler2d_w7_rhs.argtypes = [vp, vp, vp, i, i, d, d, d, i, i, i, vp, sz, vp]
-            L.wsr_euler2d_w7_run.argtypes = [vp, vp, i, i, d, d, d, d, d, d, i, i, i, C.POINTER(d), C.POINTER(i),
+            L.wsr_euler2d_w7_rhs.argtypes = [vp, vp, vp, i, i, d, d, d, i, i, i, i, vp, sz, vp]
+            L.wsr_euler2d_w7_run.argtypes = [vp, vp, i, i, d, d, d, d, d, d, i, i, i, i, C.POINTER(d), C.POINTER(i),
                                              C.POINTER(d), vp, sz, vp]
             L.wsr_euler2d_w7_counters.argtypes = [vp, vp, sz, i, i, C.POINTER(C.c_ulonglong)]
             L.wsr_euler2d_max_speed.argtypes = [vp, vp, i, i, d, C.POINTER(d), vp, sz, vp]

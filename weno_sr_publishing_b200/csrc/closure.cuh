@@ -629,11 +629,34 @@ __device__ __forceinline__ double sr_value(const double s[5], int head, double a
   return combine(w, c);
 }
 
+// The linear-weight value of a head as one five-term combination of the stencil, its coefficients
+// sum_k d_k C_k,i formed at compile time from the same candidate literals and linear weights (a plateau
+// stencil's value then costs five multiply-adds; it differs from the candidate-by-candidate evaluation
+// by rounding only).
+struct Lin5 {
+  double c[5];
+};
+__host__ __device__ constexpr Lin5 lin5(int head) {
+  constexpr double r3 = 1.7320508075688772;
+  if (head == 0) return {{0.1 * (1.0 / 3.0), 0.1 * (-7.0 / 6.0) + 0.6 * (-1.0 / 6.0),
+                          0.1 * (11.0 / 6.0) + 0.6 * (5.0 / 6.0) + 0.3 * (1.0 / 3.0),
+                          0.6 * (1.0 / 3.0) + 0.3 * (5.0 / 6.0), 0.3 * (-1.0 / 6.0)}};
+  if (head == 1) return {{0.3 * (-1.0 / 6.0), 0.3 * (5.0 / 6.0) + 0.6 * (1.0 / 3.0),
+                          0.3 * (1.0 / 3.0) + 0.6 * (5.0 / 6.0) + 0.1 * (11.0 / 6.0),
+                          0.6 * (-1.0 / 6.0) + 0.1 * (-7.0 / 6.0), 0.1 * (1.0 / 3.0)}};
+  const double da = (210.0 + r3) / 1080.0, db = 11.0 / 18.0, dc = (210.0 - r3) / 1080.0;
+  if (head == 2) return {{da * -0.144337567297407, da * 0.577350269189626 + db * 0.144337567297406,
+                          da * 0.566987298107780 + db + dc * 1.433012701892220,
+                          db * -0.144337567297407 + dc * -0.577350269189626, dc * 0.144337567297406}};
+  return {{dc * 0.144337567297406, dc * -0.577350269189626 + db * -0.144337567297407,
+           dc * 1.433012701892220 + db + da * 0.566987298107781,
+           db * 0.144337567297406 + da * 0.577350269189625, da * -0.144337567297406}};
+}
+
 __device__ __forceinline__ double linear_value(const double s[5], int head) {
-  const Lin3 d = linear_weights(head);
-  double c[3];
-  candidates(s, head, c);
-  return d.d0 * c[0] + d.d1 * c[1] + d.d2 * c[2];
+  constexpr Lin5 k0 = lin5(0), k1 = lin5(1), k2 = lin5(2), k3 = lin5(3);
+  const Lin5& k = head == 0 ? k0 : (head == 1 ? k1 : (head == 2 ? k2 : k3));
+  return fma(k.c[4], s[4], fma(k.c[3], s[3], fma(k.c[2], s[2], fma(k.c[1], s[1], k.c[0] * s[0]))));
 }
 
 __device__ __forceinline__ double js_value(const double s[5], int head) {

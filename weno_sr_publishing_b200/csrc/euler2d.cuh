@@ -226,8 +226,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
   }
   const bool work = active;
   __syncthreads();
-  // Phase A
-#pragma unroll 1
+  // Phase A, two stencils per iteration (two independent dependency chains; unrolling by 4 or 8 spills)
+#pragma unroll 2
   for (int n = 0; n < kStencilsPerThread; ++n) {
     const int f = n >> 1, side = n & 1;
     bool need = false;
@@ -349,8 +349,9 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
   __syncthreads();
   Tally tally;
   const bool work = active;
-  // Phase A. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L (lr=1 faces fr).
-#pragma unroll 1
+  // Phase A, two stencils per iteration. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L
+  // (lr=1 faces fr).
+#pragma unroll 2
   for (int n = 0; n < kStencilsPerThread; ++n) {
     double s[5];
     load_transverse<DIR>(fl, fr, nx, i, j, n, work, s);

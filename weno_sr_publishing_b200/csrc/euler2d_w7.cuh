@@ -388,7 +388,7 @@ __constant__ double kExp2_32[32] = {
     1.8340080864093424, 1.8741676341103, 1.9152065613971474, 1.9571441241754002};
 
 __device__ __forceinline__ double exp_tab(double x, const double* __restrict__ t32) {
-  x = fmin(fmax(x, -700.0), 700.0);
+  x = x < -700.0 ? -700.0 : (x > 700.0 ? 700.0 : x);  // NaN passes through (fmin/fmax would drop it)
   constexpr double kShift = 6755399441055744.0;  // 1.5 * 2^52: x 32/ln2 + kShift holds round(x 32/ln2) in its low word
   constexpr double kInvL = 46.16624130844683, kL1 = 0.02166084939249829, kL2 = 7.247021293269686e-19;
   const double kd = fma(x, kInvL, kShift);
@@ -507,7 +507,8 @@ template <int DIR>
 __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_normal(const double* __restrict__ u, double* __restrict__ out_l,
                                                         double* __restrict__ out_r, int nx, int ny, int bc, Gas gas,
                                                         const StepCtl* __restrict__ ctl,
-                                                        unsigned long long* __restrict__ counters,
+                                                        unsigned long long* __restrict__ counters, int opts,
+                                                        unsigned long long* __restrict__ fallbacks,
                                                         const __grid_constant__ Mlp7d P) {
   __shared__ double s_ch[4][8][kBlock7];
   __shared__ double s_val[8][kBlock7];
@@ -522,6 +523,7 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_normal(const
   const int nxt = nx + 2 * kG;
   const bool active = DIR == 1 ? (r >= 1 && r < ny + 7 && c <= nx) : (r <= ny && c >= 1 && c < nx + 7);
   if (t == 0) s_count = 0;
+  int fb = 0;  // JS fallbacks taken by this thread
   RoeJ J;
   if (active) {
     auto cell = [&](int k) {
@@ -571,19 +573,38 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_normal(const
 #pragma unroll
     for (int k = 0; k < 7; ++k) cq[k] = side ? q[6 - k] : q[k];
     w7sr_betas(cq, side == 1, P, s_t32, b);
-    s_val[n][o] = w7sr_face(q, side + 1, b);
+    if ((opts & OPT_JS_FALLBACK) && !(isfinite(b[0]) && isfinite(b[1]) && isfinite(b[2]) && isfinite(b[3]))) {
+      s_val[n][o] = w7_js_face(q, side + 1);  // the closure's betas are not finite: WENO7-JS weights
+      ++fb;
+    } else {
+      s_val[n][o] = w7sr_face(q, side + 1, b);
+    }
   }
   __syncthreads();
   if (active) {
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
       const double cf[4] = {s_val[side][t], s_val[2 + side][t], s_val[4 + side][t], s_val[6 + side][t]};
-      const d4 face = char_to_con<DIR>(cf, J);
+      d4 face = char_to_con<DIR>(cf, J);
+      if ((opts & OPT_JS_FALLBACK) && !admissible(face, gas.g)) {
+        // positivity fallback: this face value again, all four fields with WENO7-JS weights
+        double jf[4];
+#pragma unroll 1
+        for (int f = 0; f < 4; ++f) {
+          double q[7];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][t];
+          jf[f] = w7_js_face(q, side + 1);
+        }
+        face = char_to_con<DIR>(jf, J);
+        ++fb;
+      }
       const size_t idx = DIR == 1 ? (size_t)r * (nx + 2) + c + side : (size_t)(r + side) * (nx + 8) + c;
       store_cell(side == 0 ? out_r : out_l, idx, face);
     }
   }
   if (t == 0 && count) atomicAdd(counters, (unsigned long long)count);
+  if (fb) atomicAdd(fallbacks, (unsigned long long)fb);
 }
 
 // Transverse stencil m = 2 comp + side of face (i, j) (side 0: u_L from fr, side 1: u_R from fl), the
@@ -610,7 +631,8 @@ template <int DIR>
 __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_flux(const double* __restrict__ fl, const double* __restrict__ fr,
                                                       double* __restrict__ fout, int nx, int ny, Gas gas, int reverse,
                                                       const StepCtl* __restrict__ ctl,
-                                                      unsigned long long* __restrict__ counters,
+                                                      unsigned long long* __restrict__ counters, int opts,
+                                                      unsigned long long* __restrict__ fallbacks,
                                                       const __grid_constant__ Mlp7d P) {
   __shared__ double s_g[16][kBlock7];
   __shared__ double s_t32[32];
@@ -625,6 +647,7 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_flux(const d
   const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
   const bool active = i < nfx && j < nfy;
   if (t == 0) s_count = 0;
+  int fb = 0;  // JS fallbacks taken by this thread
   __syncthreads();
   // Phase A
 #pragma unroll 1
@@ -659,7 +682,14 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_flux(const d
 #pragma unroll
     for (int k = 0; k < 7; ++k) cq[k] = gp ? q[6 - k] : q[k];
     w7sr_betas(cq, gp == 1, P, s_t32, b);
-    s_g[n][o] = w7sr_gauss(q, gp + 1, b);
+    if ((opts & OPT_JS_FALLBACK) && !(isfinite(b[0]) && isfinite(b[1]) && isfinite(b[2]) && isfinite(b[3]))) {
+      double g1, g2;  // the closure's betas are not finite: WENO7-JS weights
+      w7_js_gauss(q, g1, g2);
+      s_g[n][o] = gp ? g2 : g1;
+      ++fb;
+    } else {
+      s_g[n][o] = w7sr_gauss(q, gp + 1, b);
+    }
   }
   __syncthreads();
   if (active) {
@@ -679,6 +709,7 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_flux(const d
     store_cell(fout, (size_t)j * nfx + i, o);
   }
   if (t == 0 && count) atomicAdd(counters, (unsigned long long)count);
+  if (fb) atomicAdd(fallbacks, (unsigned long long)fb);
 }
 
 // rhs[j][i] = -1/2 (f[j][i+1] - f[j][i]) / dx - 1/2 (g[j+1][i] - g[j][i]) / dy (point_rk4.py:290-312).

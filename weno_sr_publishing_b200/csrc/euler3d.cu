@@ -304,6 +304,14 @@ __device__ __forceinline__ double js3(const double q[5], int head) {
   return (a0 / s) * c[0] + (a1 / s) * c[1] + (a2 / s) * c[2];
 }
 
+// rho > 0 and p > 0 of a conserved 3D state
+__device__ __forceinline__ bool admissible5(const V5& q) {
+  const double rho = q.v[0];
+  if (!(rho > 0.0)) return false;
+  const double p = (kGam - 1.0) * (q.v[4] - 0.5 * (q.v[1] * q.v[1] + q.v[2] * q.v[2] + q.v[3] * q.v[3]) / rho);
+  return p > 0.0;
+}
+
 template <int M>
 __device__ __forceinline__ double recon(const double q[5], int head, const typename ClosureParams<M>::type& P,
                                         int opts, Tally& tally) {
@@ -449,13 +457,27 @@ __global__ void __launch_bounds__(kT3) k3_normal(const double* __restrict__ q, d
       const double st[5] = {ch[0].v[c], ch[1].v[c], ch[2].v[c], ch[3].v[c], ch[4].v[c]};
       cv.v[c] = recon<M>(st, side == 0 ? 1 : 0, P, opts, tally);
     }
-    st5(side == 0 ? nl : nr, o, E.right(cv));
+    V5 face = E.right(cv);
+    if constexpr (M != M_JS) {
+      if ((opts & OPT_JS_FALLBACK) && !admissible5(face)) {
+        // positivity fallback: the five characteristic values of this face again with WENO5-JS weights
+#pragma unroll 1
+        for (int c = 0; c < 5; ++c) {
+          const double st[5] = {ch[0].v[c], ch[1].v[c], ch[2].v[c], ch[3].v[c], ch[4].v[c]};
+          cv.v[c] = js3(st, side == 0 ? 1 : 0);
+        }
+        face = E.right(cv);
+        ++tally.fallbacks;
+      }
+    }
+    st5(side == 0 ? nl : nr, o, face);
   }
 
   if (counters && (opts & OPT_COUNT)) {
     if (tally.mlp) atomicAdd(&counters[0], (unsigned long long)tally.mlp);
     if (tally.plateau) atomicAdd(&counters[1], (unsigned long long)tally.plateau);
   }
+  if (counters && tally.fallbacks) atomicAdd(&counters[6], (unsigned long long)tally.fallbacks);
 }
 
 // --- first transverse pass: both Gauss points of both normal arrays ------------------------------------
@@ -486,6 +508,7 @@ __global__ void __launch_bounds__(kT3) k3_trans(const double* __restrict__ nl, c
     if (tally.mlp) atomicAdd(&counters[2], (unsigned long long)tally.mlp);
     if (tally.plateau) atomicAdd(&counters[3], (unsigned long long)tally.plateau);
   }
+  if (counters && tally.fallbacks) atomicAdd(&counters[6], (unsigned long long)tally.fallbacks);
 }
 
 // --- second transverse pass and face fluxes (kernels.py:1015-1076; solver.py:175-199) ------------------
@@ -540,6 +563,7 @@ __global__ void __launch_bounds__(kT3) k3_flux(const double* __restrict__ a_l1, 
     if (tally.mlp) atomicAdd(&counters[4], (unsigned long long)tally.mlp);
     if (tally.plateau) atomicAdd(&counters[5], (unsigned long long)tally.plateau);
   }
+  if (counters && tally.fallbacks) atomicAdd(&counters[6], (unsigned long long)tally.fallbacks);
 }
 
 // --- RK stage update (kernels.py:1079-1163) -----------------------------------------------------------
@@ -754,7 +778,8 @@ extern "C" int wsr_euler3d_stage(wsr_ctx* ctx, double* q, int nx, int ny, int nz
   const Ws3 w = carve3(workspace, nx, ny, nz);
   const Run3 r = make_run(q, nx, ny, nz, dx, dy, dz, flux, opts, inflow);
   k3_init_ctl<<<1, 1, 0, st>>>(w.ctl, 0.0, 1.0e300, dt, 1.0, 1.0, 1);
-  if (opts & OPT_COUNT) WSR_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st));
+  if (opts & (OPT_COUNT | OPT_JS_FALLBACK))
+    WSR_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st));
   WSR_LAUNCHED(ctx, "k3_init_ctl");
   return stage_dispatch(ctx, method, r, w, stage, st);
 }
@@ -798,7 +823,8 @@ extern "C" int wsr_euler3d_run(wsr_ctx* ctx, double* q, int nx, int ny, int nz, 
   double* dts_dev = nullptr;
   if (dts_host) WSR_CUDA(ctx, cudaMallocAsync(&dts_dev, (size_t)max_steps * sizeof(double), st));
   k3_init_ctl<<<1, 1, 0, st>>>(w.ctl, t_start, t_end, 0.0, cfl, hmin, max_steps);
-  if (opts & OPT_COUNT) WSR_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st));
+  if (opts & (OPT_COUNT | OPT_JS_FALLBACK))
+    WSR_CUDA(ctx, cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), st));
   k3_max_speed<<<grid3(nx, ny, nz), kT3, 0, st>>>(q, r.d, w.ctl);
   WSR_LAUNCHED(ctx, "k3_max_speed");
   for (int s = 0; s < max_steps; ++s) {
@@ -833,6 +859,6 @@ extern "C" int wsr_euler3d_counters(wsr_ctx* ctx, void* workspace, size_t worksp
   if (!ctx || !workspace || !out_host) return WSR_ERR_ARG;
   if (workspace_bytes < ws3_bytes(nx, ny, nz)) return fail(ctx, WSR_ERR_ARG, "workspace too small");
   const Ws3 w = carve3(workspace, nx, ny, nz);
-  WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return WSR_OK;
 }

@@ -22,7 +22,7 @@ namespace {
 struct Ws7 {
   StepCtl* ctl;
   double* dts;                     // ring of kDtsRing
-  unsigned long long* counters;    // SR closure evaluations: normal x, normal y, flux x, flux y
+  unsigned long long* counters;    // SR closure evaluations: normal x, normal y, flux x, flux y; [4] JS fallbacks
   double *xl, *xr, *yl, *yr, *fx, *fy;
   double *u1, *u2, *u3;
   double* rhs[6];  // rhs0, rhs_t0, rhs1, rhs_t1, rhs2, rhs3 (interior)
@@ -30,7 +30,7 @@ struct Ws7 {
 
 size_t ws7_bytes(int nx, int ny) {
   const size_t np = (size_t)(nx + 8) * (ny + 8), ni = (size_t)nx * ny;
-  return align_up(sizeof(StepCtl)) + align_up(kDtsRing * sizeof(double)) + align_up(4 * sizeof(unsigned long long)) +
+  return align_up(sizeof(StepCtl)) + align_up(kDtsRing * sizeof(double)) + align_up(8 * sizeof(unsigned long long)) +
          2 * cells_bytes((size_t)(ny + 8) * (nx + 2)) + 2 * cells_bytes((size_t)(ny + 2) * (nx + 8)) +
          cells_bytes((size_t)ny * (nx + 1)) + cells_bytes((size_t)(ny + 1) * nx) + 3 * cells_bytes(np) +
          6 * cells_bytes(ni);
@@ -46,7 +46,7 @@ Ws7 carve7(void* base, int nx, int ny) {
   Ws7 w;
   w.ctl = reinterpret_cast<StepCtl*>(take(align_up(sizeof(StepCtl))));
   w.dts = take(align_up(kDtsRing * sizeof(double)));
-  w.counters = reinterpret_cast<unsigned long long*>(take(align_up(4 * sizeof(unsigned long long))));
+  w.counters = reinterpret_cast<unsigned long long*>(take(align_up(8 * sizeof(unsigned long long))));
   w.xl = take(cells_bytes((size_t)(ny + 8) * (nx + 2)));
   w.xr = take(cells_bytes((size_t)(ny + 8) * (nx + 2)));
   w.yl = take(cells_bytes((size_t)(ny + 2) * (nx + 8)));
@@ -103,20 +103,22 @@ int launch_rhs7_t(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, 
 
 // The same right-hand side with the FP64 WENO7 closure.
 int launch_rhs7_sr(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g,
-                   int bc, int reverse, const Ws7& w, cudaStream_t st) {
+                   int bc, int reverse, int opts, const Ws7& w, cudaStream_t st) {
   const Gas gas = make_gas(g);
   const Mlp7d& P = ctx->q64;
   w7::k7s_normal<1><<<dim3((nx + 1 + 127) / 128, ny + 7), 128, 0, st>>>(src, w.xl, w.xr, nx, ny, bc, gas, w.ctl,
-                                                                       w.counters + 0, P);
+                                                                       w.counters + 0, opts, w.counters + 4, P);
   WSR_LAUNCHED(ctx, "k7s_normal<x>");
   w7::k7s_normal<2><<<dim3((nx + 7 + 31) / 32, (ny + 1 + 3) / 4), 128, 0, st>>>(src, w.yl, w.yr, nx, ny, bc, gas,
-                                                                               w.ctl, w.counters + 1, P);
+                                                                               w.ctl, w.counters + 1, opts,
+                                                                               w.counters + 4, P);
   WSR_LAUNCHED(ctx, "k7s_normal<y>");
   w7::k7s_flux<1><<<dim3((nx + 1 + 31) / 32, (ny + 3) / 4), 128, 0, st>>>(w.xl, w.xr, w.fx, nx, ny, gas, reverse,
-                                                                         w.ctl, w.counters + 2, P);
+                                                                         w.ctl, w.counters + 2, opts, w.counters + 4,
+                                                                         P);
   WSR_LAUNCHED(ctx, "k7s_flux<x>");
   w7::k7s_flux<2><<<dim3((nx + 127) / 128, ny + 1), 128, 0, st>>>(w.yl, w.yr, w.fy, nx, ny, gas, reverse, w.ctl,
-                                                                 w.counters + 3, P);
+                                                                 w.counters + 3, opts, w.counters + 4, P);
   WSR_LAUNCHED(ctx, "k7s_flux<y>");
   w7::k7_rhs<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(w.fx, w.fy, rhs, nx, ny, 1.0 / dx, 1.0 / dy, w.ctl);
   WSR_LAUNCHED(ctx, "k7_rhs");
@@ -124,8 +126,8 @@ int launch_rhs7_sr(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny,
 }
 
 int launch_rhs7(wsr_ctx* ctx, const double* src, double* rhs, int nx, int ny, double dx, double dy, double g, int bc,
-                int reverse, int method, const Ws7& w, cudaStream_t st) {
-  if (method == WSR_METHOD_SR_F64) return launch_rhs7_sr(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st);
+                int reverse, int method, int opts, const Ws7& w, cudaStream_t st) {
+  if (method == WSR_METHOD_SR_F64) return launch_rhs7_sr(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, opts, w, st);
   return method == WSR_METHOD_Z ? launch_rhs7_t<true>(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st)
                                 : launch_rhs7_t<false>(ctx, src, rhs, nx, ny, dx, dy, g, bc, reverse, w, st);
 }
@@ -139,23 +141,23 @@ int launch_shu7(wsr_ctx* ctx, const w7::ShuArgs& a, int nx, int ny, const Ws7& w
 
 // One Shu RK4 step of u (in place): L(u), L~(u), L(u1), L~(u1), L(u2), L(u3) and four combinations
 // (point_rk4.py:514-538).
-int shu_step7(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double g, int bc, int method, const Ws7& w,
-              cudaStream_t st) {
+int shu_step7(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double g, int bc, int method, int opts,
+              const Ws7& w, cudaStream_t st) {
   int rc;
   double* const* R = w.rhs;
   w7::ShuArgs a{u, w.u1, w.u2, w.u3, R[0], R[1], R[2], R[3], R[4], R[5], nullptr};
-  if ((rc = launch_rhs7(ctx, u, R[0], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, u, R[0], nx, ny, dx, dy, g, bc, 0, method, opts, w, st))) return rc;
   a.out = w.u1;
   if ((rc = launch_shu7<1>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, u, R[1], nx, ny, dx, dy, g, bc, 1, method, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u1, R[2], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, u, R[1], nx, ny, dx, dy, g, bc, 1, method, opts, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u1, R[2], nx, ny, dx, dy, g, bc, 0, method, opts, w, st))) return rc;
   a.out = w.u2;
   if ((rc = launch_shu7<2>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u1, R[3], nx, ny, dx, dy, g, bc, 1, method, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u2, R[4], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u1, R[3], nx, ny, dx, dy, g, bc, 1, method, opts, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u2, R[4], nx, ny, dx, dy, g, bc, 0, method, opts, w, st))) return rc;
   a.out = w.u3;
   if ((rc = launch_shu7<3>(ctx, a, nx, ny, w, st))) return rc;
-  if ((rc = launch_rhs7(ctx, w.u3, R[5], nx, ny, dx, dy, g, bc, 0, method, w, st))) return rc;
+  if ((rc = launch_rhs7(ctx, w.u3, R[5], nx, ny, dx, dy, g, bc, 0, method, opts, w, st))) return rc;
   a.out = u;
   return launch_shu7<4>(ctx, a, nx, ny, w, st);
 }
@@ -163,7 +165,7 @@ int shu_step7(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, dou
 __global__ void k7_init(StepCtl* ctl, unsigned long long* counters, double t_start, double t_end, double cfl,
                         double hmin, int max_steps) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int k = 0; k < 4; ++k) counters[k] = 0ull;
+  for (int k = 0; k < 8; ++k) counters[k] = 0ull;
   ctl->t = t_start;
   ctl->t_end = t_end;
   ctl->dt = 0.0;
@@ -187,7 +189,7 @@ extern "C" size_t wsr_euler2d_w7_workspace_bytes(int nx, int ny) {
 }
 
 extern "C" int wsr_euler2d_w7_rhs(wsr_ctx* ctx, const double* u, double* rhs, int nx, int ny, double dx, double dy,
-                                  double gamma, int bc, int method, int reverse, void* workspace,
+                                  double gamma, int bc, int method, int reverse, int opts, void* workspace,
                                   size_t workspace_bytes, void* stream) {
   int rc = check7(ctx, nx, ny, bc, method, workspace, workspace_bytes);
   if (rc) return rc;
@@ -199,11 +201,11 @@ extern "C" int wsr_euler2d_w7_rhs(wsr_ctx* ctx, const double* u, double* rhs, in
   Ws7 w = carve7(workspace, nx, ny);
   k7_init<<<1, 1, 0, st>>>(w.ctl, w.counters, 0.0, 1.0, 0.0, 0.0, 1);
   WSR_LAUNCHED(ctx, "k7_init");
-  return launch_rhs7(ctx, u, rhs, nx, ny, dx, dy, gamma, bc, reverse != 0, method, w, st);
+  return launch_rhs7(ctx, u, rhs, nx, ny, dx, dy, gamma, bc, reverse != 0, method, opts, w, st);
 }
 
 extern "C" int wsr_euler2d_w7_run(wsr_ctx* ctx, double* u, int nx, int ny, double dx, double dy, double gamma,
-                                  double cfl, double t_start, double t_end, int bc, int method, int max_steps,
+                                  double cfl, double t_start, double t_end, int bc, int method, int opts, int max_steps,
                                   double* dts_host, int* steps_out, double* t_out, void* workspace,
                                   size_t workspace_bytes, void* stream) {
   int rc = check7(ctx, nx, ny, bc, method, workspace, workspace_bytes);
@@ -228,7 +230,7 @@ extern "C" int wsr_euler2d_w7_run(wsr_ctx* ctx, double* u, int nx, int ny, doubl
       w7::k7_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, w.ctl);
       w7::k7_step_begin<<<1, 1, 0, st>>>(w.ctl, w.dts, kDtsRing);
       WSR_LAUNCHED(ctx, "k7_step_begin");
-      if ((rc = shu_step7(ctx, u, nx, ny, dx, dy, gamma, bc, method, w, st))) return rc;
+      if ((rc = shu_step7(ctx, u, nx, ny, dx, dy, gamma, bc, method, opts, w, st))) return rc;
       k_step_end<<<1, 1, 0, st>>>(w.ctl);
       WSR_LAUNCHED(ctx, "k_step_end");
     }
@@ -254,7 +256,7 @@ extern "C" int wsr_euler2d_w7_counters(wsr_ctx* ctx, void* workspace, size_t wor
     return fail(ctx, WSR_ERR_ARG, "workspace does not hold a %d x %d WENO7 grid", nx, ny);
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
   Ws7 w = carve7(workspace, nx, ny);
-  WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return WSR_OK;
 }
 

@@ -134,10 +134,17 @@ class Weno7PointBeta:
         self.gamma = float(gamma)
 
 
+def _opts(method: str, js_fallback: bool) -> int:
+    if js_fallback and method != "sr_f64":
+        raise ValueError("js_fallback applies to method 'sr_f64' only")
+    return N.OPT_JS_FALLBACK if js_fallback else 0
+
+
 def rhs(u: torch.Tensor, params: Params, boundary: str = "periodic", reverse: bool = False,
-        ws: Workspace | None = None, method: str = "js", closure=None) -> torch.Tensor:
+        ws: Workspace | None = None, method: str = "js", closure=None, js_fallback: bool = False) -> torch.Tensor:
     """L(u) (or the downwind L~(u)) on the interior, shape [ny, nx, 4] (compute_rhs, point_rk4.py:435-511;
-    compute_rhs_mlp, point_rk4_mlp.py:198-277, for method "sr_f64")."""
+    compute_rhs_mlp, point_rk4_mlp.py:198-277, for method "sr_f64"). js_fallback: WENO7-JS weights where the
+    closure's betas are not finite or a normal face state loses positivity (counted in closure_counts)."""
     _check(u, params)
     bc = _bc(boundary)
     dev = u.device.index
@@ -147,7 +154,8 @@ def rhs(u: torch.Tensor, params: Params, boundary: str = "periodic", reverse: bo
     out = torch.empty((params.ny, params.nx, 4), dtype=torch.float64, device=u.device)
     ctx.check(N.lib().wsr_euler2d_w7_rhs(ctx.handle, C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),
                                          params.nx, params.ny, params.dx, params.dy, params.gamma, bc,
-                                         m, int(bool(reverse)), C.c_void_p(ws.ptr), ws.nbytes, _stream(dev)))
+                                         m, int(bool(reverse)), _opts(method, js_fallback), C.c_void_p(ws.ptr),
+                                         ws.nbytes, _stream(dev)))
     return out
 
 
@@ -160,9 +168,9 @@ class RunResult:
 
 def run(u: torch.Tensor, params: Params, boundary: str = "periodic", t_end: float | None = None,
         max_steps: int = 10_000_000, t_start: float = 0.0, ws: Workspace | None = None,
-        method: str = "js", closure=None) -> RunResult:
+        method: str = "js", closure=None, js_fallback: bool = False) -> RunResult:
     """Advance u in place from t_start to t_end with the device-resident Shu RK4 loop (run_from_initial's
-    stopping rule)."""
+    stopping rule). js_fallback as in rhs."""
     _check(u, params)
     bc = _bc(boundary)
     dev = u.device.index
@@ -175,17 +183,18 @@ def run(u: torch.Tensor, params: Params, boundary: str = "periodic", t_end: floa
     steps, t = C.c_int(0), C.c_double(0.0)
     ctx.check(N.lib().wsr_euler2d_w7_run(
         ctx.handle, C.c_void_p(u.data_ptr()), params.nx, params.ny, params.dx, params.dy, params.gamma, params.cfl,
-        float(t_start), t_end, bc, m, cap, dts.ctypes.data_as(C.POINTER(C.c_double)),
+        float(t_start), t_end, bc, m, _opts(method, js_fallback), cap, dts.ctypes.data_as(C.POINTER(C.c_double)),
         C.byref(steps), C.byref(t), C.c_void_p(ws.ptr), ws.nbytes, _stream(dev)))
     return RunResult([float(x) for x in dts[:steps.value]], steps.value, t.value)
 
 
 def closure_counts(ws: Workspace, params: Params, device=None) -> dict[str, int]:
-    """Closure evaluations (stencils that ran the MLP pair) of the last rhs / run on `ws` ("sr_f64")."""
-    out = (C.c_ulonglong * 4)()
+    """Closure evaluations (stencils that ran the MLP pair) of the last rhs / run on `ws` ("sr_f64"), per kernel
+    class, and the JS fallbacks taken ("fallbacks")."""
+    out = (C.c_ulonglong * 5)()
     ctx = N.context(torch.device(device).index if device is not None else ws.buf.device.index)
     ctx.check(N.lib().wsr_euler2d_w7_counters(ctx.handle, C.c_void_p(ws.ptr), ws.nbytes, params.nx, params.ny, out))
-    return dict(zip(("normal_x", "normal_y", "flux_x", "flux_y"), (int(v) for v in out)))
+    return dict(zip(("normal_x", "normal_y", "flux_x", "flux_y", "fallbacks"), (int(v) for v in out)))
 
 
 def interior_stats(u_host: np.ndarray, params: Params) -> dict[str, float]:

@@ -120,10 +120,11 @@ def run(q: torch.Tensor, nx: int, ny: int, nz: int, dx: float, dy: float, dz: fl
 
 
 def counters(ws: Workspace3) -> dict[str, tuple[int, int]]:
-    """(MLP, plateau) stencils of the last stage/run made with WSR_OPT_COUNT, per kernel class."""
-    out = (C.c_ulonglong * 6)()
+    """(MLP, plateau) stencils of the last stage/run made with WSR_OPT_COUNT, per kernel class, and the JS
+    fallbacks of the last stage/run made with OPT_JS_FALLBACK ("fallbacks")."""
+    out = (C.c_ulonglong * 7)()
     ctx = N.context(device_index(ws.buf.device))
     nx, ny, nz = ws.shape
     ctx.check(N.lib().wsr_euler3d_counters(ctx.handle, C.c_void_p(ws.ptr), ws.nbytes, nx, ny, nz, out))
     return {"normal": (int(out[0]), int(out[1])), "transverse": (int(out[2]), int(out[3])),
-            "flux": (int(out[4]), int(out[5]))}
+            "flux": (int(out[4]), int(out[5])), "fallbacks": int(out[6])}

@@ -297,6 +297,9 @@ class TrainConfig:
     checkpoint_interval: int = 250
     state_interval: int = 2500
     device: str = "cuda"
+    # every sod_monitor_interval steps (0 = never) rank 0 evaluates that step's checkpoint on the Sod problem
+    # (sod_monitor.record_checkpoint) and adds the record to circle_validation_metrics.csv/.npz of out_dir
+    sod_monitor_interval: int = 0
 
     def signature(self) -> dict:
         return {"steps": self.steps, "grid": self.grid, "batch": self.batch, "distances": tuple(self.distances),
@@ -430,6 +433,13 @@ def train(cfg: TrainConfig, resume: Path | None = None, max_steps: int | None = 
                 csv.DictWriter(f, fieldnames=fields).writerow(last)
         if rank == 0 and step % cfg.checkpoint_interval == 0:
             _save_model(out / "checkpoints" / f"model_step_{step:06d}.npz", model, step, cfg)
+        if rank == 0 and cfg.sod_monitor_interval > 0 and step % cfg.sod_monitor_interval == 0:
+            from . import sod_monitor as SM
+            ck = out / "checkpoints" / f"model_step_{step:06d}.npz"
+            if step % cfg.checkpoint_interval != 0:
+                _save_model(ck, model, step, cfg)
+            SM.record_checkpoint(out, ck, step, SM.SodMonitorConfig(
+                precision="sr_f32" if cfg.precision == "f32" else "sr_f64"), dev)
         if step % cfg.state_interval == 0:
             save_state(step)
     save_state(end)
