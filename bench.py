@@ -746,6 +746,21 @@ def bench_1d(args, world, rank, local):
         line.update({"value": world * work / (ms * 1e-3), "ms_per_step": ms / K, "clocks": clk.summary(),
                      "gpu_launches": 4 * K, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                      "distances": [int(d) for d in order[W:]]})
+        # closure tallies of the timed forwards: the training forward equals the 1D batch path bit for bit, so
+        # the batch path with its counters on the same initial states and steps counts its closure evaluations
+        from weno_sr_publishing_b200 import adv1d as A1
+        cl = A1.Closure(5, packed, prec)
+        mlp_n = plat_n = 0
+        for b in batches[W:]:
+            u0 = P1.cell_averages(b.desc.cpu().numpy(), b.n, 0.0)
+            _, info = A1.run_batched(list(u0), b.velocity.cpu().numpy(), 1.0 / b.n, b.steps, b.dt, scheme=5,
+                                     model=cl, device=dev, count=True)
+            mlp_n += info["mlp"]
+            plat_n += info["plateau"]
+        # forward, its recomputation from the checkpoints, and a reverse pass of twice the forward's work
+        line["roofline"] = _closure_roofline(
+            "k_train_fwd + k_train_bwd (4 x the counted forward closure work)", method,
+            [(4.0 * mlp_n / K, 4.0 * plat_n / K, 1)], ms / K, local, stream)
         # end to end through the autograd API: host profile descriptors in, host loss and gradient out
         t0 = time.perf_counter()
         for d in order[W:]:
@@ -993,6 +1008,11 @@ def bench_3d(args, world, rank, local):
            opts=4)
     line["closure_tally_per_step"] = {k: {"mlp": v[0] / K, "plateau": v[1] / K} for k, v in E3.counters(ws).items()
                                       if k != "fallbacks"}
+    if method != "js":
+        line["roofline"] = _closure_roofline(
+            "k3_normal + k3_trans + k3_flux (closure work only)", method,
+            [(v[0] / K, v[1] / K, 1 if k == "normal" else 2) for k, v in E3.counters(ws).items() if k != "fallbacks"],
+            ms / K, local, stream)
     if not args.skip_extras:
         # end to end: the padded state from pinned host memory, K steps, and back
         host = torch.empty(q0.shape, dtype=torch.float64, pin_memory=True)
@@ -1097,6 +1117,31 @@ def _roofline_1d(scheme, method, work_cellsteps, mlp_n, plat_n, ms, peak, ctx, s
     b = R.bound({"w32": w32, "w64": w64, "bytes": 0.0}, ms * 1e-3, peak32, peak64, 6541.0)
     return {"kernel": "k_adv1d", "bound": b["bound"], "achieved": b["achieved"], "peak": b["peak"], "unit": b["unit"],
             "frac": b["frac"], "traffic": None,
+            "peak_source": {"fp32_tflops": f"measured FMA probe {peak32:.1f}",
+                            "fp64_tflops": f"measured FMA probe {peak64:.1f}"}}
+
+
+def _closure_roofline(kernels, method, classes, ms, local, stream):
+    """Roofline of the closure work alone (a lower bound on the kernels' work, so `frac` is a lower bound): per
+    evaluation the MLP pair in the closure precision plus the FP64 sensors, features and weights; per plateau
+    stencil the sensors and the linear head. classes: (MLP evaluations, plateau stencils, heads per stencil) per
+    step."""
+    from weno_sr_publishing_b200 import _native as N
+    from weno_sr_publishing_b200 import roofline as R
+    ctx = N.context(local)
+    peak32 = ctx.peak_tflops(32, C_stream(stream))
+    peak64 = ctx.peak_tflops(64, C_stream(stream))
+    w32 = w64 = 0.0
+    for mlp_n, plat_n, heads in classes:
+        if method == "sr_f64":
+            w64 += mlp_n * R.MLP_PAIR_FLOPS
+        else:
+            w32 += mlp_n * R.MLP_PAIR_FLOPS
+        w64 += mlp_n * (R.SENSORS64 + R.FEATURES64 + heads * R.HEAD64) + plat_n * (R.SENSORS64 +
+                                                                                   heads * R.HEAD64_PLATEAU)
+    b = R.bound({"w32": w32, "w64": w64, "bytes": 0.0}, ms * 1e-3, peak32, peak64, hbm_peak()["gbs"])
+    return {"kernel": kernels, "bound": b["bound"], "achieved": b["achieved"], "peak": b["peak"], "unit": b["unit"],
+            "frac": b["frac"], "traffic": None, "work": "closure work only (lower bound)",
             "peak_source": {"fp32_tflops": f"measured FMA probe {peak32:.1f}",
                             "fp64_tflops": f"measured FMA probe {peak64:.1f}"}}
 

@@ -14,8 +14,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libwsr.so"
 SOURCES = [CSRC / "wsr_api.cu", CSRC / "wsr_api_1d.cu", CSRC / "wsr_api_w7.cu", CSRC / "euler3d.cu"]
-# euler3d.cu reproduces the reference's 3D Warp module, which is compiled without contraction
+# euler3d.cu's main object reproduces the reference's 3D Warp module for WENO5-JS, which is compiled without
+# contraction; the same file with WSR_EULER3D_SR_UNIT gives the SR stages, with contraction
 EXTRA_FLAGS = {"euler3d.cu": ["-fmad=false"]}
+EXTRA_OBJECTS = {"euler3d.cu": [("_euler3d_sr", ["-DWSR_EULER3D_SR_UNIT", "-diag-suppress=177"])]}
 HEADERS = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "wsr.h"]
 
 NVCC_FLAGS = [
@@ -44,9 +46,13 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or stale():
         compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
         objs, procs = [], []
+        jobs = []
         for src in SOURCES:
-            obj = PKG / ("_" + src.stem + ".o")
-            cmd = [nvcc(), *compile_flags, *EXTRA_FLAGS.get(src.name, []), "-c", "-o", str(obj), str(src)]
+            jobs.append((src, PKG / ("_" + src.stem + ".o"), EXTRA_FLAGS.get(src.name, [])))
+            for stem, flags in EXTRA_OBJECTS.get(src.name, []):
+                jobs.append((src, PKG / (stem + ".o"), flags))
+        for src, obj, flags in jobs:
+            cmd = [nvcc(), *compile_flags, *flags, "-c", "-o", str(obj), str(src)]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             procs.append(subprocess.Popen(cmd))

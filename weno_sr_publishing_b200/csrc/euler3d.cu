@@ -9,9 +9,12 @@
 // dt rule, stages). The HLLC flux and the x-low inflow state have no counterpart there: the 3D workload
 // asks for them (the 2D HLLC of for_paper_results/solvers/weno5_hllc.py:22-113 in three dimensions).
 //
-// This translation unit is built without floating-point contraction (-fmad=false), like the reference's
-// Warp module (fuse_fp False), so that the WENO5-JS path reproduces the reference bit for bit; the MLP
-// keeps explicit fused multiply-adds (closure.cuh fma_t).
+// The file is compiled twice. The main object, with the extern "C" entry points and the WENO5-JS stages, is
+// built without floating-point contraction (-fmad=false), like the reference's Warp module (fuse_fp False), so
+// that the WENO5-JS path reproduces the reference bit for bit. The SR stages (FP64/FP32/BF16 closure), which
+// agree with the reference only to rounding anyway, come from a second object built with contraction
+// (-DWSR_EULER3D_SR_UNIT): euler3d_sr_stage below, called by the main object with plain arguments. The MLP
+// keeps explicit fused multiply-adds in both (closure.cuh fma_t).
 //
 // Work decomposition, per direction d of a stage:
 //   k3_normal  one thread per cell of the normal-extended block: the characteristic reconstruction of the
@@ -698,19 +701,36 @@ int stage3(wsr_ctx* ctx, const Run3& r, const Ws3& w, int stage, cudaStream_t st
   return WSR_OK;
 }
 
+}  // namespace
+
+// One SR stage (defined in the contracted object); the stage's run description as plain arguments.
+int euler3d_sr_stage(wsr_ctx* ctx, int method, double* q, int nx, int ny, int nz, double dx, double dy, double dz,
+                     int flux, int opts, const double* inflow, void* workspace, int stage, cudaStream_t st);
+
+namespace {
+
+#ifndef WSR_EULER3D_SR_UNIT
 int stage_dispatch(wsr_ctx* ctx, int method, const Run3& r, const Ws3& w, int stage, cudaStream_t st) {
+  if (method == WSR_METHOD_JS)
+    return r.flux == 1 ? stage3<M_JS, 1>(ctx, r, w, stage, st) : stage3<M_JS, 0>(ctx, r, w, stage, st);
+  return euler3d_sr_stage(ctx, method, r.q, r.d.nx, r.d.ny, r.d.nz, r.dx, r.dy, r.dz, r.flux, r.opts,
+                          r.in.on ? r.in.v : nullptr, w.ctl, stage, st);
+}
+#else
+int stage_dispatch_sr(wsr_ctx* ctx, int method, const Run3& r, const Ws3& w, int stage, cudaStream_t st) {
   const bool h = r.flux == 1;
   switch (method) {
-    case WSR_METHOD_JS:
-      return h ? stage3<M_JS, 1>(ctx, r, w, stage, st) : stage3<M_JS, 0>(ctx, r, w, stage, st);
     case WSR_METHOD_SR_F64:
       return h ? stage3<M_SR64, 1>(ctx, r, w, stage, st) : stage3<M_SR64, 0>(ctx, r, w, stage, st);
     case WSR_METHOD_SR_F32:
       return h ? stage3<M_SR32, 1>(ctx, r, w, stage, st) : stage3<M_SR32, 0>(ctx, r, w, stage, st);
-    default:
+    case WSR_METHOD_SR_BF16:
       return h ? stage3<M_SRBF16, 1>(ctx, r, w, stage, st) : stage3<M_SRBF16, 0>(ctx, r, w, stage, st);
+    default:
+      return fail(ctx, WSR_ERR_ARG, "bad SR method %d", method);
   }
 }
+#endif
 
 int check3(wsr_ctx* ctx, const double* q, int nx, int ny, int nz, double dx, double dy, double dz, int method,
            int flux, void* ws, size_t wsb) {
@@ -760,6 +780,14 @@ __global__ void k3_init_ctl(Ctl3* ctl, double t, double t_end, double dt, double
 }
 
 }  // namespace
+
+#ifdef WSR_EULER3D_SR_UNIT
+int euler3d_sr_stage(wsr_ctx* ctx, int method, double* q, int nx, int ny, int nz, double dx, double dy, double dz,
+                     int flux, int opts, const double* inflow, void* workspace, int stage, cudaStream_t st) {
+  const Run3 r = make_run(q, nx, ny, nz, dx, dy, dz, flux, opts, inflow);
+  return stage_dispatch_sr(ctx, method, r, carve3(workspace, nx, ny, nz), stage, st);
+}
+#else
 
 extern "C" size_t wsr_euler3d_workspace_bytes(int nx, int ny, int nz) {
   if (nx < 1 || ny < 1 || nz < 1) return 0;
@@ -862,3 +890,4 @@ extern "C" int wsr_euler3d_counters(wsr_ctx* ctx, void* workspace, size_t worksp
   WSR_CUDA(ctx, cudaMemcpy(out_host, w.counters, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return WSR_OK;
 }
+#endif  // WSR_EULER3D_SR_UNIT
