@@ -356,8 +356,11 @@ def main():
         v["share"] = v["ms_per_launch"] * v["launches"] / tot
     dom = max(per_kernel, key=lambda k: per_kernel[k]["share"])
     d = per_kernel[dom]
+    traffic = NCU_TRAFFIC.get((dom, args.method, n))
     line["roofline"] = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
-                        "unit": d["unit"], "frac": d["frac"], "traffic": None,
+                        "unit": d["unit"], "frac": d["frac"], "traffic": traffic,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                          "profiles/k_normal_k_flux_sr_f32_2000.md" if traffic else None,
                         "peak_source": {"fp32_tflops": f"measured FMA probe {peak32:.1f}",
                                         "fp64_tflops": f"measured FMA probe {peak64:.1f}",
                                         "hbm_gbs": hbm["source"]}}
@@ -1144,6 +1147,11 @@ def _closure_roofline(kernels, method, classes, ms, local, stream):
             "frac": b["frac"], "traffic": None, "work": "closure work only (lower bound)",
             "peak_source": {"fp32_tflops": f"measured FMA probe {peak32:.1f}",
                             "fp64_tflops": f"measured FMA probe {peak64:.1f}"}}
+
+
+# DRAM bytes (read + write) of one launch of the dominant kernel, from the ncu capture of the same workload
+# (kernel class, method, grid): the headline configuration only.
+NCU_TRAFFIC = {("flux_x", "sr_f32", 2000): 361.4e6, ("flux_x", "js", 2000): 360.2e6}
 
 
 def C_stream(stream):
