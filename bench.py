@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--method", default="sr_f32", choices=["sr_f32", "sr_f64", "sr_bf16", "js"])
+    ap.add_argument("--method", default="sr_f32", choices=["sr_f32", "sr_f64", "sr_bf16", "sr_bf16_tc", "js"],
+                    help="sr_bf16_tc: the BF16 closure's MLP on the tensor cores (2D step only)")
     ap.add_argument("--n", type=int, default=2000)
     ap.add_argument("--t0", type=float, default=0.125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -72,7 +73,8 @@ def workload_config(args, n_gpus):
     return {"workload": f"2D Euler quadrant Riemann problem {args.n}x{args.n}, seed 0, state at t0={args.t0}",
             "grid": [args.n, args.n], "ghost": 3, "gamma": 1.4, "cfl": 0.4, "boundary": "transmissive",
             "flux": "hllc", "time_integrator": "SSPRK3", "method": args.method,
-            "closure_precision": {"sr_f32": "fp32", "sr_f64": "fp64", "sr_bf16": "bf16", "js": None}[args.method],
+            "closure_precision": {"sr_f32": "fp32", "sr_f64": "fp64", "sr_bf16": "bf16", "sr_bf16_tc": "bf16",
+                                  "js": None}[args.method],
             "state_precision": "fp64", "l2_policy": "inputs larger than L2 (state 4 x 129 MB + 0.8 GB workspace)",
             "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU"}
 

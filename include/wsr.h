@@ -42,6 +42,11 @@ extern "C" {
 #define WSR_METHOD_SR_F32 2   /* WENO5-SR, FP32 MLP, FP64 elsewhere (MIXED) */
 #define WSR_METHOD_SR_BF16 3  /* WENO5-SR, BF16 inputs/parameters/activations, FP32 accumulation */
 #define WSR_METHOD_Z 4        /* WENO5-Z (Borges p = 2, eps = h^2 per direction); 2D functions only */
+#define WSR_METHOD_SR_BF16_TC 5 /* WENO5-SR with the BF16 closure's MLP on the tensor cores (warp mma.sync, BF16 x BF16
+                                 * -> FP32); the same results as WSR_METHOD_SR_BF16 up to the accumulation order. An
+                                 * addition without a counterpart in the reference; measured slower than
+                                 * WSR_METHOD_SR_BF16 on B200, kept for that comparison. wsr_euler2d_stage(_at) and
+                                 * wsr_euler2d_run only */
 
 /* boundaries */
 #define WSR_BC_TRANSMISSIVE 0

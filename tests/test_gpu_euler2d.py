@@ -240,3 +240,29 @@ def test_force_ten_step_run_matches_oracle(case, method, tol):
     bufs2 = [_t(init)] + [torch.zeros_like(_t(init)) for _ in range(3)]
     res2 = E.run(bufs2, p, 1.0, method, bc, mlp_params=PARAMS[method], fixed_steps=10)
     assert _rel(_interior(bufs2[res2.final_slot].cpu().numpy(), nx, ny), _interior(got, nx, ny)) > 1e-8
+
+
+# The BF16 closure with its MLP on the tensor cores (sr_bf16_tc) against the same closure on the FMA pipes (sr_bf16)
+# and the oracle: only the FP32 accumulation order inside the tensor core differs, which can move a bfloat16
+# activation by one rounding unit at a tie.
+@pytest.mark.parametrize("case", CASES)
+def test_bf16_tensor_core_closure_matches_fma_closure(case):
+    e = np.load(G / f"euler2d_{case}.npz")
+    nx, ny, bc = int(e["nx"]), int(e["ny"]), str(e["bc"])
+    p = Params(nx=nx, ny=ny, x_length=1.0, y_length=1.0, cfl=0.4)
+    u0 = e["initial"]
+    dt = 0.3 * min(p.dx, p.dy) / O.max_speed(u0, nx, ny)
+    outs = {}
+    for method in ("sr_bf16", "sr_bf16_tc"):
+        out = torch.zeros(p.padded_shape, dtype=torch.float64, device=DEV)
+        E.stage(_t(u0), _t(u0), out, p, dt, 1, method, bc, mlp_params=P32)
+        outs[method] = _interior(out.cpu().numpy(), nx, ny)
+    ref = O.euler2d_stage(u0, u0, np.zeros_like(u0), nx, ny, p.dx, p.dy, dt, 1, "sr_bf16", bc, params=P32)
+    assert _rel(outs["sr_bf16_tc"], outs["sr_bf16"]) <= 1e-4
+    assert _rel(outs["sr_bf16_tc"], _interior(ref, nx, ny)) <= STAGE_TOL["sr_bf16"]
+    bufs = [_t(u0)] + [torch.zeros_like(_t(u0)) for _ in range(3)]
+    res = E.run(bufs, p, 1.0, "sr_bf16_tc", bc, mlp_params=P32, fixed_steps=5)
+    bufs2 = [_t(u0)] + [torch.zeros_like(_t(u0)) for _ in range(3)]
+    res2 = E.run(bufs2, p, 1.0, "sr_bf16", bc, mlp_params=P32, fixed_steps=5)
+    got, want = bufs[res.final_slot].cpu().numpy(), bufs2[res2.final_slot].cpu().numpy()
+    assert _rel(_interior(got, nx, ny), _interior(want, nx, ny)) <= 1e-3

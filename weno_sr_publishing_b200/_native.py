@@ -15,9 +15,9 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libwsr.so"
 
 WSR_OK, WSR_ERR_ARG, WSR_ERR_CUDA, WSR_ERR_NO_CLOSURE = 0, 1, 2, 3
-METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3, "z": 4}
+METHOD = {"js": 0, "sr_f64": 1, "sr_f32": 2, "sr_bf16": 3, "z": 4, "sr_bf16_tc": 5}
 # methods whose weights come from an uploaded MLP closure
-SR_METHODS = ("sr_f64", "sr_f32", "sr_bf16")
+SR_METHODS = ("sr_f64", "sr_f32", "sr_bf16", "sr_bf16_tc")
 BC = {"transmissive": 0, "periodic": 1, "double-mach": 2}
 BC_Y_HALO = 16  # flag: y ghost rows read as stored (slabs of a y-decomposed grid)
 FLUX = {"hllc": 0, "force": 1}

@@ -25,11 +25,12 @@
 
 namespace wsr {
 
-enum Method { M_JS = 0, M_SR64 = 1, M_SR32 = 2, M_SRBF16 = 3, M_Z = 4 };
+// M_SRBF16_TC: the BF16 closure with its MLP on the tensor cores (closure_mma.cuh; the 2D reconstruction kernels only)
+enum Method { M_JS = 0, M_SR64 = 1, M_SR32 = 2, M_SRBF16 = 3, M_Z = 4, M_SRBF16_TC = 5 };
 
 // Methods whose weights come from the MLP closure (and so run the compacted plateau/queue split).
 template <int M>
-__host__ __device__ constexpr bool has_mlp() { return M == M_SR64 || M == M_SR32 || M == M_SRBF16; }
+__host__ __device__ constexpr bool has_mlp() { return M == M_SR64 || M == M_SR32 || M == M_SRBF16 || M == M_SRBF16_TC; }
 
 // Packed parameters, layout w1[5][10] b1[10] w2[10][6] b2[6] w3[6][6] b3[6] w4[6][3] b4[3].
 constexpr int kW1 = 0, kB1 = 50, kW2 = 60, kB2 = 120, kW3 = 126, kB3 = 162, kW4 = 168, kB4 = 186;
@@ -65,6 +66,10 @@ struct ClosureParams<M_SR32> {
 };
 template <>
 struct ClosureParams<M_SRBF16> {
+  using type = Mlp5f;  // pre-rounded to bfloat16 on upload
+};
+template <>
+struct ClosureParams<M_SRBF16_TC> {
   using type = Mlp5f;  // pre-rounded to bfloat16 on upload
 };
 template <>
@@ -533,7 +538,7 @@ __device__ __forceinline__ void closure_from_features(const typename QIn<M>::T* 
     r1 = 0.5 * (ra[1] + rb[1]);
     r2 = 0.5 * (ra[2] + rb[0]);
   } else {
-    constexpr bool B = M == M_SRBF16;
+    constexpr bool B = M == M_SRBF16 || M == M_SRBF16_TC;
     float xa[5] = {x[0], x[1], x[2], x[3], x[4]};
     float xb[5] = {x[2], x[1], x[0], x[3], x[4]};
     float ra[3], rb[3];
@@ -555,12 +560,35 @@ template <int M>
 __device__ __forceinline__ typename QIn<M>::T to_queue(double f) {
   if constexpr (M == M_SR64)
     return f;
-  else if constexpr (M == M_SRBF16)
+  else if constexpr (M == M_SRBF16 || M == M_SRBF16_TC)
     return bf16r((float)f);
   else
     return (float)f;
 }
 
+
+// MLP inputs of the reduced-precision closures (FP32; BF16 rounds them to bfloat16): the differences are FP64
+// (they cancel), the normalisation, gamma and the scale feature are formed in FP32 (the MLP consumes FP32 inputs;
+// dmax >= 1e-13 here, so every value is a normal float).
+template <int M>
+__device__ __forceinline__ void sr_features32(const double s[5], const Sens& se, float x[5]) {
+  const double d20 = s[0] - 2.0 * s[1] + s[2], d21 = s[1] - 2.0 * s[2] + s[3], d22 = s[2] - 2.0 * s[3] + s[4];
+  const float inv = rcp_nr((float)se.dmax);
+  const float e = 1.0e-15f;
+  x[0] = (float)se.d0 * inv;
+  x[1] = (float)se.d1 * inv;
+  x[2] = (float)se.d2 * inv;
+  const float g0 = __fdividef(fabsf((float)d20), (float)(fabs(s[1] - s[0]) + fabs(s[2] - s[1])) + e);
+  const float g1 = __fdividef(fabsf((float)d21), (float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
+  const float g2 = __fdividef(fabsf((float)d22), (float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
+  x[3] = fminf(1.0f, fmaxf(fmaxf(g0, g1), g2));
+  const float rel = (float)se.dmax * rcp_nr((float)se.qscale);
+  x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (__log10f(rel) + 4.0f) * 0.25f)));
+  if constexpr (M == M_SRBF16 || M == M_SRBF16_TC) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) x[k] = bf16r(x[k]);
+  }
+}
 
 // SR closure of one non-plateau stencil -> reciprocal scaled betas (features FP64 as in DEPLOY:96-120,
 // the MLP in the closure precision, ratios averaged and inverted in FP64 as in DEPLOY:234-247).
@@ -570,26 +598,8 @@ __device__ __forceinline__ void sr_betas(const double s[5], const typename Closu
   const Sens se = sensors5(s);
 #if WSR_FEATURES_F32
   if constexpr (M != M_SR64) {
-    // FP32 closure: the differences are FP64 (they cancel), the normalisation, gamma and the scale
-    // feature are formed in FP32 (the MLP consumes FP32 inputs; dmax >= 1e-13 here, so every value is
-    // a normal float).
-    const double d20 = s[0] - 2.0 * s[1] + s[2], d21 = s[1] - 2.0 * s[2] + s[3], d22 = s[2] - 2.0 * s[3] + s[4];
-    const float inv = rcp_nr((float)se.dmax);
-    const float e = 1.0e-15f;
     float x[5];
-    x[0] = (float)se.d0 * inv;
-    x[1] = (float)se.d1 * inv;
-    x[2] = (float)se.d2 * inv;
-    const float g0 = __fdividef(fabsf((float)d20), (float)(fabs(s[1] - s[0]) + fabs(s[2] - s[1])) + e);
-    const float g1 = __fdividef(fabsf((float)d21), (float)(fabs(s[2] - s[1]) + fabs(s[3] - s[2])) + e);
-    const float g2 = __fdividef(fabsf((float)d22), (float)(fabs(s[3] - s[2]) + fabs(s[4] - s[3])) + e);
-    x[3] = fminf(1.0f, fmaxf(fmaxf(g0, g1), g2));
-    const float rel = (float)se.dmax * rcp_nr((float)se.qscale);
-    x[4] = rel >= 1.0f ? 1.0f : (rel <= 1.0e-4f ? 0.0f : fminf(1.0f, fmaxf(0.0f, (__log10f(rel) + 4.0f) * 0.25f)));
-    if constexpr (M == M_SRBF16) {
-#pragma unroll
-      for (int k = 0; k < 5; ++k) x[k] = bf16r(x[k]);
-    }
+    sr_features32<M>(s, se, x);
     closure_from_features<M>(x, P, a0, a1, a2);
     return;
   }

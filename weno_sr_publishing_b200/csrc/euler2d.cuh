@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include "closure.cuh"
+#include "closure_mma.cuh"
 #include "euler_math.cuh"
 
 namespace wsr {
@@ -248,7 +249,33 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
     if constexpr (has_mlp<M>()) queue_push(need, n * kBlock + t, s_q, &s_count);
   }
   // Phase B
-  if constexpr (has_mlp<M>()) {
+  if constexpr (M == M_SRBF16_TC) {
+    // BF16 closure on the tensor cores: each warp takes 32 queue entries at a time (closure_mma.cuh)
+    __syncthreads();
+    const int count = s_count;
+    if (count > 0) {
+      const MmaW5 W = mma_weights(P.p, t & 31);
+#pragma unroll 1
+      for (int base = t & ~31; base < count; base += kBlock) {  // the same bound for every lane of a warp
+        const int e = base + (t & 31);
+        const bool valid = e < count;
+        int n = 0, o = 0;
+        double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        float x[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (valid) {
+          const int id = s_q[e];
+          n = id / kBlock;
+          o = id % kBlock;
+#pragma unroll
+          for (int k = 0; k < 5; ++k) s[k] = s_ch[n >> 1][k + (n & 1)][o];
+          sr_features32<M>(s, sensors5(s), x);
+        }
+        double a0, a1, a2;
+        closure_bf16_mma(W, x, a0, a1, a2);
+        if (valid) s_val[n][o] = sr_value<M>(s, n & 1, a0, a1, a2, opts, tally);
+      }
+    }
+  } else if constexpr (has_mlp<M>()) {
     __syncthreads();
     const int count = s_count;
 #pragma unroll 1
@@ -382,7 +409,35 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
     if constexpr (has_mlp<M>()) queue_push(need, n * kBlock + t, s_q, &s_count);
   }
   // Phase B: one closure evaluation per queued stencil serves both Gauss points.
-  if constexpr (has_mlp<M>()) {
+  if constexpr (M == M_SRBF16_TC) {
+    // BF16 closure on the tensor cores: each warp takes 32 queue entries at a time (closure_mma.cuh)
+    __syncthreads();
+    const int count = s_count;
+    if (count > 0) {
+      const MmaW5 W = mma_weights(P.p, t & 31);
+#pragma unroll 1
+      for (int base = t & ~31; base < count; base += kBlock) {  // the same bound for every lane of a warp
+        const int e = base + (t & 31);
+        const bool valid = e < count;
+        int n = 0, o = 0;
+        double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        float x[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (valid) {
+          const int id = s_q[e];
+          n = id / kBlock;
+          o = id % kBlock;
+          load_transverse<DIR>(fl, fr, nx, TL::x(o), TL::y(o), n, true, s);
+          sr_features32<M>(s, sensors5(s), x);
+        }
+        double a0, a1, a2;
+        closure_bf16_mma(W, x, a0, a1, a2);
+        if (valid) {
+          s_g[0][n][o] = sr_value<M>(s, 2, a0, a1, a2, opts, tally);
+          s_g[1][n][o] = sr_value<M>(s, 3, a0, a1, a2, opts, tally);
+        }
+      }
+    }
+  } else if constexpr (has_mlp<M>()) {
     __syncthreads();
     const int count = s_count;
 #pragma unroll 1

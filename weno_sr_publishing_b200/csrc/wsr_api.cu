@@ -67,7 +67,7 @@ int check_2d(wsr_ctx* ctx, int nx, int ny, int method, int bc, int flux, void* w
   if (nx < 3 || ny < 3) return fail(ctx, WSR_ERR_ARG, "nx and ny must be >= 3 (got %d, %d)", nx, ny);
   if ((long long)(nx + 6) * (ny + 6) > (1ll << 31) / 4)
     return fail(ctx, WSR_ERR_ARG, "grid %d x %d too large for one launch", nx, ny);
-  if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16_TC) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
   const int base = bc & ~WSR_BC_Y_HALO;
   if (base != WSR_BC_TRANSMISSIVE && base != WSR_BC_PERIODIC && base != WSR_BC_DOUBLE_MACH)
     return fail(ctx, WSR_ERR_ARG, "bad boundary %d", bc);
@@ -187,6 +187,8 @@ int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, 
       return launch_stage<M_SR32>(ctx, a, w, st);
     case WSR_METHOD_Z:
       return launch_stage<M_Z>(ctx, a, w, st);
+    case WSR_METHOD_SR_BF16_TC:
+      return launch_stage<M_SRBF16_TC>(ctx, a, w, st);
     default:
       return launch_stage<M_SRBF16>(ctx, a, w, st);
   }

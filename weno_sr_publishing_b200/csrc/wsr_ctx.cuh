@@ -92,5 +92,9 @@ template <>
 inline const Mlp5f& params_of<M_SRBF16>(const wsr_ctx* ctx) {
   return ctx->pbf16;
 }
+template <>
+inline const Mlp5f& params_of<M_SRBF16_TC>(const wsr_ctx* ctx) {
+  return ctx->pbf16;
+}
 
 }  // namespace wsr_detail
