@@ -15,6 +15,7 @@
 //                    computed per face in k_flux_y, and k_update forms the flux divergence, the SSPRK3
 //                    combination and (after the last stage) the max wave speed for the next dt.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -333,24 +334,101 @@ __device__ __forceinline__ d4 riemann(const d4& ul, const d4& ur, int flux, doub
 // y faces: face (j, i), j in [0, ny], i in [0, nx): u_R from yl[j+1][i+1..i+5], u_L from yr[j][i+1..i+5]
 // (REFSYM:198-266). Output fy[j][i] of a [ny+1][nx] face array.
 // Each of the 8 stencils (4 components x 2 sides) evaluates its closure once for both Gauss points.
+// Stencil tiles of the transverse kernels, staged into shared memory by TMA (cp.async.bulk.tensor). A face-value
+// array [rows][cols][4] FP64 is the 4D tensor {2 values, 2 pairs, cols, rows} (byte strides 16, 32, 32 cols), so a
+// box holds one pair of components with a 16-byte inner extent and an x coordinate of 0 (every copy starts on a
+// 16-byte boundary). Per block: x faces (32 x 4) read rows j0+1 .. j0+8 and columns i0 .. i0+32 of xl and xr;
+// y faces (128 x 1) read row j+1 of yl and row j of yr, columns i0+1 .. i0+132. Boxes past the array's end are
+// filled with zeros by the copy (those values belong to inactive faces).
 template <int DIR>
-__device__ __forceinline__ void load_transverse(const double* __restrict__ fl, const double* __restrict__ fr, int nx,
-                                                int i, int j, int n, bool active, double s[5]) {
+struct FluxTile {
+  static constexpr int cols = DIR == 1 ? 33 : 132, rows = DIR == 1 ? 8 : 1;
+  static constexpr int box_doubles = 2 * cols * rows;
+  static constexpr int stride = (box_doubles + 15) / 16 * 16;  // 128-byte aligned boxes
+  static constexpr unsigned box_bytes = box_doubles * sizeof(double);
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void tma_load_box(double* dst, const CUtensorMap* map, int pair, int col, int row,
+                                             unsigned long long* mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(0), "r"(pair), "r"(col), "r"(row), "r"(smem_u32(mbar))
+      : "memory");
+}
+
+// Issues the block's four boxes (thread 0) and waits for them (every thread), at most about 2^22 polls; false
+// when the copies did not complete in time.
+template <int DIR>
+__device__ __forceinline__ bool load_flux_tile(double* tile, unsigned long long* mbar, const CUtensorMap* map_l,
+                                               const CUtensorMap* map_r, int i0, int j0) {
+  using FT = FluxTile<DIR>;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
+                 "r"(4u * FT::box_bytes)
+                 : "memory");
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int side = b >> 1, pair = b & 1;
+      const int col = DIR == 1 ? i0 : i0 + 1;
+      const int row = DIR == 1 ? j0 + 1 : (side == 0 ? j0 + 1 : j0);
+      tma_load_box(tile + b * FT::stride, side == 0 ? map_l : map_r, pair, col, row, mbar);
+    }
+  }
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(mbar))
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// After a timed-out wait: wait once more (bounded) so that no copy is still writing the block's shared memory
+// when it exits.
+__device__ __forceinline__ void load_flux_tile_wait_again(unsigned long long* mbar) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(mbar))
+        : "memory");
+    if (done) return;
+  }
+}
+
+// Stencil n = 2 comp + side of face (i, j) from the block's tile (i0, j0: the block's first face).
+template <int DIR>
+__device__ __forceinline__ void tile_transverse(const double* tile, int i, int j, int i0, int j0, int n, bool active,
+                                                double s[5]) {
+  using FT = FluxTile<DIR>;
   const int comp = n >> 1, side = n & 1;
-  const double* src = side == 0 ? fl : fr;
   if (!active) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) s[k] = 0.0;
     return;
   }
+  const double* box = tile + (side * 2 + (comp >> 1)) * FT::stride + (comp & 1);
   if (DIR == 1) {
-    const int ncols = nx + 2, col = side == 0 ? i + 1 : i;
+    const int cc = side == 0 ? i - i0 + 1 : i - i0;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)(j + 1 + k) * ncols + col) * 4 + comp);
+    for (int k = 0; k < 5; ++k) s[k] = box[((j - j0 + k) * FT::cols + cc) * 2];
   } else {
-    const int ncols = nx + 6, row = side == 0 ? j + 1 : j;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) s[k] = __ldg(src + ((size_t)row * ncols + (i + 1 + k)) * 4 + comp);
+    for (int k = 0; k < 5; ++k) s[k] = box[(i - i0 + k) * 2];
   }
 }
 
@@ -360,20 +438,30 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
                                                     const StepCtl* __restrict__ ctl, int opts,
                                                     int* __restrict__ fallbacks,
                                                     unsigned long long* __restrict__ counters,
-                                                    const __grid_constant__ typename ClosureParams<M>::type P) {
+                                                    const __grid_constant__ typename ClosureParams<M>::type P,
+                                                    const __grid_constant__ CUtensorMap map_l,
+                                                    const __grid_constant__ CUtensorMap map_r) {
   __shared__ double s_g[2][kStencilsPerThread][kBlock];  // values at Gauss points 1 and 2
   __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
+  __shared__ __align__(128) double s_tile[4 * FluxTile<DIR>::stride];
+  __shared__ unsigned long long s_mbar;
   __shared__ int s_count;
   if (ctl->done) return;  // uniform across the launch
   using TL = Tile<DIR == 1>;
   const int t = threadIdx.x;
   const int i = TL::x(t);
   const int j = TL::y(t);
+  const int i0 = blockIdx.x * TL::bx, j0 = blockIdx.y * TL::by;
   const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
   const bool active = i < nfx && j < nfy;
   const double dt_h = DIR == 1 ? ctl->dt_dx : ctl->dt_dy;
   if (t == 0) s_count = 0;
-  __syncthreads();
+  const bool tile_ok = load_flux_tile<DIR>(s_tile, &s_mbar, &map_l, &map_r, i0, j0);
+  if (__syncthreads_or(!tile_ok)) {  // the same decision in every thread of the block
+    if (t == 0) atomicExch(&fallbacks[1], 1);
+    if (!tile_ok) load_flux_tile_wait_again(&s_mbar);
+    return;
+  }
   Tally tally;
   const bool work = active;
   // Phase A, two stencils per iteration. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L
@@ -381,7 +469,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
 #pragma unroll 2
   for (int n = 0; n < kStencilsPerThread; ++n) {
     double s[5];
-    load_transverse<DIR>(fl, fr, nx, i, j, n, work, s);
+    tile_transverse<DIR>(s_tile, i, j, i0, j0, n, work, s);
     bool need = false;
     if (!work) {
       // nothing to reconstruct
@@ -426,7 +514,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
           const int id = s_q[e];
           n = id / kBlock;
           o = id % kBlock;
-          load_transverse<DIR>(fl, fr, nx, TL::x(o), TL::y(o), n, true, s);
+          tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o), i0, j0, n, true, s);
           sr_features32<M>(s, sensors5(s), x);
         }
         double a0, a1, a2;
@@ -445,7 +533,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       const int id = s_q[e];
       const int n = id / kBlock, o = id % kBlock;
       double s[5];
-      load_transverse<DIR>(fl, fr, nx, TL::x(o), TL::y(o), n, true, s);
+      tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o), i0, j0, n, true, s);
       double a0, a1, a2;
       sr_betas<M>(s, P, a0, a1, a2);
       s_g[0][n][o] = sr_value<M>(s, 2, a0, a1, a2, opts, tally);

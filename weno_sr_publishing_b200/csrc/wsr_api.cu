@@ -9,6 +9,8 @@
 #include <mutex>
 #include <new>
 
+#include <cuda.h>
+
 #include "../../include/wsr.h"
 #include "euler2d.cuh"
 #include "wsr_ctx.cuh"
@@ -60,6 +62,48 @@ Ws2d carve(void* base, int nx, int ny) {
   p += cells_bytes((size_t)ny * (nx + 1));
   w.fy = reinterpret_cast<double*>(p);
   return w;
+}
+
+// Tensor maps of the four face-value arrays for the TMA tile loads of k_flux (euler2d.cuh FluxTile): each array
+// [rows][cols][4] FP64 as the 4D tensor {2, 2, cols, rows}; boxes {2, 1, 33, 8} (x faces) and {2, 1, 132, 1}
+// (y faces). cuTensorMapEncodeTiled comes through the runtime's driver entry point (no link to libcuda).
+struct FaceMaps {
+  CUtensorMap xl, xr, yl, yr;
+};
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+bool face_map(CUtensorMap* m, double* base, int cols, int rows, int box_cols, int box_rows) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {2, 2, (cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[3] = {16, 32, (cuuint64_t)cols * 32};
+  const cuuint32_t box[4] = {2, 1, (cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+bool face_maps(const Ws2d& w, int nx, int ny, FaceMaps* fm) {
+  return face_map(&fm->xl, w.xl, nx + 2, ny + 6, FluxTile<1>::cols, FluxTile<1>::rows) &&
+         face_map(&fm->xr, w.xr, nx + 2, ny + 6, FluxTile<1>::cols, FluxTile<1>::rows) &&
+         face_map(&fm->yl, w.yl, nx + 6, ny + 2, FluxTile<2>::cols, FluxTile<2>::rows) &&
+         face_map(&fm->yr, w.yr, nx + 6, ny + 2, FluxTile<2>::cols, FluxTile<2>::rows);
 }
 
 int check_2d(wsr_ctx* ctx, int nx, int ny, int method, int bc, int flux, void* ws, size_t wsb) {
@@ -137,7 +181,7 @@ typename ClosureParams<M>::type stage_params(const wsr_ctx* ctx, const StageArgs
 }
 
 template <int M>
-int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
+int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st) {
   const auto P = stage_params<M>(ctx, a);
   const dim3 blk(128);  // the reconstruction kernels compact closure work per warp of a 128-thread block
   {
@@ -158,14 +202,14 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t s
     ProfScope ps(ctx, st, 2);
     dim3 grd((a.nx + 1 + 31) / 32, (a.ny + 3) / 4);
     k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
-                                      w.counters + 4, P);
+                                      w.counters + 4, P, fm.xl, fm.xr);
   }
   WSR_LAUNCHED(ctx, "k_flux<x>");
   {
     ProfScope ps(ctx, st, 3);
     dim3 grd((a.nx + 127) / 128, a.ny + 1);
     k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
-                                      w.counters + 6, P);
+                                      w.counters + 6, P, fm.yl, fm.yr);
   }
   WSR_LAUNCHED(ctx, "k_flux<y>");
   {
@@ -177,20 +221,20 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, cudaStream_t s
   return WSR_OK;
 }
 
-int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
+int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st) {
   switch (method) {
     case WSR_METHOD_JS:
-      return launch_stage<M_JS>(ctx, a, w, st);
+      return launch_stage<M_JS>(ctx, a, w, fm, st);
     case WSR_METHOD_SR_F64:
-      return launch_stage<M_SR64>(ctx, a, w, st);
+      return launch_stage<M_SR64>(ctx, a, w, fm, st);
     case WSR_METHOD_SR_F32:
-      return launch_stage<M_SR32>(ctx, a, w, st);
+      return launch_stage<M_SR32>(ctx, a, w, fm, st);
     case WSR_METHOD_Z:
-      return launch_stage<M_Z>(ctx, a, w, st);
+      return launch_stage<M_Z>(ctx, a, w, fm, st);
     case WSR_METHOD_SR_BF16_TC:
-      return launch_stage<M_SRBF16_TC>(ctx, a, w, st);
+      return launch_stage<M_SRBF16_TC>(ctx, a, w, fm, st);
     default:
-      return launch_stage<M_SRBF16>(ctx, a, w, st);
+      return launch_stage<M_SRBF16>(ctx, a, w, fm, st);
   }
 }
 
@@ -212,7 +256,8 @@ __global__ void k_init_ctl(StepCtl* ctl, int* fallbacks, unsigned long long* cou
   ctl->max_steps = max_steps;
   ctl->cfl = cfl;
   ctl->hmin = hmin;
-  *fallbacks = 0;
+  fallbacks[0] = 0;
+  fallbacks[1] = 0;  // set by k_flux when a stencil tile load timed out
   for (int k = 0; k < 8; ++k) counters[k] = 0ull;
 }
 
@@ -322,8 +367,10 @@ int wsr_euler2d_stage_at(wsr_ctx* ctx, const double* u_stage, const double* u0, 
   Ws2d w = carve(workspace, nx, ny);
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, boundary_time, 1.0e300, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
   WSR_LAUNCHED(ctx, "k_init_ctl");
+  FaceMaps fm;
+  if (!face_maps(w, nx, ny, &fm)) return fail(ctx, WSR_ERR_CUDA, "encoding the face-value tensor maps failed");
   StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma, 0.0};
-  return dispatch_stage(ctx, method, a, w, st);
+  return dispatch_stage(ctx, method, a, w, fm, st);
 }
 
 int wsr_euler2d_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, double* u_out, int nx, int ny,
@@ -382,6 +429,8 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   WSR_LAUNCHED(ctx, "k_init_ctl");
   k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u[0], nx, ny, gamma, &w.ctl->max_speed_bits);
   WSR_LAUNCHED(ctx, "k_max_speed");
+  FaceMaps fm;
+  if (!face_maps(w, nx, ny, &fm)) return fail(ctx, WSR_ERR_CUDA, "encoding the face-value tensor maps failed");
   const int batch = 16;  // steps launched between host polls (<= kDtsRing)
   int host_steps = 0;    // steps the host has launched
   int seen_steps = 0;    // steps whose dt has been copied out
@@ -404,9 +453,9 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
       StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma, 0.0};
       StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma, 1.0};
       StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma, 0.5};
-      if ((rc = dispatch_stage(ctx, method, a1, w, st))) return rc;
-      if ((rc = dispatch_stage(ctx, method, a2, w, st))) return rc;
-      if ((rc = dispatch_stage(ctx, method, a3, w, st))) return rc;
+      if ((rc = dispatch_stage(ctx, method, a1, w, fm, st))) return rc;
+      if ((rc = dispatch_stage(ctx, method, a2, w, fm, st))) return rc;
+      if ((rc = dispatch_stage(ctx, method, a3, w, fm, st))) return rc;
       {
         ProfScope ps(ctx, st, 5);
         k_step_end<<<1, 1, 0, st>>>(w.ctl);
@@ -423,12 +472,13 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
     seen_steps = snap.steps;
     done = snap.done;
   }
-  int fb = 0;
-  WSR_CUDA(ctx, cudaMemcpy(&fb, w.fallbacks, sizeof(int), cudaMemcpyDeviceToHost));
+  int fb[2] = {0, 0};
+  WSR_CUDA(ctx, cudaMemcpy(fb, w.fallbacks, sizeof(fb), cudaMemcpyDeviceToHost));
+  if (fb[1]) return fail(ctx, WSR_ERR_CUDA, "a stencil tile load (TMA) did not complete in time");
   if (steps_out) *steps_out = snap.steps;
   if (t_out) *t_out = snap.t;
   if (final_slot) *final_slot = (snap.steps & 1) ? 3 : 0;
-  if (fallbacks_out) *fallbacks_out = fb;
+  if (fallbacks_out) *fallbacks_out = fb[0];
   return WSR_OK;
 }
 
@@ -569,16 +619,19 @@ int noalloc_scratch_for(int dev, void** out) {
 }
 
 template <int M>
-int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a, const Ws2d& w, cudaStream_t st) {
+int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a, const Ws2d& w, const FaceMaps& fm,
+                   cudaStream_t st) {
   const dim3 blk(128);
   k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny + 5), blk, 0, st>>>(
       a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
   k_normal<M, 2><<<dim3((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4), blk, 0, st>>>(
       a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
   k_flux<M, 1><<<dim3((a.nx + 1 + 31) / 32, (a.ny + 3) / 4), blk, 0, st>>>(
-      w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P);
+      w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P, fm.xl,
+      fm.xr);
   k_flux<M, 2><<<dim3((a.nx + 127) / 128, a.ny + 1), blk, 0, st>>>(
-      w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P);
+      w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P, fm.yl,
+      fm.yr);
   k_update<<<dim3((a.nx + 255) / 256, a.ny), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk,
                                                           a.g, w.ctl);
   // the error state was drained on entry, so an error here comes from these launches
@@ -608,31 +661,33 @@ extern "C" int wsr_euler2d_stage_noalloc(const double* u_stage, const double* u0
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   Ws2d w = carve(scratch, nx, ny);
+  FaceMaps fm;
+  if (!face_maps(w, nx, ny, &fm)) return WSR_ERR_CUDA;
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
   if (cudaPeekAtLastError() != cudaSuccess) return WSR_ERR_CUDA;
   StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma, 0.0};
   switch (method) {
     case WSR_METHOD_JS:
-      return noalloc_launch<M_JS>(NoParams{}, a, w, st);
+      return noalloc_launch<M_JS>(NoParams{}, a, w, fm, st);
     case WSR_METHOD_Z:
-      return noalloc_launch<M_Z>(ZEps{dx * dx, dy * dy}, a, w, st);
+      return noalloc_launch<M_Z>(ZEps{dx * dx, dy * dy}, a, w, fm, st);
     case WSR_METHOD_SR_F64: {
       Mlp5d P;
       for (int k = 0; k < kParams5; ++k) P.p[k] = closure_params[k];
-      return noalloc_launch<M_SR64>(P, a, w, st);
+      return noalloc_launch<M_SR64>(P, a, w, fm, st);
     }
     case WSR_METHOD_SR_F32: {
       Mlp5f P;
       for (int k = 0; k < kParams5; ++k) P.p[k] = static_cast<float>(closure_params[k]);
       P.duplicate();
-      return noalloc_launch<M_SR32>(P, a, w, st);
+      return noalloc_launch<M_SR32>(P, a, w, fm, st);
     }
     default: {
       Mlp5f P;
       for (int k = 0; k < kParams5; ++k)
         P.p[k] = __bfloat162float(__float2bfloat16_rn(static_cast<float>(closure_params[k])));
       P.duplicate();
-      return noalloc_launch<M_SRBF16>(P, a, w, st);
+      return noalloc_launch<M_SRBF16>(P, a, w, fm, st);
     }
   }
 }
