@@ -247,6 +247,34 @@ int wsr_profile_enable(wsr_ctx *ctx, int on);
  * launch count (arrays of WSR_PROF_KINDS). */
 int wsr_profile_read(wsr_ctx *ctx, double *ms, long long *launches);
 
+/* ---- device-resident time loop of one y-slab (an addition: the reference runs one grid per GPU) ----
+ * The dt rule, the stop test and t live in the workspace's control block, as in wsr_euler2d_run, so a decomposed
+ * run needs no host synchronisation per step. Per step, on the slab's stream:
+ *   wsr_euler2d_slab_step(phase 0)   dt from the wave-speed slot (which must hold the MAX over all slabs), the stop
+ *                                    test, the slot cleared for the step's own maximum;
+ *   3 x (halo exchange by the caller, WSR_BC_Y_HALO rows; wsr_euler2d_slab_stage(rk = 1, 2, 3))  the SSPRK3 stages
+ *                                    with the control block's dt; the third leaves the local wave speed in the slot;
+ *   all-reduce (MAX) of the slot across ranks by the caller (the slot holds the non-negative double's bit pattern,
+ *                                    so a 64-bit integer MAX is the MAX of the speeds);
+ *   wsr_euler2d_slab_step(phase 1)   t += dt, steps += 1.
+ * wsr_euler2d_slab_begin initialises the control block and puts the initial state's local wave speed in the slot
+ * (all-reduce it before the first step); wsr_euler2d_slab_speed_slot returns the slot's device address;
+ * wsr_euler2d_slab_status synchronises the stream and reads steps, t, the stop flag and the ring of the last 64 dts
+ * (dts_ring[s % 64] = dt of step s). Steps launched after the stop flag is set do nothing, so the caller may launch
+ * several steps between status reads; the result is in the buffer of step `steps`. */
+int wsr_euler2d_slab_begin(wsr_ctx *ctx, const double *u, int nx, int ny, double dx, double dy, double gamma,
+                           double cfl, double t_start, double t_end, int max_steps, void *workspace,
+                           size_t workspace_bytes, void *stream);
+int wsr_euler2d_slab_speed_slot(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny,
+                                unsigned long long **slot);
+int wsr_euler2d_slab_step(wsr_ctx *ctx, int phase, int nx, int ny, double dx, double dy, void *workspace,
+                          size_t workspace_bytes, void *stream);
+int wsr_euler2d_slab_stage(wsr_ctx *ctx, const double *u_stage, const double *u0, double *u_out, int nx, int ny,
+                           double dx, double dy, double gamma, int rk, int method, int bc, int flux, int opts,
+                           void *workspace, size_t workspace_bytes, void *stream);
+int wsr_euler2d_slab_status(wsr_ctx *ctx, void *workspace, size_t workspace_bytes, int nx, int ny, int *steps,
+                            double *t, int *done, double *dts_ring, void *stream);
+
 /* Closure tallies of the last run/stage made with WSR_OPT_COUNT, per kernel class k = normal x,
  * normal y, flux x, flux y: out_host[2k] = stencils that ran the MLP pair, out_host[2k+1] = plateau
  * stencils that took the linear weights (out_host holds 8 values). */

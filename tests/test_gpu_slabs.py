@@ -101,6 +101,18 @@ def test_one_rank_nccl_group(boundary):
                     S.DistSlabs(), S.CudaStages("sr_f32", _closure("sr_f32")))
         assert res.steps == rres.steps and res.t == rres.t
         np.testing.assert_array_equal(S.gather_interior(res.slabs), ref)
+        # the device-resident loop (dt and the stop test on the device) equals the host-driven loop bit for bit,
+        # also when the run stops inside a batch of launched steps (max_steps)
+        host = S.run([torch.as_tensor(init, device=DEV).clone()], [S.slab_params(p, 1, 0)], 0.02, boundary,
+                     S.DistSlabs(), S.CudaStages("sr_f32", _closure("sr_f32")), host_loop=True)
+        assert host.dts == res.dts and host.steps == res.steps
+        np.testing.assert_array_equal(S.gather_interior(host.slabs), S.gather_interior(res.slabs))
+        part = S.run([torch.as_tensor(init, device=DEV).clone()], [S.slab_params(p, 1, 0)], 0.02, boundary,
+                     S.DistSlabs(), S.CudaStages("sr_f32", _closure("sr_f32")), max_steps=21)
+        part_h = S.run([torch.as_tensor(init, device=DEV).clone()], [S.slab_params(p, 1, 0)], 0.02, boundary,
+                       S.DistSlabs(), S.CudaStages("sr_f32", _closure("sr_f32")), max_steps=21, host_loop=True)
+        assert part.steps == part_h.steps == min(21, res.steps) and part.dts == part_h.dts
+        np.testing.assert_array_equal(S.gather_interior(part.slabs), S.gather_interior(part_h.slabs))
     finally:
         dist.destroy_process_group()
 

@@ -64,6 +64,12 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
                                           C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
                                           vp, sz, vp]
+            L.wsr_euler2d_slab_begin.argtypes = [vp, vp, i, i, d, d, d, d, d, d, i, vp, sz, vp]
+            L.wsr_euler2d_slab_speed_slot.argtypes = [vp, vp, sz, i, i, C.POINTER(vp)]
+            L.wsr_euler2d_slab_step.argtypes = [vp, i, i, i, d, d, vp, sz, vp]
+            L.wsr_euler2d_slab_stage.argtypes = [vp, vp, vp, vp, i, i, d, d, d, i, i, i, i, i, vp, sz, vp]
+            L.wsr_euler2d_slab_status.argtypes = [vp, vp, sz, i, i, C.POINTER(i), C.POINTER(d), C.POINTER(i),
+                                                  C.POINTER(d), vp]
             L.wsr_adv1d_workspace_bytes.argtypes = []
             L.wsr_adv1d_workspace_bytes.restype = sz
             L.wsr_adv1d_run.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, C.POINTER(i), C.POINTER(i),
@@ -95,7 +101,8 @@ def exported_symbols() -> list[str]:
             "wsr_profile_enable", "wsr_profile_read", "wsr_euler2d_counters", "wsr_probe_peak_flops", "wsr_probe_exp_tab",
             "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
             "wsr_train1d_backward", "wsr_euler3d_workspace_bytes", "wsr_euler3d_stage", "wsr_euler3d_max_speed",
-            "wsr_euler3d_run", "wsr_euler3d_counters", "wsr_euler2d_stage_noalloc"]
+            "wsr_euler3d_run", "wsr_euler3d_counters", "wsr_euler2d_stage_noalloc", "wsr_euler2d_slab_begin",
+            "wsr_euler2d_slab_speed_slot", "wsr_euler2d_slab_step", "wsr_euler2d_slab_stage", "wsr_euler2d_slab_status"]
 
 
 def pack_params(params) -> np.ndarray:

@@ -517,6 +517,93 @@ int wsr_profile_read(wsr_ctx* ctx, double* ms, long long* launches) {
   return WSR_OK;
 }
 
+// ---- device-resident time loop of a y-slab (one slab of a decomposed grid per rank) ----
+// The control block of the workspace carries t, dt and the stop flag as in wsr_euler2d_run; between these calls
+// the caller exchanges the halo rows and all-reduces (MAX) the 64-bit wave-speed slot, all on the device.
+int wsr_euler2d_slab_begin(wsr_ctx* ctx, const double* u, int nx, int ny, double dx, double dy, double gamma,
+                           double cfl, double t_start, double t_end, int max_steps, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  int rc = check_2d(ctx, nx, ny, WSR_METHOD_JS, WSR_BC_TRANSMISSIVE, WSR_FLUX_HLLC, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (!u || misaligned(u)) return fail(ctx, WSR_ERR_ARG, "state must be a 16-byte aligned device array");
+  if (max_steps < 1 || !(cfl > 0.0) || !(dx > 0.0) || !(dy > 0.0))
+    return fail(ctx, WSR_ERR_ARG, "max_steps, cfl, dx, dy must be positive");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, t_start, t_end, 0.0, dx, dy, cfl, dx < dy ? dx : dy, 0,
+                              0, max_steps);
+  WSR_LAUNCHED(ctx, "k_init_ctl");
+  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, &w.ctl->max_speed_bits);
+  WSR_LAUNCHED(ctx, "k_max_speed");
+  return WSR_OK;
+}
+
+int wsr_euler2d_slab_speed_slot(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, int nx, int ny,
+                                unsigned long long** slot) {
+  if (!ctx || !workspace || !slot) return WSR_ERR_ARG;
+  if (workspace_bytes < ws_bytes(nx, ny)) return fail(ctx, WSR_ERR_ARG, "workspace too small");
+  *slot = &carve(workspace, nx, ny).ctl->max_speed_bits;
+  return WSR_OK;
+}
+
+int wsr_euler2d_slab_step(wsr_ctx* ctx, int phase, int nx, int ny, double dx, double dy, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+  if (!ctx || !workspace || (phase != 0 && phase != 1)) return WSR_ERR_ARG;
+  if (workspace_bytes < ws_bytes(nx, ny)) return fail(ctx, WSR_ERR_ARG, "workspace too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  if (phase == 0) {
+    k_step_begin_ring<<<1, 1, 0, st>>>(w.ctl, w.dts);
+    k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
+  } else {
+    k_step_end<<<1, 1, 0, st>>>(w.ctl);
+  }
+  WSR_LAUNCHED(ctx, "slab step control");
+  return WSR_OK;
+}
+
+int wsr_euler2d_slab_stage(wsr_ctx* ctx, const double* u_stage, const double* u0, double* u_out, int nx, int ny,
+                           double dx, double dy, double gamma, int rk, int method, int bc, int flux, int opts,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
+  if (rc) return rc;
+  if ((bc & ~WSR_BC_Y_HALO) == WSR_BC_DOUBLE_MACH) return fail(ctx, WSR_ERR_ARG, "slabs take no double-Mach boundary");
+  if (!u_stage || !u0 || !u_out || misaligned(u_stage) || misaligned(u0) || misaligned(u_out))
+    return fail(ctx, WSR_ERR_ARG, "state arrays must be 16-byte aligned device arrays");
+  if (rk < 1 || rk > 3) return fail(ctx, WSR_ERR_ARG, "rk must be 1, 2 or 3 (got %d)", rk);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  FaceMaps fm;
+  if (!face_maps(w, nx, ny, &fm)) return fail(ctx, WSR_ERR_CUDA, "encoding the face-value tensor maps failed");
+  StageArgs a{u_stage, u0, u_out, nx, ny, bc, flux, opts, rk, dx, dy, gamma, rk == 1 ? 0.0 : (rk == 2 ? 1.0 : 0.5)};
+  return dispatch_stage(ctx, method, a, w, fm, st);
+}
+
+int wsr_euler2d_slab_status(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, int nx, int ny, int* steps,
+                            double* t, int* done, double* dts_ring, void* stream) {
+  if (!ctx || !workspace) return WSR_ERR_ARG;
+  if (workspace_bytes < ws_bytes(nx, ny)) return fail(ctx, WSR_ERR_ARG, "workspace too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  Ws2d w = carve(workspace, nx, ny);
+  WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, w.ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+  WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned + 128, w.dts, kDtsRing * sizeof(double), cudaMemcpyDeviceToHost, st));
+  WSR_CUDA(ctx, cudaStreamSynchronize(st));
+  StepCtl snap;
+  std::memcpy(&snap, ctx->host_pinned, sizeof(StepCtl));
+  if (steps) *steps = snap.steps;
+  if (t) *t = snap.t;
+  if (done) *done = snap.done;
+  if (dts_ring) std::memcpy(dts_ring, ctx->host_pinned + 128, kDtsRing * sizeof(double));
+  int fb[2] = {0, 0};
+  WSR_CUDA(ctx, cudaMemcpy(fb, w.fallbacks, sizeof(fb), cudaMemcpyDeviceToHost));
+  if (fb[1]) return fail(ctx, WSR_ERR_CUDA, "a stencil tile load (TMA) did not complete in time");
+  return WSR_OK;
+}
+
 int wsr_euler2d_counters(wsr_ctx* ctx, void* workspace, size_t workspace_bytes, int nx, int ny,
                          unsigned long long* out_host) {
   if (!ctx || !workspace || !out_host) return WSR_ERR_ARG;

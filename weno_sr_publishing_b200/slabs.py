@@ -21,6 +21,7 @@ planes as given (WSR_OPT_Z_HALO). The loop applies the 3D solver's dt and stop r
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 from dataclasses import dataclass, field
 
@@ -195,17 +196,81 @@ class SlabRun:
     t: float = 0.0
 
 
+class _DeviceWord:
+    """One int64 in device memory as a torch tensor (the wave-speed slot of a slab's control block)."""
+
+    def __init__(self, ptr: int):
+        self.__cuda_array_interface__ = {"shape": (1,), "typestr": "<i8", "data": (ptr, False), "version": 3}
+
+
+def _device_loop_applies(slabs, comm, stages) -> bool:
+    return (isinstance(comm, DistSlabs) and isinstance(stages, CudaStages) and len(slabs) == 1
+            and isinstance(slabs[0], torch.Tensor) and slabs[0].is_cuda and comm.dist.get_backend(comm.group) == "nccl")
+
+
+def _run_device(u: torch.Tensor, p, t_end: float, periodic: bool, comm, stages, max_steps: int, t_start: float,
+                batch: int = 16) -> SlabRun:
+    """The device-resident loop of one slab per rank: dt, t and the stop test stay in the slab's control block
+    (wsr_euler2d_slab_*), the halos and the wave speed's MAX all-reduce go over NCCL on the same stream, and the
+    host reads the control block every `batch` steps; no host synchronisation inside a batch."""
+    dev = u.device
+    L = N.lib()
+    ctx = E.prepare_closure(stages.method, stages.mlp_params, dev.index)
+    ws = stages._workspace(u, p)
+    stream = E._stream_ptr(dev.index)
+    bufs = [u] + [torch.empty_like(u) for _ in range(3)]
+    ctx.check(L.wsr_euler2d_slab_begin(ctx.handle, C.c_void_p(u.data_ptr()), p.nx, p.ny, p.dx, p.dy, p.gamma, p.cfl,
+                                       float(t_start), float(t_end), int(max_steps), C.c_void_p(ws.ptr), ws.nbytes,
+                                       stream))
+    slot_ptr = C.c_void_p()
+    ctx.check(L.wsr_euler2d_slab_speed_slot(ctx.handle, C.c_void_p(ws.ptr), ws.nbytes, p.nx, p.ny,
+                                            C.byref(slot_ptr)))
+    slot = torch.as_tensor(_DeviceWord(slot_ptr.value), device=dev)
+    d = comm.dist
+    d.all_reduce(slot, op=d.ReduceOp.MAX, group=comm.group)
+    bc = N.BC["periodic" if periodic else "transmissive"] | N.BC_Y_HALO
+    method, flux = N.METHOD[stages.method], N.FLUX[stages.flux]
+    ring = (C.c_double * 64)()
+    steps, t, done = C.c_int(0), C.c_double(0.0), C.c_int(0)
+    launched, dts = 0, []
+    while launched < max_steps and not done.value:
+        for s in range(launched, min(launched + batch, max_steps)):
+            a, b = (bufs[0], bufs[3]) if s % 2 == 0 else (bufs[3], bufs[0])
+            ctx.check(L.wsr_euler2d_slab_step(ctx.handle, 0, p.nx, p.ny, p.dx, p.dy, C.c_void_p(ws.ptr), ws.nbytes,
+                                              stream))
+            for rk, src, dst in ((1, a, bufs[1]), (2, bufs[1], bufs[2]), (3, bufs[2], b)):
+                comm.exchange([src], periodic)
+                ctx.check(L.wsr_euler2d_slab_stage(ctx.handle, C.c_void_p(src.data_ptr()), C.c_void_p(a.data_ptr()),
+                                                   C.c_void_p(dst.data_ptr()), p.nx, p.ny, p.dx, p.dy, p.gamma, rk,
+                                                   method, bc, flux, int(stages.opts), C.c_void_p(ws.ptr), ws.nbytes,
+                                                   stream))
+            d.all_reduce(slot, op=d.ReduceOp.MAX, group=comm.group)
+            ctx.check(L.wsr_euler2d_slab_step(ctx.handle, 1, p.nx, p.ny, p.dx, p.dy, C.c_void_p(ws.ptr), ws.nbytes,
+                                              stream))
+        launched = min(launched + batch, max_steps)
+        seen = len(dts)
+        ctx.check(L.wsr_euler2d_slab_status(ctx.handle, C.c_void_p(ws.ptr), ws.nbytes, p.nx, p.ny, C.byref(steps),
+                                            C.byref(t), C.byref(done), ring, stream))
+        dts += [float(ring[k % 64]) for k in range(seen, steps.value)]
+    final = bufs[0] if steps.value % 2 == 0 else bufs[3]
+    return SlabRun([final], [p], dts, steps.value, t.value)
+
+
 def run(slabs: list, params: list, t_end: float, boundary: str, comm, stages,
-        max_steps: int = 1 << 20, t_start: float = 0.0) -> SlabRun:
+        max_steps: int = 1 << 20, t_start: float = 0.0, host_loop: bool = False) -> SlabRun:
     """SSPRK3 time loop over the local slabs (`slabs[k]` padded, `params[k]` its SlabParams); `comm` is a
     LocalSlabs (all slabs here) or DistSlabs (one per rank); `stages` computes stages and wave speeds
-    (CudaStages for the GPU). The slabs are advanced out of place; the returned SlabRun holds the final ones."""
+    (CudaStages for the GPU). The slabs are advanced out of place; the returned SlabRun holds the final ones.
+    One CUDA slab per rank over NCCL runs the device-resident loop (no host synchronisation per step) unless
+    host_loop is set; the results are the same bit for bit."""
     if boundary not in ("transmissive", "periodic"):
         raise NotImplementedError(f"the y-slab decomposition supports transmissive and periodic boundaries, not "
                                   f"{boundary!r}")
     if boundary not in N.BC:
         raise ValueError(f"unsupported boundary {boundary!r}")
     periodic = boundary == "periodic"
+    if not host_loop and _device_loop_applies(slabs, comm, stages):
+        return _run_device(slabs[0], params[0], t_end, periodic, comm, stages, max_steps, t_start)
     p0 = params[0]
     hmin = min(p0.dx, p0.dy)
     bufs = [[u] + [stages.empty_like(u) for _ in range(3)] for u in slabs]
