@@ -41,7 +41,9 @@ extern "C" {
 #define WSR_METHOD_SR_F64 1   /* WENO5-SR, FP64 MLP (REFSYM) */
 #define WSR_METHOD_SR_F32 2   /* WENO5-SR, FP32 MLP, FP64 elsewhere (MIXED) */
 #define WSR_METHOD_SR_BF16 3  /* WENO5-SR, BF16 inputs/parameters/activations, FP32 accumulation */
-#define WSR_METHOD_Z 4        /* WENO5-Z (Borges p = 2, eps = h^2 per direction); 2D functions only */
+#define WSR_METHOD_Z 4        /* WENO-Z (Borges et al.): WENO5 p = 2, eps = h^2 of the reconstruction direction (2D,
+                               * 3D, 1D scheme 5); WENO7 p = 3, eps = h^3 (1D scheme 7; the WENO7 2D functions
+                               * document their own) */
 #define WSR_METHOD_SR_BF16_TC 5 /* WENO5-SR with the BF16 closure's MLP on the tensor cores (warp mma.sync, BF16 x BF16
                                  * -> FP32); the same results as WSR_METHOD_SR_BF16 up to the accumulation order. An
                                  * addition without a counterpart in the reference; measured slower than
@@ -162,6 +164,8 @@ int wsr_euler2d_run(wsr_ctx *ctx, double *const u[4], int nx, int ny, double dx,
  * schedule is n_full steps of t/n_full). u is updated in place. order (optional, B entries) is the
  * visiting order of trajectories (longest first balances the launch). nmax >= every n_b, at most 2048.
  * scheme 5: WENO5 (5-point stencils, closure kind 5); scheme 7: WENO7 (7-point stencils, closure kind 7).
+ * method WSR_METHOD_Z gives the WENO-Z baselines of weno_z_borges_p2_results/torch_weno_z.py:14-107 (WENO5-Z:
+ * tau5 = |b0 - b2|, eps = dx[b]^2, p = 2; WENO7-Z: tau7 = |-b0 - 3 b1 + 3 b2 + b3|, eps = dx[b]^3, p = 3).
  * All array arguments are device pointers. fallbacks_out, errors_out and counters_out (2 values: MLP
  * evaluations, plateau stencils when opts has WSR_OPT_COUNT) are host pointers or NULL; when any is
  * given the call synchronises `stream`. */
@@ -198,9 +202,10 @@ int wsr_train1d_backward(wsr_ctx *ctx, const double *velocity, int B, int n, dou
                          int ckpt_every, int method, double *grad_out, double *grad_u0, void *workspace,
                          size_t workspace_bytes, void *stream);
 
-/* ---- 3D Euler, WENO5 (JS / SR) with 2 x 2 Gauss-point transverse quadrature ----
+/* ---- 3D Euler, WENO5 (JS / SR / Z) with 2 x 2 Gauss-point transverse quadrature ----
  * Replaces the reference's 3D Warp port (warp_weno5_3d_rk3/solver.py:165-329 Weno5Rk3Solver: _rk_stage,
- * advance; kernels.py:776-1163). State layout: padded row-major q[nz+6][ny+6][nx+6][5] doubles, conserved
+ * advance; kernels.py:776-1163) and its WENO-Z variant (weno_z_borges_p2_results/weno5_3d_solver_z.py,
+ * weno5_3d_kernels_z.py: method WSR_METHOD_Z, eps = h^2 of each reconstruction's direction). State layout: padded row-major q[nz+6][ny+6][nx+6][5] doubles, conserved
  * (rho, rho u, rho v, rho w, E), ghost width 3, gamma 1.4 (config.py:45-52). Boundaries are transmissive;
  * `inflow` (a HOST array of 5 conserved values, or NULL) instead fixes the x-low ghost cells.
  * flux: WSR_FLUX3_EVILIN (the reference's interface state) or WSR_FLUX3_HLLC (HLLC in 3D, an addition).

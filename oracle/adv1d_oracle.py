@@ -15,12 +15,14 @@ numpy, the reference's PyTorch code (paths inside the reference project, code/sn
                                   plateau, omega (beta = 4 r), classical omega, MLP 6->24->16->16->4
     rk4_advection.py     31-220   7-point stencils, face states, L and L~ (reverse upwind), Shu RK4
   for_paper_results/run_gste.py 103-118 (GSTE schedule: steps = ceil(t/(cfl dx)), dt = t/steps)
+  weno_z_borges_p2_results/torch_weno_z.py 14-79 (WENO5-Z: p 2, eps h^2, tau5 = |b0 - b2|; WENO7-Z: p 3,
+                                  eps h^3, tau7 = |-b0 - 3 b1 + 3 b2 + b3|; velocity +1 in the reference)
 
 Pinned by tests/test_adv1d_oracle.py against fixtures that tests/golden/make_golden_1d.py produced
 by running the reference's own torch functions.
 
 A closure is described by (kind, precision, packed parameters): kind 5 (189 parameters) or 7 (908),
-precision "f64", "f32" or "bf16". JS weights use closure=None.
+precision "f64", "f32" or "bf16". JS weights use closure=None, WENO-Z weights closure="z".
 """
 from __future__ import annotations
 
@@ -170,8 +172,16 @@ def candidates7(q, lr):
 # ------------------------------------------------------------------------------------------------
 # Reconstruction at both physical faces of every cell's stencil
 # ------------------------------------------------------------------------------------------------
-def face_values(u: np.ndarray, scheme: int, closure) -> tuple[np.ndarray, np.ndarray]:
-    """Left and right states at face i+1/2 for every i (lr=1 of cell i, lr=2 of cell i+1)."""
+def beta5(q):
+    q0, q1, q2, q3, q4 = q.T
+    return np.stack([(13 / 12) * (q0 - 2 * q1 + q2) ** 2 + 0.25 * (q0 - 4 * q1 + 3 * q2) ** 2,
+                     (13 / 12) * (q1 - 2 * q2 + q3) ** 2 + 0.25 * (q1 - q3) ** 2,
+                     (13 / 12) * (q2 - 2 * q3 + q4) ** 2 + 0.25 * (3 * q2 - 4 * q3 + q4) ** 2], axis=1)
+
+
+def face_values(u: np.ndarray, scheme: int, closure, h: float | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """Left and right states at face i+1/2 for every i (lr=1 of cell i, lr=2 of cell i+1); h is the cell
+    width (WENO-Z only)."""
     width = 5 if scheme == 5 else 7
     q = stencils(u, width)
     if scheme == 5:
@@ -186,14 +196,22 @@ def face_values(u: np.ndarray, scheme: int, closure) -> tuple[np.ndarray, np.nda
         dtab, bscale, off = D7, 4.0, 16.0
         beta_cls = np.sum(forms * forms * DELTA7_COEFF, axis=-1)
     vals = {}
-    if closure is None:
+    if isinstance(closure, str) and closure == "z":
+        if h is None:
+            raise ValueError("WENO-Z needs the cell width h")
         if scheme == 5:
-            q0, q1, q2, q3, q4 = q.T
-            beta = np.stack([(13 / 12) * (q0 - 2 * q1 + q2) ** 2 + 0.25 * (q0 - 4 * q1 + 3 * q2) ** 2,
-                             (13 / 12) * (q1 - 2 * q2 + q3) ** 2 + 0.25 * (q1 - q3) ** 2,
-                             (13 / 12) * (q2 - 2 * q3 + q4) ** 2 + 0.25 * (3 * q2 - 4 * q3 + q4) ** 2], axis=1)
+            beta = beta5(q)
+            tau, eps, p = np.abs(beta[:, 0] - beta[:, 2]), h ** 2, 2
         else:
             beta = beta_cls
+            tau, eps, p = np.abs(-beta[:, 0] - 3.0 * beta[:, 1] + 3.0 * beta[:, 2] + beta[:, 3]), h ** 3, 3
+        ratio = tau[:, None] / (beta + eps)
+        for lr in (1, 2):
+            a = dtab[lr][None, :] * (1.0 + ratio ** p)
+            w = a / np.sum(a, axis=1, keepdims=True)
+            vals[lr] = np.sum(w * cand[lr], axis=1)
+    elif closure is None:
+        beta = beta5(q) if scheme == 5 else beta_cls
         for lr in (1, 2):
             a = dtab[lr][None, :] / np.square(beta + 1.0e-6)
             w = a / np.sum(a, axis=1, keepdims=True)
@@ -215,7 +233,7 @@ def face_values(u: np.ndarray, scheme: int, closure) -> tuple[np.ndarray, np.nda
 
 
 def rhs(u, a, dx, scheme, closure, reverse=False):
-    left, right = face_values(u, scheme, closure)
+    left, right = face_values(u, scheme, closure, dx)
     face = (right if a > 0 else left) if reverse else (left if a > 0 else right)
     flux = a * face
     return -(flux - np.roll(flux, 1)) * (1.0 / dx)

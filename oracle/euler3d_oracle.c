@@ -1,5 +1,5 @@
 /*
- * CPU oracle for the 3D Euler WENO5 (JS / SR) finite-volume step.
+ * CPU oracle for the 3D Euler WENO5 (JS / SR / Z) finite-volume step.
  *
  * TEST INFRASTRUCTURE ONLY. A plain-C restatement of the reference's 3D Warp port, used by the test
  * suite as the parity checker of the CUDA 3D kernels and by bench.py as the timed CPU baseline. The
@@ -18,6 +18,8 @@
  *   mlp_normal_scalar.py  the characteristic MLP reconstruction, including the lr = 1 round trip
  *   solver.py    165-329 the order of the sweeps, the four (first_lr, second_lr) flags of the 2x2 Gauss
  *                transverse quadrature, the dt rule and the three RK stages
+ *   weno_z_borges_p2_results/weno5_3d_kernels_z.py, weno5_3d_solver_z.py: the same solver with WENO-Z
+ *                weights (eps = h^2 of each reconstruction's own direction)
  *
  * Pinned against the reference itself: tests/golden/make_golden_3d.py runs the reference's Warp solver
  * (through a pure-Python stand-in for warp) on a small grid.
@@ -40,8 +42,9 @@ enum { O3_FLUX_EVILIN = 0, O3_FLUX_HLLC = 1 };
 typedef struct { double v[5]; } v5;
 typedef struct { double m[5][5]; } m55;
 
-/* from euler2d_oracle.c: the 2D/3D scalar closure */
-double or_reconstruct(const double q[5], int head, int method, const double *P64, const float *P32);
+/* from euler2d_oracle.c: the 2D/3D scalar closure; WENO-Z (method 4) takes eps = h^2 of the reconstruction
+ * direction (weno_z_borges_p2_results/weno5_3d_kernels_z.py:527-562, 673-706) */
+double or_reconstruct_h(const double q[5], int head, int method, const double *P64, const float *P32, double h);
 
 static const double GAMMA3 = 1.4;
 
@@ -295,8 +298,10 @@ static void boundary(double *q, const o3_cfg *c) {
         }
 }
 
-static double recon(const double s[5], int head, const o3_cfg *c) {
-    return or_reconstruct(s, head, c->method, c->P64, c->P32);
+static double spacing(const o3_cfg *c, int dir) { return dir == 1 ? c->dx : (dir == 2 ? c->dy : c->dz); }
+
+static double recon(const double s[5], int head, int dir, const o3_cfg *c) {
+    return or_reconstruct_h(s, head, c->method, c->P64, c->P32, spacing(c, dir));
 }
 
 /* Characteristic normal reconstruction of the cell at stencil centre (normal_*_kernel, kernels.py:869-927,
@@ -310,7 +315,7 @@ static void normal_cell(const v5 q[5], int dir, const o3_cfg *c, v5 *left, v5 *r
     v5 cv;
     for (int comp = 0; comp < 5; ++comp) {
         double s[5] = {ch[0].v[comp], ch[1].v[comp], ch[2].v[comp], ch[3].v[comp], ch[4].v[comp]};
-        cv.v[comp] = recon(s, 1, c);
+        cv.v[comp] = recon(s, 1, dir, c);
     }
     *left = matvec(&R, cv);
     for (int p = 0; p < 5; ++p) r[p] = matvec(&R, ch[p]);
@@ -318,16 +323,16 @@ static void normal_cell(const v5 q[5], int dir, const o3_cfg *c, v5 *left, v5 *r
     for (int p = 0; p < 5; ++p) ch[p] = matvec(&L1, r[p]);
     for (int comp = 0; comp < 5; ++comp) {
         double s[5] = {ch[0].v[comp], ch[1].v[comp], ch[2].v[comp], ch[3].v[comp], ch[4].v[comp]};
-        cv.v[comp] = recon(s, 0, c);
+        cv.v[comp] = recon(s, 0, dir, c);
     }
     *right = matvec(&R1, cv);
 }
 
-static v5 gauss_vec(const v5 q[5], int lr, const o3_cfg *c) {
+static v5 gauss_vec(const v5 q[5], int lr, int dir, const o3_cfg *c) {
     v5 out;
     for (int comp = 0; comp < 5; ++comp) {
         double s[5] = {q[0].v[comp], q[1].v[comp], q[2].v[comp], q[3].v[comp], q[4].v[comp]};
-        out.v[comp] = recon(s, lr == 1 ? 2 : 3, c);
+        out.v[comp] = recon(s, lr == 1 ? 2 : 3, dir, c);
     }
     return out;
 }
@@ -374,8 +379,8 @@ static void sweep(const double *q, int dir, double dt_h, const o3_cfg *c, o3_buf
                         sl[p] = ld(b->nl, o);
                         sr[p] = ld(b->nr, o);
                     }
-                    st(b->sl, at(c, k, j, i), gauss_vec(sl, first_lr, c));
-                    st(b->sr, at(c, k, j, i), gauss_vec(sr, first_lr, c));
+                    st(b->sl, at(c, k, j, i), gauss_vec(sl, first_lr, ta, c));
+                    st(b->sr, at(c, k, j, i), gauss_vec(sr, first_lr, ta, c));
                 }
         /* pass b: along tb, over the interior of both transverse directions */
         int kb = dir == 3 ? nz + 2 : nz, jb = dir == 2 ? ny + 2 : ny, ib = dir == 1 ? nx + 2 : nx;
@@ -389,8 +394,8 @@ static void sweep(const double *q, int dir, double dt_h, const o3_cfg *c, o3_buf
                         sl[p] = ld(b->sl, o);
                         sr[p] = ld(b->sr, o);
                     }
-                    st(b->pl, at(c, k, j, i), gauss_vec(sl, second_lr, c));
-                    st(b->pr, at(c, k, j, i), gauss_vec(sr, second_lr, c));
+                    st(b->pl, at(c, k, j, i), gauss_vec(sl, second_lr, tb, c));
+                    st(b->pr, at(c, k, j, i), gauss_vec(sr, second_lr, tb, c));
                 }
         /* face fluxes: face f between normal-index cells f (right state) and f + 1 (left state) */
         int kf = dir == 3 ? nz + 1 : nz, jf = dir == 2 ? ny + 1 : ny, iff = dir == 1 ? nx + 1 : nx;

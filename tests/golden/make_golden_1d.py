@@ -6,7 +6,10 @@
   WENO5-SR (FP64, FP32) and WENO7-JS/SR (the paper's GSTE table), with initial, final and exact
   cell averages and the L1 errors;
 * adv1d_steps.npz: a few seeded trajectories (several N, both velocity signs) advanced by the
-  reference's ssprk3_step_signed / rollout_distance (WENO5) and shu_rk4_step_signed (WENO7).
+  reference's ssprk3_step_signed / rollout_distance (WENO5) and shu_rk4_step_signed (WENO7);
+* adv1d_z.npz: the WENO-Z GSTE rows of weno_z_borges_p2_results/run_gste.py (N=200, t=10, CFL 0.6:
+  WENO5-Z with SSPRK3, WENO7-Z with Shu RK4, through its integrate()), and seeded trajectories advanced a
+  few steps by torch_weno_z.ssprk3_step / shu_rk4_step (velocity +1, the only sign that module has).
 """
 from __future__ import annotations
 
@@ -37,7 +40,7 @@ def seeded_profiles(rng, n):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", type=Path, required=True)
-    ap.add_argument("--only", default="gste,steps")
+    ap.add_argument("--only", default="gste,steps,z")
     args = ap.parse_args()
     only = set(args.only.split(","))
     snap = args.reference / "code" / "snapshot"
@@ -98,6 +101,34 @@ def main() -> None:
                     rec[f"c{case}_w7_{key}_3steps"] = u.numpy()
         np.savez_compressed(HERE / "adv1d_steps.npz", **rec)
         print("adv1d_steps.npz written", flush=True)
+    if "z" in only:
+        zg = importlib.import_module("weno_z_borges_p2_results.run_gste")
+        Z = importlib.import_module("weno_z_borges_p2_results.torch_weno_z")
+        gste = importlib.import_module("for_paper_results.run_gste")
+        Z.self_test()
+        rec = {}
+        x, initial = gste.cell_averages(200, 0.0, 15)
+        _, exact = gste.cell_averages(200, 10.0, 15)
+        rec["initial"], rec["exact"] = initial, exact
+        for key, stepper in (("weno5_z", Z.ssprk3_step), ("weno7_z", Z.shu_rk4_step)):
+            final, steps, dt, _ = zg.integrate(initial, 10.0, 0.6, stepper, "cpu")
+            rec[f"{key}_final"] = final
+            rec[f"{key}_steps"] = steps
+            rec[f"{key}_dt"] = dt
+            rec[f"{key}_l1"] = float(np.mean(np.abs(final - exact)))
+        rng = np.random.default_rng(7919)
+        for case, n in enumerate((37, 64, 100)):
+            u0 = np.stack([seeded_profiles(rng, n) for _ in range(3)])
+            rec[f"c{case}_u0"] = u0
+            dx = 1.0 / n
+            with torch.no_grad():
+                for key, stepper in (("w5", Z.ssprk3_step), ("w7", Z.shu_rk4_step)):
+                    u = torch.tensor(u0)
+                    for _ in range(3):
+                        u = stepper(u, 0.5 * dx, 1.0 / dx)
+                    rec[f"c{case}_{key}_3steps"] = u.numpy()
+        np.savez_compressed(HERE / "adv1d_z.npz", **rec)
+        print("adv1d_z.npz written", {k: v for k, v in rec.items() if k.endswith("_l1")}, flush=True)
 
 
 if __name__ == "__main__":

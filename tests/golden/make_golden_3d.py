@@ -8,7 +8,10 @@ kernels) is imported with warp_shim.py standing in for warp and executed on a 6 
 * ``ic``: the solver's own shock-bubble initialisation (3 x 3 x 3 Gauss cell averages) and one WENO5-JS
   step from it;
 * ``js``, ``sr_f64``, ``sr_f32``: from a seeded smooth-plus-interface state, the first RK stage and one
-  (JS: two) full steps, with the closure of the FP64 / FP32 reference checkpoints for SR.
+  (JS: two) full steps, with the closure of the FP64 / FP32 reference checkpoints for SR;
+* ``z``: the same two JS steps with the WENO-Z solver of code/snapshot/weno_z_borges_p2_results
+  (Weno5ZRk3Solver, weno5_3d_kernels_z.py). That module replaces the base solver's kernel module when it is
+  imported, so ``z`` runs last.
 
 Each case stores the padded state before and after, and the dt of every step (3d_<case>.npz).
 """
@@ -43,7 +46,7 @@ def seeded_state(nx, ny, nz, seed=5):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", type=Path, required=True)
-    ap.add_argument("--only", default="ic,js,sr_f64,sr_f32")
+    ap.add_argument("--only", default="ic,js,sr_f64,sr_f32,z")
     args = ap.parse_args()
     sys.path.insert(0, str(HERE))
     import warp_shim  # noqa: PLC0415
@@ -56,11 +59,19 @@ def main() -> None:
 
     nx, ny, nz = 6, 5, 5
     models = {"sr_f64": MODELS / "weno5_sr_fp64_step012250.npz", "sr_f32": MODELS / "weno5_sr_fp32_step016500.npz"}
-    for case in args.only.split(","):
+    cases = args.only.split(",")
+    cases = [c for c in cases if c != "z"] + (["z"] if "z" in cases else [])
+    for case in cases:
         t0 = time.time()
         cfg = CF.ShockBubbleConfig(nx=nx, ny=ny, nz=nz, t_end=1.0 if case != "ic" else 2.0e-5)
         model = models.get(case)
-        sol = S.Weno5Rk3Solver(cfg, device="cpu", strict_sync=False, model=model)
+        solver_cls = S.Weno5Rk3Solver
+        if case == "z":
+            from weno_z_borges_p2_results import weno5_3d_solver_z as SZ  # noqa: PLC0415
+
+            solver_cls = SZ.Weno5ZRk3Solver
+            K = SZ.K
+        sol = solver_cls(cfg, device="cpu", strict_sync=False, model=model)
         if case == "ic":
             sol.initialize()
         else:
@@ -70,7 +81,7 @@ def main() -> None:
         rec = {"q_init": np.array(sol.q, copy=True), "dx": cfg.dx, "dy": cfg.dy, "dz": cfg.dz, "cfl": cfg.cfl,
                "nx": nx, "ny": ny, "nz": nz}
         # first stage alone, on a copy of the solver state
-        stage = S.Weno5Rk3Solver(cfg, device="cpu", strict_sync=False, model=model)
+        stage = solver_cls(cfg, device="cpu", strict_sync=False, model=model)
         stage.q[...] = sol.q
         stage.primitive[...] = sol.primitive
         m = stage.max_speed()
@@ -79,7 +90,7 @@ def main() -> None:
         stage._rk_stage(1, dt)
         rec["stage1_dt"] = dt
         rec["q_stage1"] = np.array(stage.q, copy=True)
-        steps = 2 if case == "js" else 1
+        steps = 2 if case in ("js", "z") else 1
         dts = []
         for _ in range(steps):
             sol.advance()

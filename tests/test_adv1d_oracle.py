@@ -75,3 +75,35 @@ def test_shard_by_cost_partitions_and_balances():
         np.testing.assert_array_equal(parts[0], A1.shard_by_cost(cost, world, 0))  # deterministic
     with pytest.raises(ValueError):
         A1.shard_by_cost(cost, 2, 2)
+
+
+# WENO-Z rows of the paper's GSTE table (N=200, t=10, CFL 0.6), weno_z_borges_p2_results/README.md
+PUBLISHED_GSTE_Z_L1 = {"weno5_z": 4.198206e-2, "weno7_z": 2.928891e-2}
+
+
+def test_gste_z_fixture_reproduces_published_table():
+    g = np.load(G / "adv1d_z.npz")
+    for key, l1 in PUBLISHED_GSTE_Z_L1.items():
+        assert abs(float(g[f"{key}_l1"]) - l1) <= 5e-9  # the table prints 7 significant digits
+        assert abs(np.mean(np.abs(g[f"{key}_final"] - g["exact"])) - float(g[f"{key}_l1"])) <= 1e-15
+
+
+@pytest.mark.parametrize("case,n", [(0, 37), (1, 64), (2, 100)])
+@pytest.mark.parametrize("scheme,integ,key", [(5, "ssprk3", "w5"), (7, "shu_rk4", "w7")])
+def test_weno_z_matches_reference(case, n, scheme, integ, key):
+    g = np.load(G / "adv1d_z.npz")
+    u0, dx = g[f"c{case}_u0"], 1.0 / n
+    for b in range(u0.shape[0]):
+        out = A.run(u0[b], 1.0, dx, [0.5 * dx] * 3, scheme, "z", integ)
+        ref = g[f"c{case}_{key}_3steps"][b]
+        # the reference sums the three or four alphas with torch.sum and takes h = 1 / (1 / dx)
+        assert np.abs(out - ref).max() <= 1e-14 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("scheme,integ", [(5, "ssprk3"), (7, "shu_rk4")])
+def test_gste_z_oracle_matches_reference_final_state(scheme, integ):
+    g = np.load(G / "adv1d_z.npz")
+    key = f"weno{scheme}_z"
+    steps, dt = int(g[f"{key}_steps"]), float(g[f"{key}_dt"])
+    out = A.run(g["initial"], 1.0, 2.0 / 200, [dt] * steps, scheme, "z", integ)
+    assert np.abs(out - g[f"{key}_final"]).max() <= 1e-11

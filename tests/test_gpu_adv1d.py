@@ -10,6 +10,7 @@ import torch
 from oracle import adv1d_oracle as A
 from oracle.oracle import pack_params
 from weno_sr_publishing_b200 import adv1d as D
+from weno_sr_publishing_b200 import weno_z as Z
 
 pytestmark = pytest.mark.gpu
 
@@ -134,3 +135,38 @@ def test_invalid_batches_raise():
         D.run_batched([np.zeros(3)], [1.0], 0.1, 1, 0.01, scheme=5, device=DEV)
     with pytest.raises(ValueError):
         D.run_batched([np.zeros(10)], [1.0], 0.1, 1, 0.01, scheme=7, model=MODEL5["sr_f64"], device=DEV)
+
+
+@pytest.mark.parametrize("case,n", [(0, 37), (1, 64), (2, 100)])
+@pytest.mark.parametrize("scheme,key", [(5, "w5"), (7, "w7")])
+def test_weno_z_matches_reference_fixture(case, n, scheme, key):
+    """weno_z.ssprk3_step / shu_rk4_step against torch_weno_z's own steppers (3 steps, velocity +1)."""
+    g = np.load(G / "adv1d_z.npz")
+    u = torch.as_tensor(g[f"c{case}_u0"], device=DEV)
+    dx = 1.0 / n
+    step = Z.ssprk3_step if scheme == 5 else Z.shu_rk4_step
+    for _ in range(3):
+        u = step(u, 0.5 * dx, 1.0 / dx)
+    assert _rel(u.cpu().numpy(), g[f"c{case}_{key}_3steps"]) <= TOL["js"]
+
+
+@pytest.mark.parametrize("key,l1", [("weno5_z", 4.198206e-2), ("weno7_z", 2.928891e-2)])
+def test_gste_z_reproduces_published_l1(key, l1):
+    """The WENO-Z GSTE rows (N=200, t=10, CFL 0.6; weno_z_borges_p2_results/README.md), all steps in one launch."""
+    g = np.load(G / "adv1d_z.npz")
+    final, steps, dt, _ = Z.integrate(g["initial"], 10.0, 0.6, Z.ssprk3_step if key == "weno5_z" else Z.shu_rk4_step,
+                                      DEV)
+    assert steps == int(g[f"{key}_steps"]) and dt == float(g[f"{key}_dt"])
+    assert abs(float(np.mean(np.abs(final - g["exact"]))) - l1) <= 5e-9
+    assert np.abs(final - g[f"{key}_final"]).max() <= 1e-9
+
+
+@pytest.mark.parametrize("scheme,integ", [(5, "ssprk3"), (7, "shu_rk4")])
+def test_weno_z_ragged_batch_matches_oracle(scheme, integ):
+    """Ragged rows, both velocity signs and a shortened last step against the oracle's WENO-Z."""
+    states, vel, dx, nf, dtf, dtl = _ragged(5, scheme)
+    outs, _ = D.run_batched(states, vel, dx, nf, dtf, dtl, scheme=scheme, model="z", integrator=integ, device=DEV)
+    for b, u in enumerate(states):
+        dts = [dtf[b]] * nf[b] + ([dtl[b]] if dtl[b] > 0 else [])
+        ref = A.run(u, vel[b], dx[b], dts, scheme, "z", integ)
+        assert _rel(outs[b].cpu().numpy(), ref) <= TOL["js"], b

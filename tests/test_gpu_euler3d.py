@@ -18,10 +18,11 @@ M = Path(__file__).resolve().parents[1] / "weno_sr_publishing_b200" / "models"
 DEV = "cuda:0"
 P64 = {k: v for k, v in np.load(M / "weno5_sr_fp64_step012250.npz").items() if k != "meta_json"}
 P32 = {k: v for k, v in np.load(M / "weno5_sr_fp32_step016500.npz").items() if k != "meta_json"}
-PARAMS = {"js": None, "sr_f64": P64, "sr_f32": P32}
+PARAMS = {"js": None, "sr_f64": P64, "sr_f32": P32, "z": None}
 # relative max-norm tolerances against the reference / the oracle: the JS path is bitwise, the SR closures
-# differ in exp/log/reciprocal rounding (and the FP32 closure forms its features in FP32)
-TOL = {"js": 0.0, "sr_f64": 1e-12, "sr_f32": 2e-6}
+# differ in exp/log/reciprocal rounding (and the FP32 closure forms its features in FP32); WENO-Z is built
+# without contraction and with IEEE divisions like JS, so it is bitwise too
+TOL = {"js": 0.0, "sr_f64": 1e-12, "sr_f32": 2e-6, "z": 0.0}
 INNER = (slice(3, -3),) * 3
 
 
@@ -37,7 +38,8 @@ def _fixture(case):
     return np.load(path)
 
 
-@pytest.mark.parametrize("case,method", [("ic", "js"), ("js", "js"), ("sr_f64", "sr_f64"), ("sr_f32", "sr_f32")])
+@pytest.mark.parametrize("case,method", [("ic", "js"), ("js", "js"), ("sr_f64", "sr_f64"), ("sr_f32", "sr_f32"),
+                                         ("z", "z")])
 def test_matches_reference_solver(case, method):
     g = _fixture(case)
     nx, ny, nz = int(g["nx"]), int(g["ny"]), int(g["nz"])
@@ -69,7 +71,7 @@ def _random_state(nx, ny, nz, seed):
 
 
 @pytest.mark.parametrize("flux", ["evilin", "hllc"])
-@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32"])
+@pytest.mark.parametrize("method", ["js", "sr_f64", "sr_f32", "z"])
 def test_matches_oracle_ragged_grid(method, flux):
     nx, ny, nz = 19, 11, 9
     h = (1.0 / nx, 1.0 / ny, 0.8 / nz)
@@ -175,3 +177,19 @@ def test_js_fallback_when_closure_is_not_finite():
     q_nan = torch.as_tensor(q0, device=DEV).contiguous()
     E3.run(q_nan, nx, ny, nz, dx, dy, dz, 0.4, "sr_f64", "hllc", bad, steps=1)
     assert not bool(torch.isfinite(q_nan[INNER]).all())
+
+
+def test_weno_z_shock_bubble_completes_in_the_published_step_count():
+    """The paper's 3D WENO5-Z row: Ma = 3 shock-bubble, 224 x 88 x 88, CFL 0.25, t = 1e-4, EVILIN, complete in
+    840 steps (weno_z_borges_p2_results/README.md, run_shockbubble_3d.py)."""
+    nx, ny, nz = 224, 88, 88
+    dx, dy, dz = 0.225 / nx, 0.089 / ny, 0.089 / nz
+    q = torch.as_tensor(PR.shockbubble_reference_state(nx, ny, nz), device=DEV).contiguous()
+    res = E3.run(q, nx, ny, nz, dx, dy, dz, 0.25, "z", "evilin", t_end=1.0e-4)
+    assert res.steps == 840
+    assert abs(res.t - 1.0e-4) <= 1e-18
+    inner = q[3:-3, 3:-3, 3:-3].cpu().numpy()
+    assert np.isfinite(inner).all()
+    rho = inner[..., 0]
+    p = 0.4 * (inner[..., 4] - 0.5 * (inner[..., 1] ** 2 + inner[..., 2] ** 2 + inner[..., 3] ** 2) / rho)
+    assert rho.min() > 0.0 and p.min() > 0.0

@@ -24,7 +24,8 @@ def _fixture(case):
 
 
 @pytest.mark.parametrize("case,method,params,tol", [("ic", "js", None, 0.0), ("js", "js", None, 0.0),
-                                                    ("sr_f64", "sr_f64", P64, 1e-14), ("sr_f32", "sr_f32", P32, 1e-8)])
+                                                    ("sr_f64", "sr_f64", P64, 1e-14), ("sr_f32", "sr_f32", P32, 1e-8),
+                                                    ("z", "z", None, 0.0)])
 def test_oracle_reproduces_reference_solver(case, method, params, tol):
     g = _fixture(case)
     nx, ny, nz = int(g["nx"]), int(g["ny"]), int(g["nz"])

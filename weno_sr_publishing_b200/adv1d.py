@@ -10,9 +10,10 @@ Reference-shaped entry points (paths inside the reference project, code/snapshot
   teacherfree_lab_weno7_rk4_distance_balanced_fast/rk4_advection.py:137-220;
 * ``integrate_ssprk3(model, stepper, initial, cfl_limit, t_end, device)`` -- for_paper_results/run_gste.py:103-118.
 
-``model`` is ``"classical"`` (Jiang-Shu weights) or a closure: a :class:`Closure`, a checkpoint path,
-or any object with ``w1 .. b4`` parameters (a reference torch model; float32 parameters select the FP32
-closure). ``state`` is a [B, N] tensor (or array); every row is one periodic trajectory.
+``model`` is ``"classical"`` (Jiang-Shu weights), ``"z"`` (WENO-Z: p = 2, eps = dx^2 for WENO5; p = 3,
+eps = dx^3 for WENO7; weno_z_borges_p2_results/torch_weno_z.py:14-32) or a closure: a :class:`Closure`, a
+checkpoint path, or any object with ``w1 .. b4`` parameters (a reference torch model; float32 parameters select
+the FP32 closure). ``state`` is a [B, N] tensor (or array); every row is one periodic trajectory.
 
 ``run_batched`` takes ragged trajectories (different N, velocity, dx and step schedule per row) in one
 launch: one CTA per trajectory, all steps resident in shared memory.
@@ -74,7 +75,7 @@ class Closure:
 
 def as_closure(model) -> Closure | None:
     if isinstance(model, str):
-        if model != "classical":
+        if model not in ("classical", "z"):
             raise ValueError(f"unknown model {model!r}")
         return None
     if model is None:
@@ -106,7 +107,10 @@ def run_batched(states, velocities, dx, n_full, dt_full, dt_last=None, *, scheme
     if B == 0:
         return [], {}
     closure = as_closure(model)
-    method = "js" if closure is None else closure.method
+    if closure is not None:
+        method = closure.method
+    else:
+        method = "z" if isinstance(model, str) and model == "z" else "js"
     if closure is not None and closure.kind != scheme:
         raise ValueError(f"a WENO{closure.kind} closure cannot drive the WENO{scheme} scheme")
     lens = [int(len(s)) for s in states]

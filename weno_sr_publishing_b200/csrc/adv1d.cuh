@@ -1,11 +1,12 @@
-// Batched 1D periodic linear advection u_t + a u_x = 0 with WENO5 / WENO7 reconstruction (JS or SR
-// closure), SSPRK3 or Shu's fourth-order TVD Runge-Kutta with the downwind operator, sm_100a.
+// Batched 1D periodic linear advection u_t + a u_x = 0 with WENO5 / WENO7 reconstruction (JS, WENO-Z or
+// SR closure), SSPRK3 or Shu's fourth-order TVD Runge-Kutta with the downwind operator, sm_100a.
 //
 // Reference (code/snapshot/): teacherfree_lab_weno5_v20_distance_balanced_mlp_f32_fast/
 // rk3_advection.py:82-186 (signed upwind face state, rhs, SSPRK3, CFL schedule), weno5_core.py:158-239;
 // teacherfree_lab_weno7_rk4_distance_balanced_fast/weno7_core.py:28-324 (WENO7 candidates, weights,
 // delta forms, features, MLP 6->24->16->16->4) and rk4_advection.py:31-220 (face states, L and L~, Shu RK4);
-// for_paper_results/run_gste.py:103-118 (uniform GSTE schedule).
+// for_paper_results/run_gste.py:103-118 (uniform GSTE schedule); weno_z_borges_p2_results/torch_weno_z.py:14-79
+// (WENO5-Z p = 2, eps = h^2, tau5 = |b0 - b2|; WENO7-Z p = 3, eps = h^3, tau7 = |-b0 - 3 b1 + 3 b2 + b3|).
 //
 // One CTA per trajectory keeps the whole trajectory in shared memory for all of its steps: trajectories
 // are independent, so there is no global synchronisation between steps, and ragged lengths and step
@@ -147,6 +148,17 @@ struct Weno<5> {
     b[1] = (13.0 / 12.0) * t1 * t1 + 0.25 * u1 * u1;
     b[2] = (13.0 / 12.0) * t2 * t2 + 0.25 * u2 * u2;
   }
+  // WENO-Z factors g_k = 1 + (tau5 / (b_k + h^2))^2 (torch_weno_z.py:14-20)
+  __device__ static void z_factors(const double q[5], double h, double g[3]) {
+    double b[3];
+    js_beta(q, b);
+    const double tau = fabs(b[0] - b[2]), eps = h * h;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double r = tau / (b[k] + eps);
+      g[k] = 1.0 + r * r;
+    }
+  }
 };
 
 template <>
@@ -180,6 +192,17 @@ struct Weno<7> {
 #pragma unroll
     for (int k = 0; k < 4; ++k)
       b[k] = f[k][0] * f[k][0] * (1.0 / 36.0) + f[k][1] * f[k][1] * (13.0 / 12.0) + f[k][2] * f[k][2] * (781.0 / 720.0);
+  }
+  // WENO-Z factors g_k = 1 + (tau7 / (b_k + h^3))^3 with Castro-Costa-Don's tau7 (torch_weno_z.py:23-32)
+  __device__ static void z_factors(const double q[7], double h, double g[4]) {
+    double b[4];
+    js_beta(q, b);
+    const double tau = fabs(-b[0] - 3.0 * b[1] + 3.0 * b[2] + b[3]), eps = h * h * h;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double r = tau / (b[k] + eps);
+      g[k] = 1.0 + r * r * r;
+    }
   }
   __device__ static void lin(int lr, double d[4]) {
     if (lr == 1) {
@@ -275,6 +298,24 @@ __device__ __forceinline__ void adv_ratios(const double f[Weno<SCHEME>::NF], con
   }
 }
 
+// Weighted value with WENO-Z weights: w = alpha / sum, alpha_k = d_k * g_k.
+template <int SCHEME>
+__device__ __forceinline__ double weighted_z(const double q[Weno<SCHEME>::W], int lr, const double* g) {
+  using S = Weno<SCHEME>;
+  double d[S::R], s[S::R], a[S::R], sum = 0.0;
+  S::lin(lr, d);
+  S::cand(q, lr, s);
+#pragma unroll
+  for (int k = 0; k < S::R; ++k) {
+    a[k] = d[k] * g[k];
+    sum += a[k];
+  }
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k < S::R; ++k) v += (a[k] / sum) * s[k];
+  return v;
+}
+
 // Weighted value: w = alpha / sum, alpha_k = d_k * rk^2, with rk the reciprocal of (beta_k + eps).
 template <int SCHEME>
 __device__ __forceinline__ double weighted(const double q[Weno<SCHEME>::W], int lr, const double* rk, bool linear) {
@@ -315,6 +356,7 @@ __device__ __forceinline__ void adv_faces(const double* __restrict__ v, const Ad
                                           const typename AdvParams<SCHEME, M>::type& P, int opts, Tally& tally) {
   using S = Weno<SCHEME>;
   constexpr int W = S::W, H = W / 2, R = S::R;
+  constexpr bool kClosure = M != M_JS && M != M_Z;
   const int lr_up = T.a > 0.0 ? 1 : 2;
   auto stencil = [&](int i, double s[W]) {
 #pragma unroll
@@ -345,6 +387,15 @@ __device__ __forceinline__ void adv_faces(const double* __restrict__ v, const Ad
         } else {
           fl[i] = weighted<SCHEME>(s, lr_up, rk, false);
         }
+      } else if constexpr (M == M_Z) {
+        double g[R];
+        S::z_factors(s, T.dx, g);
+        if (BOTH) {
+          fl[i] = weighted_z<SCHEME>(s, 1, g);
+          fr[i] = weighted_z<SCHEME>(s, 2, g);
+        } else {
+          fl[i] = weighted_z<SCHEME>(s, lr_up, g);
+        }
       } else {
         double d[R], dmax, qs;
         need = !adv_plateau<SCHEME>(s, d, dmax, qs);
@@ -359,7 +410,7 @@ __device__ __forceinline__ void adv_faces(const double* __restrict__ v, const Ad
         ++(need ? tally.mlp : tally.plateau);
       }
     }
-    if constexpr (M != M_JS) {
+    if constexpr (kClosure) {
       const unsigned m = __ballot_sync(0xffffffffu, need);
       if (m) {
         const int lane = threadIdx.x & 31;
@@ -370,7 +421,7 @@ __device__ __forceinline__ void adv_faces(const double* __restrict__ v, const Ad
       }
     }
   }
-  if constexpr (M != M_JS) {
+  if constexpr (kClosure) {
     __syncthreads();
     const int count = *qcount;
     for (int e = threadIdx.x; e < count; e += kAdvThreads) {

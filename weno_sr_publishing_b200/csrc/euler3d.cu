@@ -307,6 +307,27 @@ __device__ __forceinline__ double js3(const double q[5], int head) {
   return (a0 / s) * c[0] + (a1 / s) * c[1] + (a2 / s) * c[2];
 }
 
+// WENO-Z (Borges et al. 2008, p = 2) with eps = h^2 of the reconstruction direction and IEEE divisions
+// (weno_z_borges_p2_results/weno5_3d_kernels_z.py:527-562, 673-706): tau5 = |beta0 - beta2|,
+// alpha_k = d_k (1 + (tau5 / (beta_k + eps))^2), w_k = alpha_k / sum. Same betas, linear weights and
+// candidates as js3, so the two differ only in the alphas.
+__device__ __forceinline__ double z3(const double q[5], int head, double eps) {
+  const Lin3 d = linear_weights(head);
+  const double t0 = q[0] - 2.0 * q[1] + q[2], u0 = q[0] - 4.0 * q[1] + 3.0 * q[2];
+  const double t1 = q[1] - 2.0 * q[2] + q[3], u1 = q[1] - q[3];
+  const double t2 = q[2] - 2.0 * q[3] + q[4], u2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
+  const double b0 = (13.0 / 12.0) * t0 * t0 + 0.25 * u0 * u0;
+  const double b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * u1 * u1;
+  const double b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * u2 * u2;
+  const double tau = fabs(b0 - b2);
+  const double r0 = tau / (b0 + eps), r1 = tau / (b1 + eps), r2 = tau / (b2 + eps);
+  const double a0 = d.d0 * (1.0 + r0 * r0), a1 = d.d1 * (1.0 + r1 * r1), a2 = d.d2 * (1.0 + r2 * r2);
+  const double s = a0 + a1 + a2;
+  double c[3];
+  candidates(q, head, c);
+  return (a0 / s) * c[0] + (a1 / s) * c[1] + (a2 / s) * c[2];
+}
+
 // rho > 0 and p > 0 of a conserved 3D state
 __device__ __forceinline__ bool admissible5(const V5& q) {
   const double rho = q.v[0];
@@ -320,6 +341,8 @@ __device__ __forceinline__ double recon(const double q[5], int head, const typen
                                         int opts, Tally& tally) {
   if constexpr (M == M_JS) {
     return js3(q, head);
+  } else if constexpr (M == M_Z) {
+    return z3(q, head, P.ex);  // P.ex = h^2 of this kernel's reconstruction direction
   } else {
     if (is_plateau(sensors5(q))) {
       ++tally.plateau;
@@ -461,7 +484,7 @@ __global__ void __launch_bounds__(kT3) k3_normal(const double* __restrict__ q, d
       cv.v[c] = recon<M>(st, side == 0 ? 1 : 0, P, opts, tally);
     }
     V5 face = E.right(cv);
-    if constexpr (M != M_JS) {
+    if constexpr (M != M_JS && M != M_Z) {
       if ((opts & OPT_JS_FALLBACK) && !admissible5(face)) {
         // positivity fallback: the five characteristic values of this face again with WENO5-JS weights
 #pragma unroll 1
@@ -654,26 +677,44 @@ struct Run3 {
 
 dim3 grid3(int ni, int nj, int nk) { return dim3((ni + kT3 - 1) / kT3, nj, nk); }
 
+// Spacing of direction D (1 x, 2 y, 3 z).
+template <int D>
+double spacing_of(const Run3& r) {
+  return D == 1 ? r.dx : (D == 2 ? r.dy : r.dz);
+}
+
+// Kernel parameters of method M for a reconstruction along direction D: the closure for SR, the WENO-Z
+// epsilon h_D^2 for Z (the product the reference forms in each kernel, weno5_3d_kernels_z.py:550).
+template <int M, int D>
+typename ClosureParams<M>::type kparams(const wsr_ctx* ctx, const Run3& r) {
+  if constexpr (M == M_Z) {
+    const double h = spacing_of<D>(r);
+    return ZEps{h * h, h * h};
+  } else {
+    return params_of<M>(ctx);
+  }
+}
+
 template <int M, int DIR, int FLUX>
 int sweep3(wsr_ctx* ctx, const Run3& r, const Ws3& w, double h, cudaStream_t st) {
-  const auto& P = params_of<M>(ctx);
   const Dims3& d = r.d;
   const int nx = d.nx, ny = d.ny, nz = d.nz, px = d.px, py = d.py, pz = d.pz;
   constexpr int TA = DIR == 1 ? 2 : (DIR == 2 ? 1 : 2);
   constexpr int TB = DIR == 3 ? 1 : 3;
   const int kn = DIR == 3 ? nz + 2 : pz, jn = DIR == 2 ? ny + 2 : py, in = DIR == 1 ? nx + 2 : px;
-  k3_normal<M, DIR><<<grid3(in, jn, kn), kT3, 0, st>>>(r.q, w.nl, w.nr, d, in, r.opts, w.ctl, w.counters, P);
+  k3_normal<M, DIR><<<grid3(in, jn, kn), kT3, 0, st>>>(r.q, w.nl, w.nr, d, in, r.opts, w.ctl, w.counters,
+                                                       kparams<M, DIR>(ctx, r));
   WSR_LAUNCHED(ctx, "k3_normal");
   const int ka = TA == 3 ? nz : (DIR == 3 ? nz + 2 : pz);
   const int ja = TA == 2 ? ny : (DIR == 2 ? ny + 2 : py);
   const int ia = TA == 1 ? nx : (DIR == 1 ? nx + 2 : px);
   k3_trans<M, TA><<<grid3(ia, ja, ka), kT3, 0, st>>>(w.nl, w.nr, w.al1, w.al2, w.ar1, w.ar2, d, ia, r.opts, w.ctl,
-                                                      w.counters, P);
+                                                      w.counters, kparams<M, TA>(ctx, r));
   WSR_LAUNCHED(ctx, "k3_trans");
   const int kf = DIR == 3 ? nz + 1 : nz, jf = DIR == 2 ? ny + 1 : ny, iff = DIR == 1 ? nx + 1 : nx;
   double* out = DIR == 1 ? w.fx : (DIR == 2 ? w.fy : w.fz);
   k3_flux<M, DIR, TB, FLUX><<<grid3(iff, jf, kf), kT3, 0, st>>>(w.al1, w.al2, w.ar1, w.ar2, out, d, kf, jf, iff, h,
-                                                                r.opts, w.ctl, w.counters, P);
+                                                                r.opts, w.ctl, w.counters, kparams<M, TB>(ctx, r));
   WSR_LAUNCHED(ctx, "k3_flux");
   return WSR_OK;
 }
@@ -713,6 +754,8 @@ namespace {
 int stage_dispatch(wsr_ctx* ctx, int method, const Run3& r, const Ws3& w, int stage, cudaStream_t st) {
   if (method == WSR_METHOD_JS)
     return r.flux == 1 ? stage3<M_JS, 1>(ctx, r, w, stage, st) : stage3<M_JS, 0>(ctx, r, w, stage, st);
+  if (method == WSR_METHOD_Z)
+    return r.flux == 1 ? stage3<M_Z, 1>(ctx, r, w, stage, st) : stage3<M_Z, 0>(ctx, r, w, stage, st);
   return euler3d_sr_stage(ctx, method, r.q, r.d.nx, r.d.ny, r.d.nz, r.dx, r.dy, r.dz, r.flux, r.opts,
                           r.in.on ? r.in.v : nullptr, w.ctl, stage, st);
 }
@@ -738,9 +781,9 @@ int check3(wsr_ctx* ctx, const double* q, int nx, int ny, int nz, double dx, dou
   if (nx < 5 || ny < 5 || nz < 5) return fail(ctx, WSR_ERR_ARG, "nx, ny, nz must be >= 5 (got %d, %d, %d)", nx, ny, nz);
   if ((size_t)(nx + 6) * (ny + 6) > 65535u * kT3 || nz + 6 > 65535 || ny + 6 > 65535)
     return fail(ctx, WSR_ERR_ARG, "grid %d x %d x %d too large for one launch", nx, ny, nz);
-  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
   if (flux != WSR_FLUX3_EVILIN && flux != WSR_FLUX3_HLLC) return fail(ctx, WSR_ERR_ARG, "bad 3D flux %d", flux);
-  if (method != WSR_METHOD_JS && !ctx->have_closure)
+  if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && !ctx->have_closure)
     return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before wsr_closure_upload");
   if (!q) return fail(ctx, WSR_ERR_ARG, "null state");
   if (misaligned(q)) return fail(ctx, WSR_ERR_ARG, "state must be 16-byte aligned");

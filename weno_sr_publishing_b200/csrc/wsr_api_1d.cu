@@ -32,6 +32,16 @@ const NoParams& adv_params_of<7, M_JS>(const wsr_ctx*) {
   return np;
 }
 template <>
+const ZEps& adv_params_of<5, M_Z>(const wsr_ctx*) {
+  static const ZEps unused{};  // WENO-Z takes eps from each trajectory's dx
+  return unused;
+}
+template <>
+const ZEps& adv_params_of<7, M_Z>(const wsr_ctx*) {
+  static const ZEps unused{};
+  return unused;
+}
+template <>
 const Mlp5d& adv_params_of<5, M_SR64>(const wsr_ctx* c) { return c->p64; }
 template <>
 const Mlp5f& adv_params_of<5, M_SR32>(const wsr_ctx* c) { return c->p32; }
@@ -72,6 +82,8 @@ int adv_dispatch_m(wsr_ctx* ctx, int method, const AdvArgs& a, cudaStream_t st) 
   switch (method) {
     case WSR_METHOD_JS:
       return adv_launch<SCHEME, M_JS, INTEG>(ctx, a, st);
+    case WSR_METHOD_Z:
+      return adv_launch<SCHEME, M_Z, INTEG>(ctx, a, st);
     case WSR_METHOD_SR_F64:
       return adv_launch<SCHEME, M_SR64, INTEG>(ctx, a, st);
     case WSR_METHOD_SR_F32:
@@ -95,10 +107,10 @@ extern "C" int wsr_adv1d_run(wsr_ctx* ctx, double* u, const long long* offsets, 
   if (scheme != 5 && scheme != 7) return fail(ctx, WSR_ERR_ARG, "scheme must be 5 or 7 (got %d)", scheme);
   if (integrator != WSR_INTEG_SSPRK3 && integrator != WSR_INTEG_SHU_RK4)
     return fail(ctx, WSR_ERR_ARG, "bad integrator %d", integrator);
-  if (method < WSR_METHOD_JS || method > WSR_METHOD_SR_BF16) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
+  if (method < WSR_METHOD_JS || method > WSR_METHOD_Z) return fail(ctx, WSR_ERR_ARG, "bad method %d", method);
   if (nmax < (scheme == 5 ? 5 : 7) || nmax > kAdvNmax)
     return fail(ctx, WSR_ERR_ARG, "nmax must be in [%d, %d] (got %d)", scheme == 5 ? 5 : 7, kAdvNmax, nmax);
-  if (method != WSR_METHOD_JS && !(scheme == 5 ? ctx->have_closure : ctx->have_closure7))
+  if (method != WSR_METHOD_JS && method != WSR_METHOD_Z && !(scheme == 5 ? ctx->have_closure : ctx->have_closure7))
     return fail(ctx, WSR_ERR_NO_CLOSURE, "SR method requested before uploading a WENO%d closure", scheme);
   if (!u || !offsets || !velocity || !dx || !n_full || !dt_full || !dt_last)
     return fail(ctx, WSR_ERR_ARG, "null array argument");

@@ -3,7 +3,8 @@
 Reference (code/snapshot/warp_weno5_3d_rk3/): ``Weno5Rk3Solver`` (solver.py:22-329) -- ``_rk_stage``,
 ``advance`` and the run loop of ``run_solver`` -- and its configuration (config.py). The state is the
 reference's padded array q[nz+6, ny+6, nx+6, 5] of FP64 conserved variables (rho, rho u, rho v, rho w, E),
-gamma 1.4, ghost width 3. ``method`` is "js", "sr_f64", "sr_f32" or "sr_bf16"; ``flux`` "evilin" (the
+gamma 1.4, ghost width 3. ``method`` is "js", "z" (WENO-Z, weno_z_borges_p2_results/weno5_3d_solver_z.py),
+"sr_f64", "sr_f32" or "sr_bf16"; ``flux`` "evilin" (the
 reference's) or "hllc"; ``inflow`` (5 conserved values) fixes the x-low ghost cells.
 """
 from __future__ import annotations
