@@ -419,6 +419,7 @@ def main():
         for _ in range(max(W, 1)):
             E.advance_host(host, p, 1, args.method, "transmissive", mlp_params=mlp, bufs=bufs, ws=ws, device=dev,
                            async_readback=True)
+        E.host_wait(dev)  # the warm-up calls' read-backs are done and their steps counted out
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -433,11 +434,16 @@ def main():
             t = torch.tensor([ms_e2e], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms_e2e = float(t.item())
-        nbytes = int(np.prod(p.padded_shape)) * 8
+        host_status = E.host_wait(dev)  # after the timed region: every timed call took its step
+        if host_status["steps"] != K:
+            raise RuntimeError(f"advance_host took {host_status['steps']} steps in {K} calls")
+        nbytes = n * n * 4 * 8  # the interior rows go in and come back; ghost cells are not copied
         line["e2e"] = {"value": world * n * n * K / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                        "d2h_bytes_per_step": nbytes,
-                       "api": "weno_sr_publishing_b200.euler2d.advance_host (pinned host buffer, 1 step per call, "
-                              "async_readback=True; the last read-back completes inside the timed region)"}
+                       "api": "weno_sr_publishing_b200.euler2d.advance_host -> wsr_euler2d_advance_host (pinned host "
+                              "buffer, 1 step per call, async_readback=True: uploads and read-backs in row bands "
+                              "overlapped with the first and last stages; the last read-back completes inside the "
+                              "timed region)"}
         if rank == 0 and world == 1:
             line["cpu_baseline"] = cpu_sample(args.method, mlp, args.t0, args.cpu_seconds)
         if rank == 0:

@@ -21,6 +21,7 @@ SR_METHODS = ("sr_f64", "sr_f32", "sr_bf16", "sr_bf16_tc")
 BC = {"transmissive": 0, "periodic": 1, "double-mach": 2}
 BC_Y_HALO = 16  # flag: y ghost rows read as stored (slabs of a y-decomposed grid)
 FLUX = {"hllc": 0, "force": 1}
+HOST_ASYNC = 1  # wsr_euler2d_advance_host: return once queued
 FLUX3 = {"evilin": 0, "hllc": 1}
 OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT, OPT_Z_HALO = 1, 2, 4, 8
 PROF_KINDS = ("normal_x", "normal_y", "flux_x", "flux_y", "update", "control")
@@ -64,6 +65,10 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_run.argtypes = [vp, C.POINTER(vp), i, i, d, d, d, d, d, d, i, i, i, i, i, i, i, i,
                                           C.POINTER(d), C.POINTER(i), C.POINTER(d), C.POINTER(i), C.POINTER(i),
                                           vp, sz, vp]
+            L.wsr_euler2d_advance_host.argtypes = [vp, vp, C.POINTER(vp), i, i, d, d, d, d, i, i, i, i, i, i, i, vp,
+                                                   sz, vp]
+            L.wsr_euler2d_host_order.argtypes = [vp, vp]
+            L.wsr_euler2d_host_wait.argtypes = [vp, C.POINTER(i), C.POINTER(i)]
             L.wsr_euler2d_slab_begin.argtypes = [vp, vp, i, i, d, d, d, d, d, d, i, vp, sz, vp]
             L.wsr_euler2d_slab_speed_slot.argtypes = [vp, vp, sz, i, i, C.POINTER(vp)]
             L.wsr_euler2d_slab_step.argtypes = [vp, i, i, i, d, d, vp, sz, vp]
@@ -102,7 +107,8 @@ def exported_symbols() -> list[str]:
             "wsr_adv1d_workspace_bytes", "wsr_adv1d_run", "wsr_train1d_workspace_bytes", "wsr_train1d_forward",
             "wsr_train1d_backward", "wsr_euler3d_workspace_bytes", "wsr_euler3d_stage", "wsr_euler3d_max_speed",
             "wsr_euler3d_run", "wsr_euler3d_counters", "wsr_euler2d_stage_noalloc", "wsr_euler2d_slab_begin",
-            "wsr_euler2d_slab_speed_slot", "wsr_euler2d_slab_step", "wsr_euler2d_slab_stage", "wsr_euler2d_slab_status"]
+            "wsr_euler2d_slab_speed_slot", "wsr_euler2d_slab_step", "wsr_euler2d_slab_stage", "wsr_euler2d_slab_status",
+            "wsr_euler2d_advance_host", "wsr_euler2d_host_order", "wsr_euler2d_host_wait"]
 
 
 def pack_params(params) -> np.ndarray:

@@ -151,11 +151,12 @@ constexpr int min_blocks() { return M == M_SR64 ? WSR_SR64_MIN_BLOCKS : WSR_MIN_
 
 // Thread tiling of a 128-thread block: kernels whose stencils run along y use 32 x 4 tiles so that the
 // rows a block reads are shared in L1; kernels whose stencils run along x use 128 x 1.
+// yb0 is the first block row of the launch (a launch may cover a band of the rows).
 template <bool TALL>
 struct Tile {
   static constexpr int bx = TALL ? 32 : kBlock, by = TALL ? 4 : 1;
   __device__ static int x(int t) { return blockIdx.x * bx + (TALL ? (t & 31) : t); }
-  __device__ static int y(int t) { return blockIdx.y * by + (TALL ? (t >> 5) : 0); }
+  __device__ static int y(int t, int yb0) { return ((int)blockIdx.y + yb0) * by + (TALL ? (t >> 5) : 0); }
 };
 
 // Pushes the stencils of this warp that need the closure onto the block queue (warp-aggregated).
@@ -190,7 +191,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
                                                       const StepCtl* __restrict__ ctl, int opts,
                                                       int* __restrict__ fallbacks,
                                                       unsigned long long* __restrict__ counters,
-                                                      const __grid_constant__ typename ClosureParams<M>::type P) {
+                                                      const __grid_constant__ typename ClosureParams<M>::type P,
+                                                      int yb0) {
   __shared__ double s_ch[4][6][kBlock];                  // characteristic values, [field][cell][thread]
   __shared__ double s_val[kStencilsPerThread][kBlock];   // reconstructed characteristic face values
   __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
   using TL = Tile<DIR == 2>;
   const int t = threadIdx.x;
   const int c = TL::x(t);
-  const int r = TL::y(t);
+  const int r = TL::y(t, yb0);
   const int nxt = nx + 2 * kGhost;
   const bool active = DIR == 1 ? (r >= 1 && r < ny + 5 && c <= nx) : (r <= ny && c >= 1 && c < nx + 5);
   if (t == 0) s_count = 0;
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
                                                     unsigned long long* __restrict__ counters,
                                                     const __grid_constant__ typename ClosureParams<M>::type P,
                                                     const __grid_constant__ CUtensorMap map_l,
-                                                    const __grid_constant__ CUtensorMap map_r) {
+                                                    const __grid_constant__ CUtensorMap map_r, int yb0) {
   __shared__ double s_g[2][kStencilsPerThread][kBlock];  // values at Gauss points 1 and 2
   __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
   __shared__ __align__(128) double s_tile[4 * FluxTile<DIR>::stride];
@@ -450,8 +452,8 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
   using TL = Tile<DIR == 1>;
   const int t = threadIdx.x;
   const int i = TL::x(t);
-  const int j = TL::y(t);
-  const int i0 = blockIdx.x * TL::bx, j0 = blockIdx.y * TL::by;
+  const int j = TL::y(t, yb0);
+  const int i0 = blockIdx.x * TL::bx, j0 = ((int)blockIdx.y + yb0) * TL::by;
   const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
   const bool active = i < nfx && j < nfy;
   const double dt_h = DIR == 1 ? ctl->dt_dx : ctl->dt_dy;
@@ -514,7 +516,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
           const int id = s_q[e];
           n = id / kBlock;
           o = id % kBlock;
-          tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o), i0, j0, n, true, s);
+          tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o, yb0), i0, j0, n, true, s);
           sr_features32<M>(s, sensors5(s), x);
         }
         double a0, a1, a2;
@@ -533,7 +535,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       const int id = s_q[e];
       const int n = id / kBlock, o = id % kBlock;
       double s[5];
-      tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o), i0, j0, n, true, s);
+      tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o, yb0), i0, j0, n, true, s);
       double a0, a1, a2;
       sr_betas<M>(s, P, a0, a1, a2);
       s_g[0][n][o] = sr_value<M>(s, 2, a0, a1, a2, opts, tally);
@@ -597,9 +599,9 @@ __device__ __forceinline__ void block_max_to(unsigned long long v, unsigned long
 static __global__ void __launch_bounds__(256) k_update(const double* __restrict__ u_stage, const double* __restrict__ u0,
                                                 double* __restrict__ u_out, const double* __restrict__ fx,
                                                 const double* __restrict__ fy, int nx, int ny, int rk, double g,
-                                                StepCtl* __restrict__ ctl) {
+                                                StepCtl* __restrict__ ctl, int yb0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
+  const int j = blockIdx.y + yb0;
   if (ctl->done) return;
   const bool active = i < nx && j < ny;
   const int nxt = nx + 2 * kGhost;
@@ -637,9 +639,9 @@ static __global__ void __launch_bounds__(256) k_update(const double* __restrict_
 }
 
 static __global__ void __launch_bounds__(256) k_max_speed(const double* __restrict__ u, int nx, int ny, double g,
-                                                   unsigned long long* __restrict__ out) {
+                                                   unsigned long long* __restrict__ out, int yb0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y;
+  const int j = blockIdx.y + yb0;
   unsigned long long sb = 0;
   if (i < nx && j < ny) sb = speed_bits(load_cell(u, nx + 2 * kGhost, j + kGhost, i + kGhost), g);
   block_max_to(sb, out);

@@ -3,6 +3,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -188,34 +189,34 @@ int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps
     ProfScope ps(ctx, st, 0);
     dim3 grd((a.nx + 1 + 127) / 128, a.ny + 5);
     k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks,
-                                        w.counters + 0, P);
+                                        w.counters + 0, P, 0);
   }
   WSR_LAUNCHED(ctx, "k_normal<x>");
   {
     ProfScope ps(ctx, st, 1);
     dim3 grd((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4);
     k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks,
-                                        w.counters + 2, P);
+                                        w.counters + 2, P, 0);
   }
   WSR_LAUNCHED(ctx, "k_normal<y>");
   {
     ProfScope ps(ctx, st, 2);
     dim3 grd((a.nx + 1 + 31) / 32, (a.ny + 3) / 4);
     k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
-                                      w.counters + 4, P, fm.xl, fm.xr);
+                                      w.counters + 4, P, fm.xl, fm.xr, 0);
   }
   WSR_LAUNCHED(ctx, "k_flux<x>");
   {
     ProfScope ps(ctx, st, 3);
     dim3 grd((a.nx + 127) / 128, a.ny + 1);
     k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
-                                      w.counters + 6, P, fm.yl, fm.yr);
+                                      w.counters + 6, P, fm.yl, fm.yr, 0);
   }
   WSR_LAUNCHED(ctx, "k_flux<y>");
   {
     ProfScope ps(ctx, st, 4);
     dim3 grd((a.nx + 255) / 256, a.ny);
-    k_update<<<grd, 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk, a.g, w.ctl);
+    k_update<<<grd, 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk, a.g, w.ctl, 0);
   }
   WSR_LAUNCHED(ctx, "k_update");
   return WSR_OK;
@@ -236,6 +237,115 @@ int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, 
     default:
       return launch_stage<M_SRBF16>(ctx, a, w, fm, st);
   }
+}
+
+// ---- a stage in row bands ----------------------------------------------------------------------------------
+// Block rows of a stage's five launches, each in its kernel's own unit: normal x (1 padded row), normal y (4 face
+// rows), flux x (4 face rows), flux y (1 face row), update (1 interior row). A stage can be issued in pieces:
+// every launch covers the block rows from what was issued before up to a target, so no row is computed twice.
+struct Rows5 {
+  int nx, ny, fx, fy, up;
+};
+
+inline Rows5 rows_total(int ny) { return Rows5{ny + 5, (ny + 4) / 4, (ny + 3) / 4, ny + 1, ny}; }
+
+// What update rows [0, U) need from the other four launches when the whole stage input is present: flux x face
+// rows < U, flux y face rows <= U, the normal y face rows that flux y reads, and normal x rows up to 5 past the
+// last flux x face row (its transverse stencils).
+inline Rows5 rows_for_update(int ny, int U) {
+  const Rows5 T = rows_total(ny);
+  Rows5 r;
+  r.up = U;
+  r.fx = std::min(T.fx, (U + 3) / 4);
+  r.fy = std::min(T.fy, U + 1);
+  r.ny = std::min(T.ny, (r.fy + 3) / 4);
+  r.nx = std::min(T.nx, 4 * r.fx + 5);
+  return r;
+}
+
+// What the first A interior rows of a stage input allow of the two normal reconstructions under the transmissive
+// boundary (ghost row p reads interior row clamp(p - 3, 0, ny - 1)): normal x row r reads padded row r, so
+// r < A + 3; normal y face row r reads padded rows r .. r + 5, so a block of 4 needs its last row r + 2 < A.
+inline Rows5 normals_for_rows(int ny, int A, Rows5 done) {
+  const Rows5 T = rows_total(ny);
+  Rows5 r = done;
+  if (A >= ny) {
+    r.nx = T.nx;
+    r.ny = T.ny;
+  } else {
+    r.nx = std::max(done.nx, std::min(T.nx, A + 3));
+    r.ny = std::max(done.ny, std::min(T.ny, A >= 2 ? (A - 2) / 4 : 0));
+  }
+  return r;
+}
+
+template <int M>
+int launch_rows(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st, Rows5& done,
+                const Rows5& want) {
+  const auto P = stage_params<M>(ctx, a);
+  const dim3 blk(128);
+  if (want.nx > done.nx) {
+    k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, want.nx - done.nx), blk, 0, st>>>(
+        a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P,
+        done.nx);
+    WSR_LAUNCHED(ctx, "k_normal<x>");
+    done.nx = want.nx;
+  }
+  if (want.ny > done.ny) {
+    k_normal<M, 2><<<dim3((a.nx + 5 + 31) / 32, want.ny - done.ny), blk, 0, st>>>(
+        a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P,
+        done.ny);
+    WSR_LAUNCHED(ctx, "k_normal<y>");
+    done.ny = want.ny;
+  }
+  if (want.fx > done.fx) {
+    k_flux<M, 1><<<dim3((a.nx + 1 + 31) / 32, want.fx - done.fx), blk, 0, st>>>(
+        w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P, fm.xl,
+        fm.xr, done.fx);
+    WSR_LAUNCHED(ctx, "k_flux<x>");
+    done.fx = want.fx;
+  }
+  if (want.fy > done.fy) {
+    k_flux<M, 2><<<dim3((a.nx + 127) / 128, want.fy - done.fy), blk, 0, st>>>(
+        w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P, fm.yl,
+        fm.yr, done.fy);
+    WSR_LAUNCHED(ctx, "k_flux<y>");
+    done.fy = want.fy;
+  }
+  if (want.up > done.up) {
+    k_update<<<dim3((a.nx + 255) / 256, want.up - done.up), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx,
+                                                                          a.ny, a.rk, a.g, w.ctl, done.up);
+    WSR_LAUNCHED(ctx, "k_update");
+    done.up = want.up;
+  }
+  return WSR_OK;
+}
+
+int dispatch_rows(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st,
+                  Rows5& done, const Rows5& want) {
+  switch (method) {
+    case WSR_METHOD_JS:
+      return launch_rows<M_JS>(ctx, a, w, fm, st, done, want);
+    case WSR_METHOD_SR_F64:
+      return launch_rows<M_SR64>(ctx, a, w, fm, st, done, want);
+    case WSR_METHOD_SR_F32:
+      return launch_rows<M_SR32>(ctx, a, w, fm, st, done, want);
+    case WSR_METHOD_Z:
+      return launch_rows<M_Z>(ctx, a, w, fm, st, done, want);
+    case WSR_METHOD_SR_BF16_TC:
+      return launch_rows<M_SRBF16_TC>(ctx, a, w, fm, st, done, want);
+    default:
+      return launch_rows<M_SRBF16>(ctx, a, w, fm, st, done, want);
+  }
+}
+
+// Accumulates a host-buffer call's outcome for wsr_euler2d_host_wait: [0] stencil tile loads that timed out,
+// [1] steps taken, [2] JS fallbacks.
+__global__ void k_host_status(const StepCtl* ctl, const int* fallbacks, unsigned long long* status) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  status[0] += fallbacks[1] ? 1ull : 0ull;
+  status[1] += (unsigned long long)ctl->steps;
+  status[2] += (unsigned long long)fallbacks[0];
 }
 
 __global__ void k_init_ctl(StepCtl* ctl, int* fallbacks, unsigned long long* counters, double t_start, double t_end, double dt, double dx, double dy, double cfl,
@@ -290,6 +400,68 @@ __global__ void k_step_begin_ring(StepCtl* ctl, double* ring) {
 
 }  // namespace
 
+// Copy streams, band events and the status word of wsr_euler2d_advance_host, one per context. The bands are the
+// interior rows cut into `nb` pieces; `pending` says that the last call's read-backs may still run.
+constexpr int kHostBandsMax = 16;
+struct wsr_host_pipe {
+  cudaStream_t h2d, d2h;
+  cudaEvent_t start, up[kHostBandsMax], ready[kHostBandsMax], down[kHostBandsMax], down_all, compute_end;
+  unsigned long long* status;  // device: the k_host_status accumulators since the last wait
+  const double* host;          // host array of the last call
+  double* bufs[4];             // its device state buffers
+  int nx, ny, nb;              // grid and band count of the last call
+  bool pending;
+};
+
+namespace {
+
+void destroy_pipe(wsr_host_pipe* p) {
+  if (!p) return;
+  if (p->status) cudaFree(p->status);
+  cudaEventDestroy(p->start);
+  cudaEventDestroy(p->down_all);
+  cudaEventDestroy(p->compute_end);
+  for (int k = 0; k < kHostBandsMax; ++k) {
+    cudaEventDestroy(p->up[k]);
+    cudaEventDestroy(p->ready[k]);
+    cudaEventDestroy(p->down[k]);
+  }
+  cudaStreamDestroy(p->h2d);
+  cudaStreamDestroy(p->d2h);
+  delete p;
+}
+
+int make_pipe(wsr_ctx* ctx) {
+  if (ctx->host) return WSR_OK;
+  wsr_host_pipe* p = new (std::nothrow) wsr_host_pipe();
+  if (!p) return fail(ctx, WSR_ERR_ARG, "out of host memory");
+  std::memset(p, 0, sizeof(*p));
+  const unsigned f = cudaEventDisableTiming;
+  cudaError_t e = cudaStreamCreateWithFlags(&p->h2d, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->d2h, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->start, f);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->down_all, f);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->compute_end, f);
+  for (int k = 0; k < kHostBandsMax && e == cudaSuccess; ++k) {
+    e = cudaEventCreateWithFlags(&p->up[k], f);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ready[k], f);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->down[k], f);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&p->status), 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(p->status, 0, 4 * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    destroy_pipe(p);
+    return fail(ctx, WSR_ERR_CUDA, "host pipe: %s", cudaGetErrorString(e));
+  }
+  ctx->host = p;
+  return WSR_OK;
+}
+
+// Interior rows [band_lo(k), band_lo(k + 1)) of band k of nb.
+inline int band_lo(int ny, int nb, int k) { return (int)((long long)ny * k / nb); }
+
+}  // namespace
+
 extern "C" {
 
 int wsr_ctx_create(int device, wsr_ctx** out) {
@@ -312,6 +484,12 @@ int wsr_ctx_create(int device, wsr_ctx** out) {
 void wsr_ctx_destroy(wsr_ctx* ctx) {
   if (!ctx) return;
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  if (ctx->host) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->host->h2d);
+    cudaStreamSynchronize(ctx->host->d2h);
+    destroy_pipe(ctx->host);
+  }
   if (ctx->prof_created)
     for (int k = 0; k < kProfEvents; ++k) {
       cudaEventDestroy(ctx->ev_a[k]);
@@ -390,7 +568,7 @@ int wsr_euler2d_max_speed(wsr_ctx* ctx, const double* u, int nx, int ny, double 
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
   Ws2d w = carve(workspace, nx, ny);
   WSR_CUDA(ctx, cudaMemsetAsync(&w.ctl->max_speed_bits, 0, sizeof(unsigned long long), st));
-  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, &w.ctl->max_speed_bits);
+  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, &w.ctl->max_speed_bits, 0);
   WSR_LAUNCHED(ctx, "k_max_speed");
   unsigned long long bits = 0;
   WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, &w.ctl->max_speed_bits, sizeof(bits), cudaMemcpyDeviceToHost, st));
@@ -427,7 +605,7 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
                               check_health, check_interval,
                               max_steps);
   WSR_LAUNCHED(ctx, "k_init_ctl");
-  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u[0], nx, ny, gamma, &w.ctl->max_speed_bits);
+  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u[0], nx, ny, gamma, &w.ctl->max_speed_bits, 0);
   WSR_LAUNCHED(ctx, "k_max_speed");
   FaceMaps fm;
   if (!face_maps(w, nx, ny, &fm)) return fail(ctx, WSR_ERR_CUDA, "encoding the face-value tensor maps failed");
@@ -479,6 +657,145 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   if (t_out) *t_out = snap.t;
   if (final_slot) *final_slot = (snap.steps & 1) ? 3 : 0;
   if (fallbacks_out) *fallbacks_out = fb[0];
+  return WSR_OK;
+}
+
+int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], int nx, int ny, double dx, double dy,
+                             double gamma, double cfl, int steps, int method, int bc, int flux, int opts, int flags,
+                             int bands, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (bc & WSR_BC_Y_HALO) return fail(ctx, WSR_ERR_ARG, "WSR_BC_Y_HALO is for wsr_euler2d_stage");
+  if (!u_host) return fail(ctx, WSR_ERR_ARG, "null host array");
+  if (!u || !u[0] || !u[1] || !u[2] || !u[3]) return fail(ctx, WSR_ERR_ARG, "null state buffer");
+  if (misaligned(u[0]) || misaligned(u[1]) || misaligned(u[2]) || misaligned(u[3]))
+    return fail(ctx, WSR_ERR_ARG, "state arrays must be 16-byte aligned");
+  if (steps < 1) return fail(ctx, WSR_ERR_ARG, "steps must be >= 1");
+  if (!(cfl > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return fail(ctx, WSR_ERR_ARG, "cfl, dx, dy must be positive");
+  if (flags & ~WSR_HOST_ASYNC) return fail(ctx, WSR_ERR_ARG, "bad flags %d", flags);
+  if (bands < 0) return fail(ctx, WSR_ERR_ARG, "bands must be >= 0");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((rc = make_pipe(ctx))) return rc;
+  wsr_host_pipe* p = ctx->host;
+  cudaPointerAttributes attr;
+  WSR_CUDA(ctx, cudaPointerGetAttributes(&attr, u_host));
+  // pageable memory copies synchronously: one band, no overlap
+  int nb = bands > 0 ? bands : ny / 256;
+  nb = attr.type == cudaMemoryTypeHost ? std::max(1, std::min(std::min(nb, kHostBandsMax), ny)) : 1;
+  Ws2d w = carve(workspace, nx, ny);
+  FaceMaps fm;
+  if (!face_maps(w, nx, ny, &fm)) return fail(ctx, WSR_ERR_CUDA, "encoding the face-value tensor maps failed");
+  const size_t pitch = (size_t)(nx + 6) * 4 * sizeof(double), width = (size_t)nx * 4 * sizeof(double);
+  auto row_at = [&](double* base, int row) { return base + ((size_t)(row + kGhost) * (nx + 6) + kGhost) * 4; };
+
+  // uploads of the interior rows, band by band. Chained on one host array, band k waits for the previous call's
+  // read-back of band k (which came after that call's last use of those rows of u[0]); otherwise for earlier work
+  // on the stream and every read-back still running.
+  const bool chained = p->pending && p->host == u_host && p->nx == nx && p->ny == ny && p->nb == nb &&
+                       p->bufs[0] == u[0] && p->bufs[1] == u[1] && p->bufs[2] == u[2] && p->bufs[3] == u[3];
+  if (!chained) {
+    WSR_CUDA(ctx, cudaEventRecord(p->start, st));
+    WSR_CUDA(ctx, cudaStreamWaitEvent(p->h2d, p->start, 0));
+    if (p->pending) WSR_CUDA(ctx, cudaStreamWaitEvent(p->h2d, p->down_all, 0));
+  }
+  for (int k = 0; k < nb; ++k) {
+    const int r0 = band_lo(ny, nb, k), r1 = band_lo(ny, nb, k + 1);
+    if (chained) WSR_CUDA(ctx, cudaStreamWaitEvent(p->h2d, p->down[k], 0));
+    WSR_CUDA(ctx, cudaMemcpy2DAsync(row_at(u[0], r0), pitch, row_at(u_host, r0), pitch, width, r1 - r0,
+                                    cudaMemcpyHostToDevice, p->h2d));
+    WSR_CUDA(ctx, cudaEventRecord(p->up[k], p->h2d));
+  }
+
+  const double hmin = dx < dy ? dx : dy;
+  k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, 0.0, 1.0e300, 0.0, dx, dy, cfl, hmin, 0, 0, steps);
+  WSR_LAUNCHED(ctx, "k_init_ctl");
+  // the first stage's normal reconstructions follow the upload band by band (transmissive: every row they read is
+  // an interior row near their own); the wave speed, and with it dt, needs every band
+  const bool overlap = bc == WSR_BC_TRANSMISSIVE;
+  for (int s = 0; s < steps; ++s) {
+    double* in = (s & 1) ? u[3] : u[0];
+    double* out = (s & 1) ? u[0] : u[3];
+    const StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma, 0.0};
+    const StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma, 1.0};
+    const StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma, 0.5};
+    Rows5 done{0, 0, 0, 0, 0};
+    if (s == 0) {
+      for (int k = 0; k < nb; ++k) {
+        const int r0 = band_lo(ny, nb, k), r1 = band_lo(ny, nb, k + 1);
+        WSR_CUDA(ctx, cudaStreamWaitEvent(st, p->up[k], 0));
+        k_max_speed<<<dim3((nx + 255) / 256, r1 - r0), 256, 0, st>>>(u[0], nx, ny, gamma, &w.ctl->max_speed_bits, r0);
+        WSR_LAUNCHED(ctx, "k_max_speed");
+        if (overlap && (rc = dispatch_rows(ctx, method, a1, w, fm, st, done, normals_for_rows(ny, r1, done))))
+          return rc;
+      }
+    }
+    k_step_begin_ring<<<1, 1, 0, st>>>(w.ctl, w.dts);
+    k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
+    WSR_LAUNCHED(ctx, "k_step_begin");
+    if ((rc = dispatch_rows(ctx, method, a1, w, fm, st, done, rows_total(ny)))) return rc;
+    if ((rc = dispatch_stage(ctx, method, a2, w, fm, st))) return rc;
+    if (s == steps - 1) {
+      // the last stage band by band, each band's read-back as soon as its rows are final
+      Rows5 d3{0, 0, 0, 0, 0};
+      for (int k = 0; k < nb; ++k) {
+        const int r0 = band_lo(ny, nb, k), r1 = band_lo(ny, nb, k + 1);
+        if ((rc = dispatch_rows(ctx, method, a3, w, fm, st, d3, rows_for_update(ny, r1)))) return rc;
+        WSR_CUDA(ctx, cudaEventRecord(p->ready[k], st));
+        WSR_CUDA(ctx, cudaStreamWaitEvent(p->d2h, p->ready[k], 0));
+        WSR_CUDA(ctx, cudaMemcpy2DAsync(row_at(u_host, r0), pitch, row_at(out, r0), pitch, width, r1 - r0,
+                                        cudaMemcpyDeviceToHost, p->d2h));
+        WSR_CUDA(ctx, cudaEventRecord(p->down[k], p->d2h));
+      }
+    } else if ((rc = dispatch_stage(ctx, method, a3, w, fm, st))) {
+      return rc;
+    }
+    k_step_end<<<1, 1, 0, st>>>(w.ctl);
+    WSR_LAUNCHED(ctx, "k_step_end");
+  }
+  k_host_status<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, p->status);
+  WSR_LAUNCHED(ctx, "k_host_status");
+  WSR_CUDA(ctx, cudaEventRecord(p->compute_end, st));
+  WSR_CUDA(ctx, cudaEventRecord(p->down_all, p->d2h));
+  p->host = u_host;
+  for (int k = 0; k < 4; ++k) p->bufs[k] = u[k];
+  p->nx = nx;
+  p->ny = ny;
+  p->nb = nb;
+  p->pending = true;
+  if (flags & WSR_HOST_ASYNC) return WSR_OK;
+  return wsr_euler2d_host_wait(ctx, nullptr, nullptr);
+}
+
+int wsr_euler2d_host_order(wsr_ctx* ctx, void* stream) {
+  if (!ctx) return WSR_ERR_ARG;
+  wsr_host_pipe* p = ctx->host;
+  if (!p || !p->pending) return WSR_OK;
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  WSR_CUDA(ctx, cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), p->down_all, 0));
+  WSR_CUDA(ctx, cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), p->compute_end, 0));
+  return WSR_OK;
+}
+
+int wsr_euler2d_host_wait(wsr_ctx* ctx, int* steps_out, int* fallbacks_out) {
+  if (!ctx) return WSR_ERR_ARG;
+  if (steps_out) *steps_out = 0;
+  if (fallbacks_out) *fallbacks_out = 0;
+  wsr_host_pipe* p = ctx->host;
+  if (!p) return WSR_OK;
+  WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  WSR_CUDA(ctx, cudaEventSynchronize(p->compute_end));
+  WSR_CUDA(ctx, cudaStreamWaitEvent(p->d2h, p->compute_end, 0));
+  WSR_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, p->status, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                p->d2h));
+  WSR_CUDA(ctx, cudaMemsetAsync(p->status, 0, 4 * sizeof(unsigned long long), p->d2h));
+  WSR_CUDA(ctx, cudaStreamSynchronize(p->d2h));
+  unsigned long long h[4];
+  std::memcpy(h, ctx->host_pinned, sizeof(h));
+  p->pending = false;
+  if (steps_out) *steps_out = (int)h[1];
+  if (fallbacks_out) *fallbacks_out = (int)h[2];
+  if (h[0]) return fail(ctx, WSR_ERR_CUDA, "a stencil tile load (TMA) did not complete in time");
   return WSR_OK;
 }
 
@@ -534,7 +851,7 @@ int wsr_euler2d_slab_begin(wsr_ctx* ctx, const double* u, int nx, int ny, double
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, t_start, t_end, 0.0, dx, dy, cfl, dx < dy ? dx : dy, 0,
                               0, max_steps);
   WSR_LAUNCHED(ctx, "k_init_ctl");
-  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, &w.ctl->max_speed_bits);
+  k_max_speed<<<dim3((nx + 255) / 256, ny), 256, 0, st>>>(u, nx, ny, gamma, &w.ctl->max_speed_bits, 0);
   WSR_LAUNCHED(ctx, "k_max_speed");
   return WSR_OK;
 }
@@ -710,17 +1027,17 @@ int noalloc_launch(const typename ClosureParams<M>::type& P, const StageArgs& a,
                    cudaStream_t st) {
   const dim3 blk(128);
   k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, a.ny + 5), blk, 0, st>>>(
-      a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P);
+      a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P, 0);
   k_normal<M, 2><<<dim3((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4), blk, 0, st>>>(
-      a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P);
+      a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P, 0);
   k_flux<M, 1><<<dim3((a.nx + 1 + 31) / 32, (a.ny + 3) / 4), blk, 0, st>>>(
       w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P, fm.xl,
-      fm.xr);
+      fm.xr, 0);
   k_flux<M, 2><<<dim3((a.nx + 127) / 128, a.ny + 1), blk, 0, st>>>(
       w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P, fm.yl,
-      fm.yr);
+      fm.yr, 0);
   k_update<<<dim3((a.nx + 255) / 256, a.ny), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk,
-                                                          a.g, w.ctl);
+                                                          a.g, w.ctl, 0);
   // the error state was drained on entry, so an error here comes from these launches
   return cudaPeekAtLastError() == cudaSuccess ? WSR_OK : WSR_ERR_CUDA;
 }

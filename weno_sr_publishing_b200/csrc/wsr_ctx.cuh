@@ -14,6 +14,8 @@
 constexpr int kProfKinds = 6;  // normal x, normal y, flux x, flux y, update, control
 constexpr int kProfEvents = 512;
 
+struct wsr_host_pipe;  // copy streams and band events of wsr_euler2d_advance_host (wsr_api.cu)
+
 struct wsr_ctx {
   int device;
   bool have_closure;
@@ -34,6 +36,7 @@ struct wsr_ctx {
   int n_ev;
   double prof_ms[kProfKinds];
   long long prof_count[kProfKinds];
+  wsr_host_pipe* host;  // created by the first host-buffer call
 };
 
 namespace wsr_detail {

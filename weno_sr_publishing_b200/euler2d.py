@@ -152,81 +152,39 @@ def run(bufs: list, params: Params, t_end: float, method: str, boundary: str, ml
     return RunResult(slot.value, [float(x) for x in dts[:steps.value]], steps.value, t.value, fb.value)
 
 
-_COPY_BANDS = 8
-_MAX_PIPES = 8  # copy pipes kept per process (one per host buffer in use); the oldest is retired beyond this
-_copy_pipes: dict = {}
-
-
-class _CopyPipe:
-    """Copy streams of one host buffer: the state goes in and out in row bands, host -> device on one stream
-    and device -> host on another, and band b of a call's input waits only for band b of the previous call's
-    output (the same pinned rows), so one call's read-back and the next call's upload share the two copy
-    directions instead of following each other."""
-
-    def __init__(self, dev: torch.device, rows: int):
-        self.h2d = torch.cuda.Stream(dev)
-        self.d2h = torch.cuda.Stream(dev)
-        edges = np.linspace(0, rows, min(_COPY_BANDS, rows) + 1).astype(int)
-        self.bands = [(int(a), int(b)) for a, b in zip(edges[:-1], edges[1:]) if b > a]
-        self.out_done = [torch.cuda.Event() for _ in self.bands]
-        self.pending = False
-
-
-def _pipe_for(key, dev: torch.device, rows: int) -> _CopyPipe:
-    pipe = _copy_pipes.get(key)
-    if pipe is None:
-        if len(_copy_pipes) >= _MAX_PIPES:
-            old_key = next(iter(_copy_pipes))
-            old = _copy_pipes.pop(old_key)
-            if old.pending:  # its read-back stays ordered before later work of this process
-                torch.cuda.current_stream(old.d2h.device).wait_stream(old.d2h)
-        pipe = _copy_pipes[key] = _CopyPipe(dev, rows)
-    return pipe
-
-
-def advance_host(u_host: np.ndarray, params: Params, steps: int, method: str, boundary: str, mlp_params=None,
+def advance_host(u_host, params: Params, steps: int, method: str, boundary: str, mlp_params=None,
                  bufs: list | None = None, ws: Workspace | None = None, device="cuda",
-                 async_readback: bool = False) -> np.ndarray:
-    """Host-buffer entry: copy the padded state to the device, run `steps` full CFL steps, copy it back
-    into u_host (in place), and return u_host.
+                 async_readback: bool = False, bands: int = 0):
+    """Host-buffer entry (wsr_euler2d_advance_host): copy the interior of the padded host state to the device,
+    run `steps` full CFL steps (bit for bit the device loop's), copy the result's interior back into u_host (in
+    place; its ghost cells are left as they are), and return u_host.
 
-    By default the call returns after the read-back has completed, so u_host holds the result. With
-    async_readback=True and pinned host memory, the read-back is asynchronous DMA in row bands on a copy stream
-    and the call returns as soon as it is queued: u_host is complete only after host_copies_done() (which orders
-    the current stream after it) and a synchronisation, or after the device is synchronised. The next call's
-    upload of the same rows waits for the previous read-back band by band, so consecutive calls overlap their
-    two copy directions. Work on the device buffers `bufs` waits for every read-back still in flight on the
-    device, whichever host buffer it targets, before it overwrites them."""
+    The copies run in row bands on the library's own copy streams: the first stage's wave speed and (transmissive
+    boundary) normal reconstructions follow the upload band by band, and the last stage runs band by band with
+    each band's read-back starting as soon as its rows are final. By default the call returns when u_host holds
+    the result. With async_readback=True (pinned host memory) it returns once queued: consecutive calls on the
+    same host array and `bufs` then overlap both copy directions with the computation, and u_host is complete
+    after host_copies_done() (which orders the current stream after the read-backs) and a synchronisation, or
+    after host_wait(). bands: 0 picks one band per 256 rows."""
     dev = torch.device(device)
     if bufs is None:
         bufs = [torch.empty(params.padded_shape, dtype=torch.float64, device=dev) for _ in range(4)]
+    for b in bufs:
+        _check_state(b, params)
     host = torch.from_numpy(u_host) if isinstance(u_host, np.ndarray) else u_host
-    idx = dev.index if dev.index is not None else torch.cuda.current_device()
-    key = (idx, host.data_ptr(), tuple(host.shape))
-    cur = torch.cuda.current_stream(dev)
-    pipe = _pipe_for(key, dev, int(host.shape[0]))
-    for other_key, other in _copy_pipes.items():  # read-backs of other host buffers may still read from bufs
-        if other is not pipe and other.pending and other_key[0] == idx:
-            cur.wait_stream(other.d2h)
-    pipe.h2d.wait_stream(cur)  # earlier work on bufs[0] is done before it is overwritten
-    with torch.cuda.stream(pipe.h2d):
-        for k, (r0, r1) in enumerate(pipe.bands):
-            if pipe.pending:
-                pipe.h2d.wait_event(pipe.out_done[k])
-            bufs[0][r0:r1].copy_(host[r0:r1], non_blocking=True)
-    cur.wait_stream(pipe.h2d)
-    res = run(bufs, params, 1.0e300, method, boundary, mlp_params=mlp_params, fixed_steps=steps, ws=ws)
-    out = bufs[res.final_slot]
-    pipe.d2h.wait_stream(cur)
-    with torch.cuda.stream(pipe.d2h):
-        for k, (r0, r1) in enumerate(pipe.bands):
-            host[r0:r1].copy_(out[r0:r1], non_blocking=True)
-            pipe.out_done[k].record(pipe.d2h)
-    if async_readback:
-        pipe.pending = True
-    else:
-        pipe.d2h.synchronize()
-        pipe.pending = False
+    if host.dtype != torch.float64 or host.is_cuda or tuple(host.shape) != tuple(params.padded_shape) \
+            or not host.is_contiguous():
+        raise ValueError(f"u_host must be a contiguous float64 host array of shape {tuple(params.padded_shape)}")
+    if boundary not in N.BC:
+        raise ValueError(f"unsupported boundary {boundary!r}")
+    ctx = prepare_closure(method, mlp_params, device_index(dev))
+    ws = ws or workspace(params.nx, params.ny, dev)
+    ptrs = (C.c_void_p * 4)(*[b.data_ptr() for b in bufs])
+    flags = N.HOST_ASYNC if async_readback else 0
+    ctx.check(N.lib().wsr_euler2d_advance_host(
+        ctx.handle, C.c_void_p(host.data_ptr()), ptrs, params.nx, params.ny, params.dx, params.dy, params.gamma,
+        params.cfl, int(steps), N.METHOD[method], N.BC[boundary], N.FLUX["hllc"], 0, flags, int(bands),
+        C.c_void_p(ws.ptr), ws.nbytes, _stream_ptr(dev)))
     return u_host
 
 
@@ -234,8 +192,15 @@ def host_copies_done(device="cuda") -> None:
     """Make the current stream wait for every read-back advance_host(async_readback=True) has issued on
     `device` (work or events recorded on the current stream afterwards come after them)."""
     dev = torch.device(device)
-    idx = dev.index if dev.index is not None else torch.cuda.current_device()
-    cur = torch.cuda.current_stream(dev)
-    for key, pipe in _copy_pipes.items():
-        if key[0] == idx:
-            cur.wait_stream(pipe.d2h)
+    ctx = N.context(device_index(dev))
+    ctx.check(N.lib().wsr_euler2d_host_order(ctx.handle, _stream_ptr(dev)))
+
+
+def host_wait(device="cuda") -> dict:
+    """Wait for every advance_host call on `device` and its read-back; returns the steps taken and the JS
+    fallbacks summed over the calls since the previous wait, and raises an error any of them met on the device."""
+    dev = torch.device(device)
+    ctx = N.context(device_index(dev))
+    steps, fb = C.c_int(0), C.c_int(0)
+    ctx.check(N.lib().wsr_euler2d_host_wait(ctx.handle, C.byref(steps), C.byref(fb)))
+    return {"steps": steps.value, "fallbacks": fb.value}
