@@ -50,8 +50,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--method", default="sr_f32", choices=["sr_f32", "sr_f64", "sr_bf16", "sr_bf16_tc", "js"],
-                    help="sr_bf16_tc: the BF16 closure's MLP on the tensor cores (2D step only)")
+    ap.add_argument("--method", default="sr_f32", choices=["sr_f32", "sr_f64", "sr_bf16", "sr_bf16_tc", "js", "z"],
+                    help="sr_bf16_tc: the BF16 closure's MLP on the tensor cores (2D step only); z: WENO5-Z "
+                         "(3D step only)")
     ap.add_argument("--n", type=int, default=2000)
     ap.add_argument("--t0", type=float, default=0.125)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -214,6 +215,8 @@ def run_reference(args, rank):
 
 def main():
     args = parse()
+    if args.method == "z" and args.workload != "euler3d":
+        raise SystemExit("--method z is for --workload euler3d")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -946,10 +949,11 @@ def bench_3d(args, world, rank, local):
     from weno_sr_publishing_b200.checkpoint import MODELS_DIR
     method = args.method
     params = None
-    if method != "js":
+    if method not in ("js", "z"):
         name = "weno5_sr_fp64_step012250.npz" if method == "sr_f64" else "weno5_sr_fp32_step016500.npz"
         params = {k: v for k, v in np.load(MODELS_DIR / name).items() if k != "meta_json"}
-    metric = f"3D Euler cell-updates/s, WENO5-SR ({method}) HLLC, 224x88x88 shock-bubble"
+    scheme = {"js": "WENO5-JS", "z": "WENO5-Z"}.get(method, f"WENO5-SR ({method})")
+    metric = f"3D Euler cell-updates/s, {scheme} HLLC, 224x88x88 shock-bubble"
     cfg = {"workload": "3D shock-bubble, 224x88x88 on [0,2.545]x[0,1]^2, seed 0 (Mach and density ratio), "
                        "post-shock inflow, from t=0", "method": method, "flux": "hllc", "cfl": 0.4,
            "time_integrator": "SSPRK3", "state_precision": "fp64",
@@ -1019,7 +1023,7 @@ def bench_3d(args, world, rank, local):
            opts=4)
     line["closure_tally_per_step"] = {k: {"mlp": v[0] / K, "plateau": v[1] / K} for k, v in E3.counters(ws).items()
                                       if k != "fallbacks"}
-    if method != "js":
+    if method not in ("js", "z"):
         line["roofline"] = _closure_roofline(
             "k3_normal + k3_trans + k3_flux (closure work only)", method,
             [(v[0] / K, v[1] / K, 1 if k == "normal" else 2) for k, v in E3.counters(ws).items() if k != "fallbacks"],
