@@ -681,7 +681,9 @@ int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], i
   cudaPointerAttributes attr;
   WSR_CUDA(ctx, cudaPointerGetAttributes(&attr, u_host));
   // pageable memory copies synchronously: one band, no overlap
-  int nb = bands > 0 ? bands : ny / 140;  // measured at 2000^2: 7 bands 5.51, 14 bands 5.31, 16 bands 5.34 ms per call
+  // one band per 280 rows: on the 2000^2 benchmark state 4 / 7 / 10 / 14 / 20 bands took 7.01 / 6.70 / 6.74 / 7.15 /
+  // 7.42 ms per call (more bands start the copies sooner but cut the heavy stage kernels into more tails)
+  int nb = bands > 0 ? bands : ny / 280;
   nb = attr.type == cudaMemoryTypeHost ? std::max(1, std::min(std::min(nb, kHostBandsMax), ny)) : 1;
   Ws2d w = carve(workspace, nx, ny);
   FaceMaps fm;
