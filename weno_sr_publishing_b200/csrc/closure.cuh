@@ -399,6 +399,20 @@ __device__ __forceinline__ Sens sensors5(const double q[5]) {
 
 __device__ __forceinline__ bool is_plateau(const Sens& s) { return s.dmax <= 1.0e-13 * s.qscale; }
 
+// is_plateau(sensors5(q)) with the scale max(max|q|, 1) formed only when it can change the answer: the threshold
+// 1e-13 * scale is at least 1e-13 (scale >= 1, and the product is rounded monotonically), so dmax <= 1e-13 is a
+// plateau whatever q is. Same decision for every input, NaN included.
+__device__ __forceinline__ bool plateau5(const double q[5]) {
+  const double d20 = q[0] - 2.0 * q[1] + q[2], d21 = q[1] - 2.0 * q[2] + q[3], d22 = q[2] - 2.0 * q[3] + q[4];
+  const double d0 = (13.0 / 12.0) * fabs(d20) + 0.25 * fabs(q[0] - 4.0 * q[1] + 3.0 * q[2]);
+  const double d1 = (13.0 / 12.0) * fabs(d21) + 0.25 * fabs(q[1] - q[3]);
+  const double d2 = (13.0 / 12.0) * fabs(d22) + 0.25 * fabs(3.0 * q[2] - 4.0 * q[3] + q[4]);
+  const double dmax = fmax(fmax(d0, d1), d2);
+  if (dmax <= 1.0e-13) return true;
+  const double qs = fmax(fmax(fmax(fabs(q[0]), fabs(q[1])), fmax(fabs(q[2]), fabs(q[3]))), fabs(q[4]));
+  return dmax <= 1.0e-13 * fmax(qs, 1.0);
+}
+
 __device__ __forceinline__ double gamma_s(const double q[5]) {
   const double eps = 1.0e-15;
   double d20 = q[0] - 2.0 * q[1] + q[2], d21 = q[1] - 2.0 * q[2] + q[3], d22 = q[2] - 2.0 * q[3] + q[4];

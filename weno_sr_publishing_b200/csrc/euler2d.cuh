@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
       } else if constexpr (M == M_Z) {
         s_val[n][t] = z_value(s, side, DIR == 1 ? P.ex : P.ey);  // eps = h^2 of the normal direction
       } else {
-        need = !is_plateau(sensors5(s));
+        need = !plateau5(s);
         if (!need) s_val[n][t] = linear_value(s, side);
         ++(need ? tally.mlp : tally.plateau);
       }
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       s_g[0][n][t] = z_value_w(z, s, 2);
       s_g[1][n][t] = z_value_w(z, s, 3);
     } else {
-      need = !is_plateau(sensors5(s));
+      need = !plateau5(s);
       if (!need) {
         s_g[0][n][t] = linear_value(s, 2);
         s_g[1][n][t] = linear_value(s, 3);
