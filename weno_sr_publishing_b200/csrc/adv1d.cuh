@@ -242,6 +242,23 @@ __device__ __forceinline__ bool adv_plateau(const double q[Weno<SCHEME>::W], dou
   return dmax <= 1.0e-13 * qs;
 }
 
+// adv_plateau's decision alone: the scale max(max|q|, 1) is formed only when dmax > 1e-13 (below that, every scale
+// >= 1 gives a plateau, the product 1e-13 * scale being rounded monotonically). Same decision for every input.
+template <int SCHEME>
+__device__ __forceinline__ bool adv_plateau_test(const double q[Weno<SCHEME>::W]) {
+  using S = Weno<SCHEME>;
+  double d[S::R];
+  S::deltas(q, d);
+  double dmax = d[0];
+#pragma unroll
+  for (int k = 1; k < S::R; ++k) dmax = fmax(dmax, d[k]);
+  if (dmax <= 1.0e-13) return true;
+  double qs = fabs(q[0]);
+#pragma unroll
+  for (int k = 1; k < S::W; ++k) qs = fmax(qs, fabs(q[k]));
+  return dmax <= 1.0e-13 * fmax(qs, 1.0);
+}
+
 template <int SCHEME>
 __device__ __forceinline__ void adv_features(const double q[Weno<SCHEME>::W], const double d[Weno<SCHEME>::R], double dmax,
                                              double qs, double f[Weno<SCHEME>::NF]) {
@@ -397,8 +414,7 @@ __device__ __forceinline__ void adv_faces(const double* __restrict__ v, const Ad
           fl[i] = weighted_z<SCHEME>(s, lr_up, g);
         }
       } else {
-        double d[R], dmax, qs;
-        need = !adv_plateau<SCHEME>(s, d, dmax, qs);
+        need = !adv_plateau_test<SCHEME>(s);
         if (!need) {
           if (BOTH) {
             fl[i] = weighted<SCHEME>(s, 1, nullptr, true);

@@ -547,12 +547,12 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_normal(const
     const int f = n >> 1, side = n & 1;
     bool need = false;
     if (active) {
-      double q[7], cq[7], d[4], dmax, qs;
+      double q[7], cq[7];
 #pragma unroll
       for (int k = 0; k < 7; ++k) q[k] = s_ch[f][k + side][t];
 #pragma unroll
       for (int k = 0; k < 7; ++k) cq[k] = side ? q[6 - k] : q[k];
-      need = !adv_plateau<7>(cq, d, dmax, qs);
+      need = !adv_plateau_test<7>(cq);
       if (!need) {
         const double one[4] = {1.0, 1.0, 1.0, 1.0};
         s_val[n][t] = w7sr_face(q, side + 1, one);
@@ -658,10 +658,10 @@ __global__ void __launch_bounds__(kBlock7, WSR_W7SR_MIN_BLOCKS) k7s_flux(const d
     for (int gp = 0; gp < 2; ++gp) {
       bool need = false;
       if (active) {
-        double cq[7], d[4], dmax, qs;
+        double cq[7];
 #pragma unroll
         for (int k = 0; k < 7; ++k) cq[k] = gp ? q[6 - k] : q[k];
-        need = !adv_plateau<7>(cq, d, dmax, qs);
+        need = !adv_plateau_test<7>(cq);
         if (!need) {
           const double one[4] = {1.0, 1.0, 1.0, 1.0};
           s_g[2 * m + gp][t] = w7sr_gauss(q, gp + 1, one);

@@ -344,7 +344,7 @@ __device__ __forceinline__ double recon(const double q[5], int head, const typen
   } else if constexpr (M == M_Z) {
     return z3(q, head, P.ex);  // P.ex = h^2 of this kernel's reconstruction direction
   } else {
-    if (is_plateau(sensors5(q))) {
+    if (plateau5(q)) {
       ++tally.plateau;
       return linear_value(q, head);
     }
