@@ -71,6 +71,13 @@ extern "C" {
 #define WSR_OPT_Z_HALO 8      /* wsr_euler3d_stage: the 3 z ghost planes below and above are filled by the caller
                                  (a slab of a z-decomposed grid) and not overwritten; x and y ghosts are filled as
                                  usual. wsr_euler3d_run rejects it. */
+#define WSR_OPT_FACE_THREADS_8 32 /* 2D WENO5-SR stages (FP64, FP32, BF16 closures): eight threads per face in the
+                                     two reconstruction kernels (16 faces per 128-thread block; each thread forms one
+                                     stencil and at most one closure evaluation) whatever the grid size; the default
+                                     picks this form for grids of at most 256 x 256 cells, where one thread per face
+                                     is latency bound by its serial closure evaluations. Same results bit for bit.
+                                     JS, WENO-Z and the tensor-core closure always use one thread per face. */
+#define WSR_OPT_FACE_THREADS_1 64 /* 2D WENO5 stages: one thread per face whatever the grid size */
 
 typedef struct wsr_ctx wsr_ctx;
 

@@ -266,3 +266,30 @@ def test_bf16_tensor_core_closure_matches_fma_closure(case):
     res2 = E.run(bufs2, p, 1.0, "sr_bf16", bc, mlp_params=P32, fixed_steps=5)
     got, want = bufs[res.final_slot].cpu().numpy(), bufs2[res2.final_slot].cpu().numpy()
     assert _rel(_interior(got, nx, ny), _interior(want, nx, ny)) <= 1e-3
+
+
+# The eight-threads-per-face reconstruction kernels (the SR default on small grids) against the one-thread-per-face
+# kernels: the same per-stencil arithmetic, so runs agree bit for bit, dts, closure tallies and JS fallbacks included
+# (JS and WENO-Z ignore the option: both layouts give the one-thread-per-face kernels).
+@pytest.mark.parametrize("method", ["js", "z", "sr_f64", "sr_f32", "sr_bf16"])
+@pytest.mark.parametrize("bc,flux", [("transmissive", "hllc"), ("periodic", "force"), ("double-mach", "hllc")])
+def test_face_thread_layouts_agree_bitwise(method, bc, flux):
+    from weno_sr_publishing_b200 import _native as N
+
+    nx, ny = 61, 47
+    if bc == "double-mach":
+        p = Params(nx=nx, ny=ny, x_length=4.0, y_length=1.0, cfl=0.4)
+        init = problems.double_mach_state(nx, ny, quadrature=3)
+    else:
+        p = Params(nx=nx, ny=ny, x_length=1.0, y_length=0.8, cfl=0.4)
+        init = problems.make_quadrant_state(nx, ny, problems.seeded_quadrant_states(4), 3)
+    out = {}
+    for layout in (N.OPT_FACE_THREADS_1, N.OPT_FACE_THREADS_8):
+        bufs = [_t(init)] + [torch.zeros_like(_t(init)) for _ in range(3)]
+        ws = E.workspace(nx, ny, DEV)
+        res = E.run(bufs, p, 1.0, method, bc, mlp_params=PARAMS[method], flux=flux, fixed_steps=4,
+                    opts=layout | N.OPT_COUNT | N.OPT_JS_FALLBACK, ws=ws)
+        out[layout] = (bufs[res.final_slot].cpu().numpy(), res.dts, E.counters(ws), res.fallbacks)
+    a, b = out[N.OPT_FACE_THREADS_1], out[N.OPT_FACE_THREADS_8]
+    np.testing.assert_array_equal(_interior(a[0], nx, ny), _interior(b[0], nx, ny))
+    assert a[1] == b[1] and a[2] == b[2] and a[3] == b[3]

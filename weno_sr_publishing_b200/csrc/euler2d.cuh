@@ -184,8 +184,33 @@ __device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q,
 //        out_r[r][c] and out_l[r+1][c], arrays [ny+2][nx+6].
 // Stencil n = 2 f + side of a face: characteristic field f; side 0 -> cells 0..4 with head 0 (lr=1),
 // side 1 -> cells 1..5 with head 1 (lr=2).
+// FACES < kBlock (small grids): the block's first FACES threads take one face each (a row of FACES faces) and all
+// kBlock threads share its closure queue, so a thread evaluates at most 8 FACES / kBlock closures instead of up to
+// 8 (on a small grid the one-face-per-thread launch is latency bound by that serial chain). The face arithmetic
+// is the same code either way.
 // -------------------------------------------------------------------------------------------
-template <int M, int DIR>
+constexpr int kSmallFaces = 16;  // faces per block of the small-grid form
+
+// Phase A of one characteristic stencil with its side (= head) a compile-time constant, as in the unrolled pairs of
+// the one-face-per-thread loop: the value at once, or true when the stencil needs the closure.
+template <int M, int DIR, int SIDE>
+__device__ __forceinline__ bool normal_stencil_a(const double s[5], const typename ClosureParams<M>::type& P,
+                                                 double& val, Tally& tally) {
+  if constexpr (M == M_JS) {
+    val = js_value(s, SIDE);
+    return false;
+  } else if constexpr (M == M_Z) {
+    val = z_value(s, SIDE, DIR == 1 ? P.ex : P.ey);  // eps = h^2 of the normal direction
+    return false;
+  } else {
+    const bool need = !plateau5(s);
+    if (!need) val = linear_value(s, SIDE);
+    ++(need ? tally.mlp : tally.plateau);
+    return need;
+  }
+}
+
+template <int M, int DIR, int FACES = kBlock>
 __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double* __restrict__ u, double* __restrict__ out_l,
                                                       double* __restrict__ out_r, int nx, int ny, StageBc bc, Gas gas,
                                                       const StepCtl* __restrict__ ctl, int opts,
@@ -193,17 +218,20 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
                                                       unsigned long long* __restrict__ counters,
                                                       const __grid_constant__ typename ClosureParams<M>::type P,
                                                       int yb0) {
-  __shared__ double s_ch[4][6][kBlock];                  // characteristic values, [field][cell][thread]
-  __shared__ double s_val[kStencilsPerThread][kBlock];   // reconstructed characteristic face values
-  __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
+  __shared__ double s_ch[4][6][FACES];                  // characteristic values, [field][cell][face thread]
+  __shared__ double s_val[kStencilsPerThread][FACES];   // reconstructed characteristic face values
+  __shared__ unsigned short s_q[kStencilsPerThread * FACES];
   __shared__ int s_count;
   if (ctl != nullptr && ctl->done) return;  // uniform across the launch
   using TL = Tile<DIR == 2>;
   const int t = threadIdx.x;
-  const int c = TL::x(t);
-  const int r = TL::y(t, yb0);
+  constexpr bool kAll = FACES == kBlock;
+  const bool face_thread = kAll || t < FACES;
+  const int c = kAll ? TL::x(t) : (int)blockIdx.x * FACES + t;
+  const int r = kAll ? TL::y(t, yb0) : (int)blockIdx.y + yb0;
   const int nxt = nx + 2 * kGhost;
-  const bool active = DIR == 1 ? (r >= 1 && r < ny + 5 && c <= nx) : (r <= ny && c >= 1 && c < nx + 5);
+  const bool active =
+      face_thread && (DIR == 1 ? (r >= 1 && r < ny + 5 && c <= nx) : (r <= ny && c >= 1 && c < nx + 5));
   if (t == 0) s_count = 0;
   Tally tally;
   RoeJ J;
@@ -221,18 +249,41 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
     };
     J = roe_jacobian(cell(2), cell(3), gas);
     const CharL L = char_left<DIR>(J, gas);
+    if (face_thread) {
 #pragma unroll 1
-    for (int k = 0; k < 6; ++k) {
-      const d4 qk = cell(k);
+      for (int k = 0; k < 6; ++k) {
+        const d4 qk = cell(k);
 #pragma unroll
-      for (int f = 0; f < 4; ++f) s_ch[f][k][t] = project<DIR>(L, f, qk);
+        for (int f = 0; f < 4; ++f) s_ch[f][k][t] = project<DIR>(L, f, qk);
+      }
     }
   }
   const bool work = active;
   __syncthreads();
+  if constexpr (!kAll) {
+    // Phase A of the small-grid form: lane n of the 8 lanes of face t / 8 takes stencil n
+    constexpr int kLanes = kBlock / FACES;
+    const int face = t / kLanes, n = t % kLanes, f = n >> 1, side = n & 1;
+    const int fc = (int)blockIdx.x * FACES + face;
+    const bool live = DIR == 1 ? (r >= 1 && r < ny + 5 && fc <= nx) : (r <= ny && fc >= 1 && fc < nx + 5);
+    bool need = false;
+    if (live) {
+      double s[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][face];
+      double v = 0.0;
+      if (side == 0)
+        need = normal_stencil_a<M, DIR, 0>(s, P, v, tally);
+      else
+        need = normal_stencil_a<M, DIR, 1>(s, P, v, tally);
+      if (!need) s_val[n][face] = v;
+    }
+    if constexpr (has_mlp<M>()) queue_push(need, n * FACES + face, s_q, &s_count);
+  }
   // Phase A, two stencils per iteration (two independent dependency chains; unrolling by 4 or 8 spills)
 #pragma unroll 2
   for (int n = 0; n < kStencilsPerThread; ++n) {
+    if (!kAll) break;
     const int f = n >> 1, side = n & 1;
     bool need = false;
     if (work) {
@@ -249,10 +300,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
         ++(need ? tally.mlp : tally.plateau);
       }
     }
-    if constexpr (has_mlp<M>()) queue_push(need, n * kBlock + t, s_q, &s_count);
+    if constexpr (has_mlp<M>()) queue_push(need, n * FACES + t, s_q, &s_count);
   }
   // Phase B
-  if constexpr (M == M_SRBF16_TC) {
+  if constexpr (M == M_SRBF16_TC && kAll) {
     // BF16 closure on the tensor cores: each warp takes 32 queue entries at a time (closure_mma.cuh)
     __syncthreads();
     const int count = s_count;
@@ -284,7 +335,7 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
 #pragma unroll 1
     for (int e = t; e < count; e += kBlock) {
       const int id = s_q[e];
-      const int n = id / kBlock, o = id % kBlock, f = n >> 1, side = n & 1;
+      const int n = id / FACES, o = id % FACES, f = n >> 1, side = n & 1;
       double s[5];
 #pragma unroll
       for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][o];
@@ -434,7 +485,59 @@ __device__ __forceinline__ void tile_transverse(const double* tile, int i, int j
   }
 }
 
+// Stencil n = 2 comp + side of face (i, j) read from the face-value arrays themselves (the small-grid form of
+// k_flux, which stages no tile): the same values as tile_transverse.
+template <int DIR>
+__device__ __forceinline__ void global_transverse(const double* __restrict__ fl, const double* __restrict__ fr, int nx,
+                                                  int i, int j, int n, bool active, double s[5]) {
+  const int comp = n >> 1, side = n & 1;
+  if (!active) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) s[k] = 0.0;
+    return;
+  }
+  const double* src = side == 0 ? fl : fr;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const size_t cell = DIR == 1 ? (size_t)(j + 1 + k) * (nx + 2) + (side == 0 ? i + 1 : i)
+                                 : (size_t)(side == 0 ? j + 1 : j) * (nx + 6) + i + 1 + k;
+    s[k] = src[cell * 4 + comp];
+  }
+}
+
+// Phase A of one transverse stencil: its values at the two Gauss points at once, or true when it needs the closure.
 template <int M, int DIR>
+__device__ __forceinline__ bool flux_stencil_a(const double s[5], const typename ClosureParams<M>::type& P, double& g0,
+                                               double& g1, Tally& tally) {
+  if constexpr (M == M_JS) {
+    const StencilW js = js_stencil(s);
+    double w[3], c[3];
+    js_head_weights(js, linear_weights(2), w);
+    candidates(s, 2, c);
+    g0 = combine(w, c);
+    js_head_weights(js, linear_weights(3), w);
+    candidates(s, 3, c);
+    g1 = combine(w, c);
+    return false;
+  } else if constexpr (M == M_Z) {
+    const StencilW z = z_stencil(s, DIR == 1 ? P.ey : P.ex);  // eps = h^2 of the transverse direction
+    g0 = z_value_w(z, s, 2);
+    g1 = z_value_w(z, s, 3);
+    return false;
+  } else {
+    const bool need = !plateau5(s);
+    if (!need) {
+      g0 = linear_value(s, 2);
+      g1 = linear_value(s, 3);
+    }
+    ++(need ? tally.mlp : tally.plateau);
+    return need;
+  }
+}
+
+// FACES < kBlock: the small-grid form, as in k_normal (the block's first FACES threads take one face each, all
+// kBlock threads share the closure queue); its stencils come from the face-value arrays directly.
+template <int M, int DIR, int FACES = kBlock>
 __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* __restrict__ fl, const double* __restrict__ fr,
                                                     double* __restrict__ fout, int nx, int ny, Gas gas, int flux,
                                                     const StepCtl* __restrict__ ctl, int opts,
@@ -443,36 +546,60 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
                                                     const __grid_constant__ typename ClosureParams<M>::type P,
                                                     const __grid_constant__ CUtensorMap map_l,
                                                     const __grid_constant__ CUtensorMap map_r, int yb0) {
-  __shared__ double s_g[2][kStencilsPerThread][kBlock];  // values at Gauss points 1 and 2
-  __shared__ unsigned short s_q[kStencilsPerThread * kBlock];
-  __shared__ __align__(128) double s_tile[4 * FluxTile<DIR>::stride];
+  constexpr bool kAll = FACES == kBlock;
+  __shared__ double s_g[2][kStencilsPerThread][FACES];  // values at Gauss points 1 and 2
+  __shared__ unsigned short s_q[kStencilsPerThread * FACES];
+  __shared__ __align__(128) double s_tile[kAll ? 4 * FluxTile<DIR>::stride : 2];
   __shared__ unsigned long long s_mbar;
   __shared__ int s_count;
   if (ctl->done) return;  // uniform across the launch
   using TL = Tile<DIR == 1>;
   const int t = threadIdx.x;
-  const int i = TL::x(t);
-  const int j = TL::y(t, yb0);
+  const bool face_thread = kAll || t < FACES;
+  const int i = kAll ? TL::x(t) : (int)blockIdx.x * FACES + t;
+  const int j = kAll ? TL::y(t, yb0) : (int)blockIdx.y + yb0;
   const int i0 = blockIdx.x * TL::bx, j0 = ((int)blockIdx.y + yb0) * TL::by;
   const int nfx = DIR == 1 ? nx + 1 : nx, nfy = DIR == 1 ? ny : ny + 1;
-  const bool active = i < nfx && j < nfy;
+  const bool active = face_thread && i < nfx && j < nfy;
   const double dt_h = DIR == 1 ? ctl->dt_dx : ctl->dt_dy;
   if (t == 0) s_count = 0;
-  const bool tile_ok = load_flux_tile<DIR>(s_tile, &s_mbar, &map_l, &map_r, i0, j0);
-  if (__syncthreads_or(!tile_ok)) {  // the same decision in every thread of the block
-    if (t == 0) atomicExch(&fallbacks[1], 1);
-    if (!tile_ok) load_flux_tile_wait_again(&s_mbar);
-    return;
+  if constexpr (kAll) {
+    const bool tile_ok = load_flux_tile<DIR>(s_tile, &s_mbar, &map_l, &map_r, i0, j0);
+    if (__syncthreads_or(!tile_ok)) {  // the same decision in every thread of the block
+      if (t == 0) atomicExch(&fallbacks[1], 1);
+      if (!tile_ok) load_flux_tile_wait_again(&s_mbar);
+      return;
+    }
+  } else {
+    __syncthreads();
   }
   Tally tally;
   const bool work = active;
+  // Phase A of the small-grid form: lane n of the 8 lanes of face t / 8 takes stencil n
+  if constexpr (!kAll) {
+    constexpr int kLanes = kBlock / FACES;
+    const int face = t / kLanes, n = t % kLanes;
+    const int fi = (int)blockIdx.x * FACES + face;
+    const bool live = fi < nfx && j < nfy;
+    double s[5];
+    global_transverse<DIR>(fl, fr, nx, fi, j, n, live, s);
+    double g0 = 0.0, g1 = 0.0;
+    const bool need = live && flux_stencil_a<M, DIR>(s, P, g0, g1, tally);
+    if (live && !need) {
+      s_g[0][n][face] = g0;
+      s_g[1][n][face] = g1;
+    }
+    if constexpr (has_mlp<M>()) queue_push(need, n * FACES + face, s_q, &s_count);
+  }
   // Phase A, two stencils per iteration. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L
   // (lr=1 faces fr).
 #pragma unroll 2
   for (int n = 0; n < kStencilsPerThread; ++n) {
+    if (!kAll) break;
     double s[5];
     tile_transverse<DIR>(s_tile, i, j, i0, j0, n, work, s);
     bool need = false;
+    // the body of flux_stencil_a written out (measured 0.7% faster at 2000^2 than the call, same results)
     if (!work) {
       // nothing to reconstruct
     } else if constexpr (M == M_JS) {
@@ -496,10 +623,10 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
       }
       ++(need ? tally.mlp : tally.plateau);
     }
-    if constexpr (has_mlp<M>()) queue_push(need, n * kBlock + t, s_q, &s_count);
+    if constexpr (has_mlp<M>()) queue_push(need, n * FACES + t, s_q, &s_count);
   }
   // Phase B: one closure evaluation per queued stencil serves both Gauss points.
-  if constexpr (M == M_SRBF16_TC) {
+  if constexpr (M == M_SRBF16_TC && kAll) {
     // BF16 closure on the tensor cores: each warp takes 32 queue entries at a time (closure_mma.cuh)
     __syncthreads();
     const int count = s_count;
@@ -533,9 +660,12 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
 #pragma unroll 1
     for (int e = t; e < count; e += kBlock) {
       const int id = s_q[e];
-      const int n = id / kBlock, o = id % kBlock;
+      const int n = id / FACES, o = id % FACES;
       double s[5];
-      tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o, yb0), i0, j0, n, true, s);
+      if constexpr (kAll)
+        tile_transverse<DIR>(s_tile, TL::x(o), TL::y(o, yb0), i0, j0, n, true, s);
+      else
+        global_transverse<DIR>(fl, fr, nx, (int)blockIdx.x * FACES + o, (int)blockIdx.y + yb0, n, true, s);
       double a0, a1, a2;
       sr_betas<M>(s, P, a0, a1, a2);
       s_g[0][n][o] = sr_value<M>(s, 2, a0, a1, a2, opts, tally);

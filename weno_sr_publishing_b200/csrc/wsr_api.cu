@@ -181,144 +181,131 @@ typename ClosureParams<M>::type stage_params(const wsr_ctx* ctx, const StageArgs
     return params_of<M>(ctx);
 }
 
+// ---- the five launches of a stage, whole or in row bands ---------------------------------------------------
+// Two forms of the reconstruction kernels: 128 faces per block (one per thread), and on small grids 16 faces per
+// block whose closure queue all 128 threads share (the FACES template argument of k_normal and k_flux).
+// Interior cells up to which the 16-face form is the SR default: SR-FP32 / SR-FP64 steps at 100^2 226 -> 154 / 713
+// -> 273 us, at 200^2 292 -> 264 / 774 -> 618 us, at 400^2 531 -> 651 / 1427 -> 1619 us (one thread -> eight threads
+// per face, seeded quadrant state).
+constexpr long long kSmallCells = 256LL * 256;
+
 template <int M>
-int launch_stage(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st) {
-  const auto P = stage_params<M>(ctx, a);
-  const dim3 blk(128);  // the reconstruction kernels compact closure work per warp of a 128-thread block
-  {
-    ProfScope ps(ctx, st, 0);
-    dim3 grd((a.nx + 1 + 127) / 128, a.ny + 5);
-    k_normal<M, 1><<<grd, blk, 0, st>>>(a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks,
-                                        w.counters + 0, P, 0);
-  }
-  WSR_LAUNCHED(ctx, "k_normal<x>");
-  {
-    ProfScope ps(ctx, st, 1);
-    dim3 grd((a.nx + 5 + 31) / 32, (a.ny + 1 + 3) / 4);
-    k_normal<M, 2><<<grd, blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks,
-                                        w.counters + 2, P, 0);
-  }
-  WSR_LAUNCHED(ctx, "k_normal<y>");
-  {
-    ProfScope ps(ctx, st, 2);
-    dim3 grd((a.nx + 1 + 31) / 32, (a.ny + 3) / 4);
-    k_flux<M, 1><<<grd, blk, 0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
-                                      w.counters + 4, P, fm.xl, fm.xr, 0);
-  }
-  WSR_LAUNCHED(ctx, "k_flux<x>");
-  {
-    ProfScope ps(ctx, st, 3);
-    dim3 grd((a.nx + 127) / 128, a.ny + 1);
-    k_flux<M, 2><<<grd, blk, 0, st>>>(w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
-                                      w.counters + 6, P, fm.yl, fm.yr, 0);
-  }
-  WSR_LAUNCHED(ctx, "k_flux<y>");
-  {
-    ProfScope ps(ctx, st, 4);
-    dim3 grd((a.nx + 255) / 256, a.ny);
-    k_update<<<grd, 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx, a.ny, a.rk, a.g, w.ctl, 0);
-  }
-  WSR_LAUNCHED(ctx, "k_update");
-  return WSR_OK;
-}
-
-int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st) {
-  switch (method) {
-    case WSR_METHOD_JS:
-      return launch_stage<M_JS>(ctx, a, w, fm, st);
-    case WSR_METHOD_SR_F64:
-      return launch_stage<M_SR64>(ctx, a, w, fm, st);
-    case WSR_METHOD_SR_F32:
-      return launch_stage<M_SR32>(ctx, a, w, fm, st);
-    case WSR_METHOD_Z:
-      return launch_stage<M_Z>(ctx, a, w, fm, st);
-    case WSR_METHOD_SR_BF16_TC:
-      return launch_stage<M_SRBF16_TC>(ctx, a, w, fm, st);
-    default:
-      return launch_stage<M_SRBF16>(ctx, a, w, fm, st);
+bool small_form(const StageArgs& a) {
+  if constexpr (M == M_SRBF16_TC || !has_mlp<M>()) {
+    // The tensor-core closure works on whole warps of queued stencils. JS and WENO-Z have no closure queue, so the
+    // small form gains them little, and their candidate arithmetic, once the side is not a compile-time constant,
+    // compiles to differently rounded multiply-adds: 128-face form only.
+    return false;
+  } else {
+    if (a.opts & WSR_OPT_FACE_THREADS_1) return false;
+    if (a.opts & WSR_OPT_FACE_THREADS_8) return true;
+    return (long long)a.nx * a.ny <= kSmallCells;
   }
 }
 
-// ---- a stage in row bands ----------------------------------------------------------------------------------
-// Block rows of a stage's five launches, each in its kernel's own unit: normal x (1 padded row), normal y (4 face
-// rows), flux x (4 face rows), flux y (1 face row), update (1 interior row). A stage can be issued in pieces:
-// every launch covers the block rows from what was issued before up to a target, so no row is computed twice.
+// Block rows of a stage's five launches, each in its kernel's own unit: normal x (1 padded row), normal y (g.ny
+// face rows), flux x (g.fx face rows), flux y (1 face row), update (1 interior row); g is 4 and 4 for the
+// 128-face form (32 x 4 tiles), 1 and 1 for the 16-face form. A stage can be issued in pieces: every launch covers
+// the block rows from what was issued before up to a target, so no row is computed twice.
 struct Rows5 {
   int nx, ny, fx, fy, up;
 };
+struct Gran {
+  int ny, fx;
+};
+inline Gran gran_of(bool small) { return small ? Gran{1, 1} : Gran{4, 4}; }
 
-inline Rows5 rows_total(int ny) { return Rows5{ny + 5, (ny + 4) / 4, (ny + 3) / 4, ny + 1, ny}; }
+inline Rows5 rows_total(int ny, Gran g) {
+  return Rows5{ny + 5, (ny + 1 + g.ny - 1) / g.ny, (ny + g.fx - 1) / g.fx, ny + 1, ny};
+}
 
 // What update rows [0, U) need from the other four launches when the whole stage input is present: flux x face
 // rows < U, flux y face rows <= U, the normal y face rows that flux y reads, and normal x rows up to 5 past the
 // last flux x face row (its transverse stencils).
-inline Rows5 rows_for_update(int ny, int U) {
-  const Rows5 T = rows_total(ny);
+inline Rows5 rows_for_update(int ny, int U, Gran g) {
+  const Rows5 T = rows_total(ny, g);
   Rows5 r;
   r.up = U;
-  r.fx = std::min(T.fx, (U + 3) / 4);
+  r.fx = std::min(T.fx, (U + g.fx - 1) / g.fx);
   r.fy = std::min(T.fy, U + 1);
-  r.ny = std::min(T.ny, (r.fy + 3) / 4);
-  r.nx = std::min(T.nx, 4 * r.fx + 5);
+  r.ny = std::min(T.ny, (r.fy + g.ny - 1) / g.ny);
+  r.nx = std::min(T.nx, g.fx * r.fx + 5);
   return r;
 }
 
 // What the first A interior rows of a stage input allow of the two normal reconstructions under the transmissive
 // boundary (ghost row p reads interior row clamp(p - 3, 0, ny - 1)): normal x row r reads padded row r, so
-// r < A + 3; normal y face row r reads padded rows r .. r + 5, so a block of 4 needs its last row r + 2 < A.
-inline Rows5 normals_for_rows(int ny, int A, Rows5 done) {
-  const Rows5 T = rows_total(ny);
+// r < A + 3; normal y face row r reads padded rows r .. r + 5, so a block of rows needs its last row r + 2 < A.
+inline Rows5 normals_for_rows(int ny, int A, Rows5 done, Gran g) {
+  const Rows5 T = rows_total(ny, g);
   Rows5 r = done;
   if (A >= ny) {
     r.nx = T.nx;
     r.ny = T.ny;
   } else {
     r.nx = std::max(done.nx, std::min(T.nx, A + 3));
-    r.ny = std::max(done.ny, std::min(T.ny, A >= 2 ? (A - 2) / 4 : 0));
+    r.ny = std::max(done.ny, std::min(T.ny, A >= 2 ? (A - 2) / g.ny : 0));
   }
   return r;
+}
+
+template <int M, int FACES>
+int launch_rows_form(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st,
+                     Rows5& done, const Rows5& want) {
+  const auto P = stage_params<M>(ctx, a);
+  const dim3 blk(kBlock);
+  constexpr bool kAll = FACES == kBlock;
+  if (want.nx > done.nx) {
+    ProfScope ps(ctx, st, 0);
+    k_normal<M, 1, FACES><<<dim3((a.nx + 1 + FACES - 1) / FACES, want.nx - done.nx), blk, 0, st>>>(
+        a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P,
+        done.nx);
+  }
+  WSR_LAUNCHED(ctx, "k_normal<x>");
+  done.nx = std::max(done.nx, want.nx);
+  if (want.ny > done.ny) {
+    ProfScope ps(ctx, st, 1);
+    k_normal<M, 2, FACES><<<dim3(kAll ? (a.nx + 5 + 31) / 32 : (a.nx + 5 + FACES - 1) / FACES, want.ny - done.ny),
+                            blk, 0, st>>>(a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts,
+                                          w.fallbacks, w.counters + 2, P, done.ny);
+  }
+  WSR_LAUNCHED(ctx, "k_normal<y>");
+  done.ny = std::max(done.ny, want.ny);
+  if (want.fx > done.fx) {
+    ProfScope ps(ctx, st, 2);
+    k_flux<M, 1, FACES><<<dim3(kAll ? (a.nx + 1 + 31) / 32 : (a.nx + 1 + FACES - 1) / FACES, want.fx - done.fx), blk,
+                          0, st>>>(w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks,
+                                   w.counters + 4, P, fm.xl, fm.xr, done.fx);
+  }
+  WSR_LAUNCHED(ctx, "k_flux<x>");
+  done.fx = std::max(done.fx, want.fx);
+  if (want.fy > done.fy) {
+    ProfScope ps(ctx, st, 3);
+    k_flux<M, 2, FACES><<<dim3((a.nx + FACES - 1) / FACES, want.fy - done.fy), blk, 0, st>>>(
+        w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P, fm.yl,
+        fm.yr, done.fy);
+  }
+  WSR_LAUNCHED(ctx, "k_flux<y>");
+  done.fy = std::max(done.fy, want.fy);
+  if (want.up > done.up) {
+    ProfScope ps(ctx, st, 4);
+    k_update<<<dim3((a.nx + 255) / 256, want.up - done.up), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx,
+                                                                          a.ny, a.rk, a.g, w.ctl, done.up);
+  }
+  WSR_LAUNCHED(ctx, "k_update");
+  done.up = std::max(done.up, want.up);
+  return WSR_OK;
 }
 
 template <int M>
 int launch_rows(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st, Rows5& done,
                 const Rows5& want) {
-  const auto P = stage_params<M>(ctx, a);
-  const dim3 blk(128);
-  if (want.nx > done.nx) {
-    k_normal<M, 1><<<dim3((a.nx + 1 + 127) / 128, want.nx - done.nx), blk, 0, st>>>(
-        a.u_stage, w.xl, w.xr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 0, P,
-        done.nx);
-    WSR_LAUNCHED(ctx, "k_normal<x>");
-    done.nx = want.nx;
+  if constexpr (M == M_SRBF16_TC) {
+    return launch_rows_form<M, kBlock>(ctx, a, w, fm, st, done, want);
+  } else {
+    if (small_form<M>(a)) return launch_rows_form<M, kSmallFaces>(ctx, a, w, fm, st, done, want);
+    return launch_rows_form<M, kBlock>(ctx, a, w, fm, st, done, want);
   }
-  if (want.ny > done.ny) {
-    k_normal<M, 2><<<dim3((a.nx + 5 + 31) / 32, want.ny - done.ny), blk, 0, st>>>(
-        a.u_stage, w.yl, w.yr, a.nx, a.ny, stage_bc(a), make_gas(a.g), w.ctl, a.opts, w.fallbacks, w.counters + 2, P,
-        done.ny);
-    WSR_LAUNCHED(ctx, "k_normal<y>");
-    done.ny = want.ny;
-  }
-  if (want.fx > done.fx) {
-    k_flux<M, 1><<<dim3((a.nx + 1 + 31) / 32, want.fx - done.fx), blk, 0, st>>>(
-        w.xl, w.xr, w.fx, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 4, P, fm.xl,
-        fm.xr, done.fx);
-    WSR_LAUNCHED(ctx, "k_flux<x>");
-    done.fx = want.fx;
-  }
-  if (want.fy > done.fy) {
-    k_flux<M, 2><<<dim3((a.nx + 127) / 128, want.fy - done.fy), blk, 0, st>>>(
-        w.yl, w.yr, w.fy, a.nx, a.ny, make_gas(a.g), a.flux, w.ctl, a.opts, w.fallbacks, w.counters + 6, P, fm.yl,
-        fm.yr, done.fy);
-    WSR_LAUNCHED(ctx, "k_flux<y>");
-    done.fy = want.fy;
-  }
-  if (want.up > done.up) {
-    k_update<<<dim3((a.nx + 255) / 256, want.up - done.up), 256, 0, st>>>(a.u_stage, a.u0, a.u_out, w.fx, w.fy, a.nx,
-                                                                          a.ny, a.rk, a.g, w.ctl, done.up);
-    WSR_LAUNCHED(ctx, "k_update");
-    done.up = want.up;
-  }
-  return WSR_OK;
 }
 
 int dispatch_rows(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st,
@@ -337,6 +324,30 @@ int dispatch_rows(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, c
     default:
       return launch_rows<M_SRBF16>(ctx, a, w, fm, st, done, want);
   }
+}
+
+// The row granularity the stage's launches use (which form dispatch_rows picks).
+Gran stage_gran(int method, const StageArgs& a) {
+  switch (method) {
+    case WSR_METHOD_JS:
+      return gran_of(small_form<M_JS>(a));
+    case WSR_METHOD_SR_F64:
+      return gran_of(small_form<M_SR64>(a));
+    case WSR_METHOD_SR_F32:
+      return gran_of(small_form<M_SR32>(a));
+    case WSR_METHOD_Z:
+      return gran_of(small_form<M_Z>(a));
+    case WSR_METHOD_SR_BF16_TC:
+      return gran_of(false);
+    default:
+      return gran_of(small_form<M_SRBF16>(a));
+  }
+}
+
+// One whole stage.
+int dispatch_stage(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st) {
+  Rows5 done{0, 0, 0, 0, 0};
+  return dispatch_rows(ctx, method, a, w, fm, st, done, rows_total(a.ny, stage_gran(method, a)));
 }
 
 // Accumulates a host-buffer call's outcome for wsr_euler2d_host_wait: [0] stencil tile loads that timed out,
@@ -721,6 +732,7 @@ int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], i
     const StageArgs a1{in, in, u[1], nx, ny, bc, flux, opts, 1, dx, dy, gamma, 0.0};
     const StageArgs a2{u[1], in, u[2], nx, ny, bc, flux, opts, 2, dx, dy, gamma, 1.0};
     const StageArgs a3{u[2], in, out, nx, ny, bc, flux, opts, 3, dx, dy, gamma, 0.5};
+    const Gran g = stage_gran(method, a1);
     Rows5 done{0, 0, 0, 0, 0};
     if (s == 0) {
       for (int k = 0; k < nb; ++k) {
@@ -728,21 +740,21 @@ int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], i
         WSR_CUDA(ctx, cudaStreamWaitEvent(st, p->up[k], 0));
         k_max_speed<<<dim3((nx + 255) / 256, r1 - r0), 256, 0, st>>>(u[0], nx, ny, gamma, &w.ctl->max_speed_bits, r0);
         WSR_LAUNCHED(ctx, "k_max_speed");
-        if (overlap && (rc = dispatch_rows(ctx, method, a1, w, fm, st, done, normals_for_rows(ny, r1, done))))
+        if (overlap && (rc = dispatch_rows(ctx, method, a1, w, fm, st, done, normals_for_rows(ny, r1, done, g))))
           return rc;
       }
     }
     k_step_begin_ring<<<1, 1, 0, st>>>(w.ctl, w.dts);
     k_set_dt_ratios<<<1, 1, 0, st>>>(w.ctl, dx, dy);
     WSR_LAUNCHED(ctx, "k_step_begin");
-    if ((rc = dispatch_rows(ctx, method, a1, w, fm, st, done, rows_total(ny)))) return rc;
+    if ((rc = dispatch_rows(ctx, method, a1, w, fm, st, done, rows_total(ny, g)))) return rc;
     if ((rc = dispatch_stage(ctx, method, a2, w, fm, st))) return rc;
     if (s == steps - 1) {
       // the last stage band by band, each band's read-back as soon as its rows are final
       Rows5 d3{0, 0, 0, 0, 0};
       for (int k = 0; k < nb; ++k) {
         const int r0 = band_lo(ny, nb, k), r1 = band_lo(ny, nb, k + 1);
-        if ((rc = dispatch_rows(ctx, method, a3, w, fm, st, d3, rows_for_update(ny, r1)))) return rc;
+        if ((rc = dispatch_rows(ctx, method, a3, w, fm, st, d3, rows_for_update(ny, r1, g)))) return rc;
         WSR_CUDA(ctx, cudaEventRecord(p->ready[k], st));
         WSR_CUDA(ctx, cudaStreamWaitEvent(p->d2h, p->ready[k], 0));
         WSR_CUDA(ctx, cudaMemcpy2DAsync(row_at(u_host, r0), pitch, row_at(out, r0), pitch, width, r1 - r0,
