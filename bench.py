@@ -1163,7 +1163,7 @@ def _closure_roofline(kernels, method, classes, ms, local, stream):
 
 # DRAM bytes (read + write) of one launch of the dominant kernel, from the ncu capture of the same workload
 # (kernel class, method, grid): the headline configuration only.
-NCU_TRAFFIC = {("flux_x", "sr_f32", 2000): 361.4e6, ("flux_x", "js", 2000): 360.2e6}
+NCU_TRAFFIC = {("flux_x", "sr_f32", 2000): 361.8e6, ("flux_x", "js", 2000): 360.6e6}
 
 
 def C_stream(stream):
