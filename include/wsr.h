@@ -73,11 +73,14 @@ extern "C" {
                                  usual. wsr_euler3d_run rejects it. */
 #define WSR_OPT_FACE_THREADS_8 32 /* 2D WENO5-SR stages (FP64, FP32, BF16 closures): eight threads per face in the
                                      two reconstruction kernels (16 faces per 128-thread block; each thread forms one
-                                     stencil and at most one closure evaluation) whatever the grid size; the default
-                                     picks this form for grids of at most 256 x 256 cells, where one thread per face
-                                     is latency bound by its serial closure evaluations. Same results bit for bit.
+                                     stencil and at most one closure evaluation) whatever the grid size. By default
+                                     SR stages use this form up to 128 x 128 cells, the four-thread form up to 256 x 256
+                                     and one thread per face above (where one thread per face is no longer latency
+                                     bound by its serial closure evaluations). Same results bit for bit in every form.
                                      JS, WENO-Z and the tensor-core closure always use one thread per face. */
 #define WSR_OPT_FACE_THREADS_1 64 /* 2D WENO5 stages: one thread per face whatever the grid size */
+#define WSR_OPT_FACE_THREADS_4 128 /* 2D WENO5-SR stages: four threads per face (32 faces per block, two stencils each)
+                                      whatever the grid size */
 
 typedef struct wsr_ctx wsr_ctx;
 

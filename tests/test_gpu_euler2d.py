@@ -284,12 +284,14 @@ def test_face_thread_layouts_agree_bitwise(method, bc, flux):
         p = Params(nx=nx, ny=ny, x_length=1.0, y_length=0.8, cfl=0.4)
         init = problems.make_quadrant_state(nx, ny, problems.seeded_quadrant_states(4), 3)
     out = {}
-    for layout in (N.OPT_FACE_THREADS_1, N.OPT_FACE_THREADS_8):
+    for layout in (N.OPT_FACE_THREADS_1, N.OPT_FACE_THREADS_8, N.OPT_FACE_THREADS_4):
         bufs = [_t(init)] + [torch.zeros_like(_t(init)) for _ in range(3)]
         ws = E.workspace(nx, ny, DEV)
         res = E.run(bufs, p, 1.0, method, bc, mlp_params=PARAMS[method], flux=flux, fixed_steps=4,
                     opts=layout | N.OPT_COUNT | N.OPT_JS_FALLBACK, ws=ws)
         out[layout] = (bufs[res.final_slot].cpu().numpy(), res.dts, E.counters(ws), res.fallbacks)
-    a, b = out[N.OPT_FACE_THREADS_1], out[N.OPT_FACE_THREADS_8]
-    np.testing.assert_array_equal(_interior(a[0], nx, ny), _interior(b[0], nx, ny))
-    assert a[1] == b[1] and a[2] == b[2] and a[3] == b[3]
+    a = out[N.OPT_FACE_THREADS_1]
+    for layout in (N.OPT_FACE_THREADS_8, N.OPT_FACE_THREADS_4):
+        b = out[layout]
+        np.testing.assert_array_equal(_interior(a[0], nx, ny), _interior(b[0], nx, ny))
+        assert a[1] == b[1] and a[2] == b[2] and a[3] == b[3]

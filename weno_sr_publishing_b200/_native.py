@@ -24,7 +24,7 @@ FLUX = {"hllc": 0, "force": 1}
 HOST_ASYNC = 1  # wsr_euler2d_advance_host: return once queued
 FLUX3 = {"evilin": 0, "hllc": 1}
 OPT_ENO_CUTOFF, OPT_JS_FALLBACK, OPT_COUNT, OPT_Z_HALO = 1, 2, 4, 8
-OPT_FACE_THREADS_8, OPT_FACE_THREADS_1 = 32, 64  # 2D reconstruction kernels: 8 threads or 1 thread per face
+OPT_FACE_THREADS_8, OPT_FACE_THREADS_1, OPT_FACE_THREADS_4 = 32, 64, 128  # 2D reconstruction kernels: threads per face
 PROF_KINDS = ("normal_x", "normal_y", "flux_x", "flux_y", "update", "control")
 N_PARAMS5 = 189
 PARAM_NAMES = ("w1", "b1", "w2", "b2", "w3", "b3", "w4", "b4")

@@ -189,7 +189,7 @@ __device__ __forceinline__ void queue_push(bool need, int id, unsigned short* q,
 // 8 (on a small grid the one-face-per-thread launch is latency bound by that serial chain). The face arithmetic
 // is the same code either way.
 // -------------------------------------------------------------------------------------------
-constexpr int kSmallFaces = 16;  // faces per block of the small-grid form
+
 
 // Phase A of one characteristic stencil with its side (= head) a compile-time constant, as in the unrolled pairs of
 // the one-face-per-thread loop: the value at once, or true when the stencil needs the closure.
@@ -261,24 +261,30 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_normal(const double
   const bool work = active;
   __syncthreads();
   if constexpr (!kAll) {
-    // Phase A of the small-grid form: lane n of the 8 lanes of face t / 8 takes stencil n
+    // Phase A of the small-grid form: the kLanes lanes of face t / kLanes take its 8 stencils in turn (lane l:
+    // stencils l, l + kLanes, ...; kLanes is even, so a lane keeps one side)
     constexpr int kLanes = kBlock / FACES;
-    const int face = t / kLanes, n = t % kLanes, f = n >> 1, side = n & 1;
+    static_assert(kLanes % 2 == 0 && kStencilsPerThread % kLanes == 0, "lanes per face must be 2, 4 or 8");
+    const int face = t / kLanes, lane = t % kLanes, side = lane & 1;
     const int fc = (int)blockIdx.x * FACES + face;
     const bool live = DIR == 1 ? (r >= 1 && r < ny + 5 && fc <= nx) : (r <= ny && fc >= 1 && fc < nx + 5);
-    bool need = false;
-    if (live) {
-      double s[5];
+#pragma unroll 1
+    for (int n = lane; n < kStencilsPerThread; n += kLanes) {
+      const int f = n >> 1;
+      bool need = false;
+      if (live) {
+        double s[5];
 #pragma unroll
-      for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][face];
-      double v = 0.0;
-      if (side == 0)
-        need = normal_stencil_a<M, DIR, 0>(s, P, v, tally);
-      else
-        need = normal_stencil_a<M, DIR, 1>(s, P, v, tally);
-      if (!need) s_val[n][face] = v;
+        for (int k = 0; k < 5; ++k) s[k] = s_ch[f][k + side][face];
+        double v = 0.0;
+        if (side == 0)
+          need = normal_stencil_a<M, DIR, 0>(s, P, v, tally);
+        else
+          need = normal_stencil_a<M, DIR, 1>(s, P, v, tally);
+        if (!need) s_val[n][face] = v;
+      }
+      if constexpr (has_mlp<M>()) queue_push(need, n * FACES + face, s_q, &s_count);
     }
-    if constexpr (has_mlp<M>()) queue_push(need, n * FACES + face, s_q, &s_count);
   }
   // Phase A, two stencils per iteration (two independent dependency chains; unrolling by 4 or 8 spills)
 #pragma unroll 2
@@ -577,19 +583,24 @@ __global__ void __launch_bounds__(kBlock, min_blocks<M>()) k_flux(const double* 
   const bool work = active;
   // Phase A of the small-grid form: lane n of the 8 lanes of face t / 8 takes stencil n
   if constexpr (!kAll) {
+    // the kLanes lanes of face t / kLanes take its 8 stencils in turn
     constexpr int kLanes = kBlock / FACES;
-    const int face = t / kLanes, n = t % kLanes;
+    static_assert(kStencilsPerThread % kLanes == 0, "lanes per face must divide 8");
+    const int face = t / kLanes, lane = t % kLanes;
     const int fi = (int)blockIdx.x * FACES + face;
     const bool live = fi < nfx && j < nfy;
-    double s[5];
-    global_transverse<DIR>(fl, fr, nx, fi, j, n, live, s);
-    double g0 = 0.0, g1 = 0.0;
-    const bool need = live && flux_stencil_a<M, DIR>(s, P, g0, g1, tally);
-    if (live && !need) {
-      s_g[0][n][face] = g0;
-      s_g[1][n][face] = g1;
+#pragma unroll 1
+    for (int n = lane; n < kStencilsPerThread; n += kLanes) {
+      double s[5];
+      global_transverse<DIR>(fl, fr, nx, fi, j, n, live, s);
+      double g0 = 0.0, g1 = 0.0;
+      const bool need = live && flux_stencil_a<M, DIR>(s, P, g0, g1, tally);
+      if (live && !need) {
+        s_g[0][n][face] = g0;
+        s_g[1][n][face] = g1;
+      }
+      if constexpr (has_mlp<M>()) queue_push(need, n * FACES + face, s_q, &s_count);
     }
-    if constexpr (has_mlp<M>()) queue_push(need, n * FACES + face, s_q, &s_count);
   }
   // Phase A, two stencils per iteration. Stencil n = 2 comp + side: side 0 -> u_R (lr=2 faces fl), side 1 -> u_L
   // (lr=1 faces fr).

@@ -184,22 +184,27 @@ typename ClosureParams<M>::type stage_params(const wsr_ctx* ctx, const StageArgs
 // ---- the five launches of a stage, whole or in row bands ---------------------------------------------------
 // Two forms of the reconstruction kernels: 128 faces per block (one per thread), and on small grids 16 faces per
 // block whose closure queue all 128 threads share (the FACES template argument of k_normal and k_flux).
-// Interior cells up to which the 16-face form is the SR default: SR-FP32 / SR-FP64 steps at 100^2 226 -> 154 / 713
-// -> 273 us, at 200^2 292 -> 264 / 774 -> 618 us, at 400^2 531 -> 651 / 1427 -> 1619 us (one thread -> eight threads
-// per face, seeded quadrant state).
-constexpr long long kSmallCells = 256LL * 256;
+// Faces per block of the small-grid forms by grid size (SR methods). Measured per step, seeded quadrant state, one
+// thread per face / 16 / 32 / 64 faces per block, SR-FP32 (SR-FP64) in us: 100^2 227 / 149 / 159 / 193 (717 / 270 /
+// 326 / 488); 200^2 288 / 259 / 235 / 304 (774 / 616 / 625 / 693); 300^2 359 / 431 / 359 / 365 (1028 / 1069 / 990 /
+// 969); 400^2 527 / 643 / 495 / 482 (1422 / 1617 / 1472 / 1433).
+constexpr long long kSmall16Cells = 128LL * 128;
+constexpr long long kSmall32Cells = 256LL * 256;
 
+// 0 for the one-face-per-thread form, else the faces per block of the small-grid form.
 template <int M>
-bool small_form(const StageArgs& a) {
+int small_faces(const StageArgs& a) {
   if constexpr (M == M_SRBF16_TC || !has_mlp<M>()) {
     // The tensor-core closure works on whole warps of queued stencils. JS and WENO-Z have no closure queue, so the
-    // small form gains them little, and their candidate arithmetic, once the side is not a compile-time constant,
-    // compiles to differently rounded multiply-adds: 128-face form only.
-    return false;
+    // small forms gain them little, and their candidate arithmetic, once the side is not a compile-time constant,
+    // compiles to differently rounded multiply-adds: one face per thread only.
+    return 0;
   } else {
-    if (a.opts & WSR_OPT_FACE_THREADS_1) return false;
-    if (a.opts & WSR_OPT_FACE_THREADS_8) return true;
-    return (long long)a.nx * a.ny <= kSmallCells;
+    if (a.opts & WSR_OPT_FACE_THREADS_1) return 0;
+    if (a.opts & WSR_OPT_FACE_THREADS_8) return 16;
+    if (a.opts & WSR_OPT_FACE_THREADS_4) return 32;
+    const long long cells = (long long)a.nx * a.ny;
+    return cells <= kSmall16Cells ? 16 : (cells <= kSmall32Cells ? 32 : 0);
   }
 }
 
@@ -300,10 +305,12 @@ int launch_rows_form(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const Face
 template <int M>
 int launch_rows(wsr_ctx* ctx, const StageArgs& a, const Ws2d& w, const FaceMaps& fm, cudaStream_t st, Rows5& done,
                 const Rows5& want) {
-  if constexpr (M == M_SRBF16_TC) {
+  if constexpr (M == M_SRBF16_TC || !has_mlp<M>()) {
     return launch_rows_form<M, kBlock>(ctx, a, w, fm, st, done, want);
   } else {
-    if (small_form<M>(a)) return launch_rows_form<M, kSmallFaces>(ctx, a, w, fm, st, done, want);
+    const int faces = small_faces<M>(a);
+    if (faces == 16) return launch_rows_form<M, 16>(ctx, a, w, fm, st, done, want);
+    if (faces == 32) return launch_rows_form<M, 32>(ctx, a, w, fm, st, done, want);
     return launch_rows_form<M, kBlock>(ctx, a, w, fm, st, done, want);
   }
 }
@@ -330,17 +337,17 @@ int dispatch_rows(wsr_ctx* ctx, int method, const StageArgs& a, const Ws2d& w, c
 Gran stage_gran(int method, const StageArgs& a) {
   switch (method) {
     case WSR_METHOD_JS:
-      return gran_of(small_form<M_JS>(a));
+      return gran_of(small_faces<M_JS>(a) != 0);
     case WSR_METHOD_SR_F64:
-      return gran_of(small_form<M_SR64>(a));
+      return gran_of(small_faces<M_SR64>(a) != 0);
     case WSR_METHOD_SR_F32:
-      return gran_of(small_form<M_SR32>(a));
+      return gran_of(small_faces<M_SR32>(a) != 0);
     case WSR_METHOD_Z:
-      return gran_of(small_form<M_Z>(a));
+      return gran_of(small_faces<M_Z>(a) != 0);
     case WSR_METHOD_SR_BF16_TC:
       return gran_of(false);
     default:
-      return gran_of(small_form<M_SRBF16>(a));
+      return gran_of(small_faces<M_SRBF16>(a) != 0);
   }
 }
 
