@@ -167,7 +167,7 @@ int wsr_euler2d_run(wsr_ctx *ctx, double *const u[4], int nx, int ny, double dx,
  * Copies the interior of u_host (a padded [ny+6][nx+6][4] HOST array; pinned memory for overlap) into u[0],
  * advances `steps` full CFL steps exactly as wsr_euler2d_run with fixed_steps does (same buffers, same results bit
  * for bit), and copies the result's interior back into u_host; the ghost cells of u_host are not touched. The
- * copies run on the context's own copy streams in `bands` row bands (0: one per 280 rows, at most 16; pageable
+ * copies run on the context's own copy streams in `bands` row bands (0: one per 250 rows, at most 16; the first and last half as high; pageable
  * memory: one band):
  *   - the first stage's wave speed and, under WSR_BC_TRANSMISSIVE, its normal reconstructions start on each
  *     band as it arrives;

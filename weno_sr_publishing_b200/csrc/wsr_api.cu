@@ -475,8 +475,16 @@ int make_pipe(wsr_ctx* ctx) {
   return WSR_OK;
 }
 
-// Interior rows [band_lo(k), band_lo(k + 1)) of band k of nb.
-inline int band_lo(int ny, int nb, int k) { return (int)((long long)ny * k / nb); }
+// Interior rows [band_lo(k), band_lo(k + 1)) of band k of nb. The first and last bands are half as high as the
+// others (nb > 2): the first read-back starts sooner and the last upload ends sooner (at 2000^2 on the benchmark
+// state 6.30-6.33 ms per call with 8 such bands against 6.36-6.37 with 7 equal ones). nb <= ny / 2 + 1 keeps every
+// band at least one row high.
+inline int band_lo(int ny, int nb, int k) {
+  if (k <= 0) return 0;
+  if (k >= nb) return ny;
+  if (nb <= 2) return (int)((long long)ny * k / nb);
+  return (int)(((double)k - 0.5) / (double)(nb - 1) * (double)ny);
+}
 
 }  // namespace
 
@@ -699,10 +707,10 @@ int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], i
   cudaPointerAttributes attr;
   WSR_CUDA(ctx, cudaPointerGetAttributes(&attr, u_host));
   // pageable memory copies synchronously: one band, no overlap
-  // one band per 280 rows: on the 2000^2 benchmark state 4 / 7 / 10 / 14 / 20 bands took 7.01 / 6.70 / 6.74 / 7.15 /
-  // 7.42 ms per call (more bands start the copies sooner but cut the heavy stage kernels into more tails)
-  int nb = bands > 0 ? bands : ny / 280;
-  nb = attr.type == cudaMemoryTypeHost ? std::max(1, std::min(std::min(nb, kHostBandsMax), ny)) : 1;
+  // one band per 250 rows: on the 2000^2 benchmark state 4 / 7 / 10 / 14 / 20 equal bands took 7.01 / 6.70 / 6.74 /
+  // 7.15 / 7.42 ms per call (more bands start the copies sooner but cut the heavy stage kernels into more tails)
+  int nb = bands > 0 ? bands : ny / 250;
+  nb = attr.type == cudaMemoryTypeHost ? std::max(1, std::min(std::min(nb, kHostBandsMax), ny / 2 + 1)) : 1;
   Ws2d w = carve(workspace, nx, ny);
   FaceMaps fm;
   if (!face_maps(w, nx, ny, &fm)) return fail(ctx, WSR_ERR_CUDA, "encoding the face-value tensor maps failed");

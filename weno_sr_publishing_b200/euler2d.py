@@ -165,7 +165,7 @@ def advance_host(u_host, params: Params, steps: int, method: str, boundary: str,
     the result. With async_readback=True (pinned host memory) it returns once queued: consecutive calls on the
     same host array and `bufs` then overlap both copy directions with the computation, and u_host is complete
     after host_copies_done() (which orders the current stream after the read-backs) and a synchronisation, or
-    after host_wait(). bands: 0 picks one band per 280 rows (at most 16)."""
+    after host_wait(). bands: 0 picks one band per 250 rows (at most 16; the first and last are half as high)."""
     dev = torch.device(device)
     if bufs is None:
         bufs = [torch.empty(params.padded_shape, dtype=torch.float64, device=dev) for _ in range(4)]
