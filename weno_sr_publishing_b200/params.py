@@ -31,26 +31,28 @@ class Params:
 
 
 def primitive_from_conserved(u: np.ndarray, gamma: float) -> np.ndarray:
-    """warp_weno5_helpers.py:167-172 (rho floored at 1e-15)."""
-    rho = np.maximum(u[..., 0], 1.0e-15)
-    vel_x = u[..., 1] / rho
-    vel_y = u[..., 2] / rho
-    p = (gamma - 1.0) * (u[..., 3] - 0.5 * rho * (vel_x * vel_x + vel_y * vel_y))
-    return np.stack([rho, vel_x, vel_y, p], axis=-1)
+    """Primitive (rho, u, v, p) of conserved (rho, rho u, rho v, E) cells, the density floored at 1e-15 before it
+    divides (the host-side decoding of warp_weno5_helpers.py:167-172, same operations in the same order)."""
+    cons = np.asarray(u, dtype=np.float64)
+    prim = np.empty(cons.shape[:-1] + (4,), dtype=np.float64)
+    rho = np.maximum(cons[..., 0], 1.0e-15, out=prim[..., 0])
+    vx = np.divide(cons[..., 1], rho, out=prim[..., 1])
+    vy = np.divide(cons[..., 2], rho, out=prim[..., 2])
+    prim[..., 3] = (gamma - 1.0) * (cons[..., 3] - 0.5 * rho * (vx * vx + vy * vy))
+    return prim
 
 
 def interior_stats(u_host: np.ndarray, params: Params) -> dict[str, float]:
-    """warp_weno5_helpers.py:210-224."""
-    gc = params.ghost
-    interior = u_host[gc: gc + params.ny, gc: gc + params.nx, :]
-    pri = primitive_from_conserved(interior, params.gamma)
-    return {
-        "mass": float(np.sum(interior[..., 0]) * params.dx * params.dy),
-        "rho_min": float(np.min(pri[..., 0])),
-        "rho_max": float(np.max(pri[..., 0])),
-        "p_min": float(np.min(pri[..., 3])),
-        "p_max": float(np.max(pri[..., 3])),
-        "nan_count": float(np.isnan(interior).sum()),
-        "rho_neg": float(np.sum(pri[..., 0] <= 0.0)),
-        "p_neg": float(np.sum(pri[..., 3] <= 0.0)),
-    }
+    """Health summary of the interior cells that the adapters report (warp_weno5_helpers.py:210-224): mass (the
+    raw density summed, times dx dy), the ranges of the floored density and of the pressure, the NaN count of the
+    conserved values, and the counts of non-positive (floored) densities and pressures."""
+    g = params.ghost
+    cells = u_host[g: g + params.ny, g: g + params.nx, :]
+    prim = primitive_from_conserved(cells, params.gamma)
+    rho, pres = prim[..., 0], prim[..., 3]
+    stats = {"mass": float(np.sum(cells[..., 0]) * params.dx * params.dy)}
+    stats.update(rho_min=float(rho.min()), rho_max=float(rho.max()), p_min=float(pres.min()), p_max=float(pres.max()))
+    stats["nan_count"] = float(np.count_nonzero(np.isnan(cells)))
+    stats["rho_neg"] = float(np.count_nonzero(rho <= 0.0))
+    stats["p_neg"] = float(np.count_nonzero(pres <= 0.0))
+    return stats
