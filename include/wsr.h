@@ -167,17 +167,18 @@ int wsr_euler2d_run(wsr_ctx *ctx, double *const u[4], int nx, int ny, double dx,
  * Copies the interior of u_host (a padded [ny+6][nx+6][4] HOST array; pinned memory for overlap) into u[0],
  * advances `steps` full CFL steps exactly as wsr_euler2d_run with fixed_steps does (same buffers, same results bit
  * for bit), and copies the result's interior back into u_host; the ghost cells of u_host are not touched. The
- * copies run on the context's own copy streams in `bands` row bands (0: one per 250 rows, at most 16; the first and last half as high; pageable
- * memory: one band):
+ * copies run on the context's own copy streams in `bands` row bands (0: one per 250 rows, at most 16, the first
+ * and last half as high; pageable memory: one band):
  *   - the first stage's wave speed and, under WSR_BC_TRANSMISSIVE, its normal reconstructions start on each
  *     band as it arrives;
  *   - the last stage runs band by band and each band's read-back starts as soon as its rows are final.
  * flags 0: returns when u_host holds the result. WSR_HOST_ASYNC: returns once everything is queued. A following
  * call on the same host array and device buffers uploads band k right after this call's read-back of band k, so
  * consecutive calls overlap both copy directions with the computation; between such calls u[0..3] belong to the
- * pipeline. wsr_euler2d_host_order makes `stream` wait for the read-backs; wsr_euler2d_host_wait synchronises,
- * reports the steps taken and JS fallbacks summed over the calls since the previous wait, and returns an error
- * that any of them met on the device. */
+ * pipeline (wsr_euler2d_stage(_at) and wsr_euler2d_run on the same context order their work after the read-backs
+ * still in flight, as wsr_euler2d_host_order does). wsr_euler2d_host_order makes `stream` wait for the read-backs;
+ * wsr_euler2d_host_wait synchronises, reports the steps taken and JS fallbacks summed over the calls since the
+ * previous wait, and returns an error that any of them met on the device. */
 #define WSR_HOST_ASYNC 1
 int wsr_euler2d_advance_host(wsr_ctx *ctx, double *u_host, double *const u[4], int nx, int ny, double dx, double dy,
                              double gamma, double cfl, int steps, int method, int bc, int flux, int opts, int flags,

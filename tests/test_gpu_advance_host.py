@@ -116,3 +116,18 @@ def test_invalid_host_arguments_raise():
         E.advance_host(np.zeros((5, 5, 4)), p, 1, "js", "transmissive", device=DEV)
     with pytest.raises(ValueError):
         E.advance_host(torch.as_tensor(init).clone(), p, 0, "js", "transmissive", device=DEV)
+
+
+def test_device_work_on_the_buffers_waits_for_the_read_back():
+    """An overlapped read-back of bufs[3] is still in flight when a device loop on the same buffers overwrites
+    bufs[3]: the loop is ordered after the read-back, so the host array holds the host-buffer call's result."""
+    p, init = _case(4)
+    want = _device_loop(p, init, 1)
+    host = torch.as_tensor(init).clone().pin_memory()
+    work = [torch.zeros(p.padded_shape, dtype=torch.float64, device=DEV) for _ in range(4)]
+    E.advance_host(host, p, 1, "sr_f32", "transmissive", mlp_params=MLP, bufs=work, device=DEV, async_readback=True)
+    other = problems.make_quadrant_state(p.nx, p.ny, problems.seeded_quadrant_states(5), 3)
+    work[0].copy_(torch.as_tensor(other, device=DEV))
+    E.run(work, p, 1.0e300, "sr_f32", "transmissive", mlp_params=MLP, fixed_steps=3)
+    E.host_wait(DEV)
+    np.testing.assert_array_equal(host.numpy()[3:-3, 3:-3], want)

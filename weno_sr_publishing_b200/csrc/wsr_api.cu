@@ -568,6 +568,7 @@ int wsr_euler2d_stage_at(wsr_ctx* ctx, const double* u_stage, const double* u0, 
   if (!(dt > 0.0) || !(dx > 0.0) || !(dy > 0.0)) return fail(ctx, WSR_ERR_ARG, "dt, dx, dy must be positive");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((rc = wsr_euler2d_host_order(ctx, stream))) return rc;  // after host-buffer read-backs still in flight
   Ws2d w = carve(workspace, nx, ny);
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, boundary_time, 1.0e300, dt, dx, dy, 0.0, 0.0, 0, 0, 1);
   WSR_LAUNCHED(ctx, "k_init_ctl");
@@ -625,6 +626,7 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   WSR_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((rc = wsr_euler2d_host_order(ctx, stream))) return rc;  // after host-buffer read-backs still in flight
   Ws2d w = carve(workspace, nx, ny);
   const double hmin = dx < dy ? dx : dy;
   k_init_ctl<<<1, 1, 0, st>>>(w.ctl, w.fallbacks, w.counters, fixed_steps > 0 ? 0.0 : t_start, t_end, 0.0, dx, dy, cfl, hmin,
