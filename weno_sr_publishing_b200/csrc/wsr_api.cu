@@ -688,9 +688,10 @@ int wsr_euler2d_run(wsr_ctx* ctx, double* const u[4], int nx, int ny, double dx,
   return WSR_OK;
 }
 
-int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], int nx, int ny, double dx, double dy,
-                             double gamma, double cfl, int steps, int method, int bc, int flux, int opts, int flags,
-                             int bands, void* workspace, size_t workspace_bytes, void* stream) {
+// Queues one host-buffer call (wsr_euler2d_advance_host); on success the call's copies and kernels are in flight.
+static int advance_host_enqueue(wsr_ctx* ctx, double* u_host, double* const u[4], int nx, int ny, double dx,
+                                double dy, double gamma, double cfl, int steps, int method, int bc, int flux, int opts,
+                                int flags, int bands, void* workspace, size_t workspace_bytes, void* stream) {
   int rc = check_2d(ctx, nx, ny, method, bc, flux, workspace, workspace_bytes);
   if (rc) return rc;
   if (bc & WSR_BC_Y_HALO) return fail(ctx, WSR_ERR_ARG, "WSR_BC_Y_HALO is for wsr_euler2d_stage");
@@ -794,6 +795,25 @@ int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], i
   p->ny = ny;
   p->nb = nb;
   p->pending = true;
+  return WSR_OK;
+}
+
+int wsr_euler2d_advance_host(wsr_ctx* ctx, double* u_host, double* const u[4], int nx, int ny, double dx, double dy,
+                             double gamma, double cfl, int steps, int method, int bc, int flux, int opts, int flags,
+                             int bands, void* workspace, size_t workspace_bytes, void* stream) {
+  const int rc = advance_host_enqueue(ctx, u_host, u, nx, ny, dx, dy, gamma, cfl, steps, method, bc, flux, opts, flags,
+                                      bands, workspace, workspace_bytes, stream);
+  if (rc != WSR_OK) {
+    // copies of this call may already be queued: let them finish before the caller can release u_host, and start
+    // the next call afresh
+    if (ctx && ctx->host) {
+      cudaStreamSynchronize(ctx->host->h2d);
+      cudaStreamSynchronize(ctx->host->d2h);
+      ctx->host->pending = false;
+      ctx->host->host = nullptr;
+    }
+    return rc;
+  }
   if (flags & WSR_HOST_ASYNC) return WSR_OK;
   return wsr_euler2d_host_wait(ctx, nullptr, nullptr);
 }
