@@ -708,13 +708,14 @@ def bench_1d(args, world, rank, local):
         t0 = time.perf_counter()
         for _ in range(K):
             outs, _ = A1.run_batched(states, vel, 1.0 / ns, steps, 0.5 / ns, scheme=args.scheme, model=closure,
-                                     integrator=integ_name, device=dev)
-            host = [o.cpu() for o in outs]
+                                     integrator=integ_name, device=dev, to_host=True)
         el = time.perf_counter() - t0
         nbytes = int(np.sum(ns)) * 8
         el = max_over_ranks(el * 1e3) * 1e-3
         line["e2e"] = {"value": total * K / el, "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
-                       "d2h_bytes_per_step": nbytes, "api": "weno_sr_publishing_b200.adv1d.run_batched (host arrays)"}
+                       "d2h_bytes_per_step": nbytes,
+                       "api": "weno_sr_publishing_b200.adv1d.run_batched (host arrays in, to_host=True: one upload and "
+                              "one read-back of the whole batch)"}
         peak = ctx.peak_tflops(32 if method in ("sr_f32", "sr_bf16") else 64, C_stream(stream))
         line["roofline"] = _roofline_1d(args.scheme, method, work, mlp_n, plat_n, ms / K, peak, ctx, stream)
         if rank == 0 and world == 1:

@@ -170,3 +170,16 @@ def test_weno_z_ragged_batch_matches_oracle(scheme, integ):
         dts = [dtf[b]] * nf[b] + ([dtl[b]] if dtl[b] > 0 else [])
         ref = A.run(u, vel[b], dx[b], dts, scheme, "z", integ)
         assert _rel(outs[b].cpu().numpy(), ref) <= TOL["js"], b
+
+
+def test_host_batch_in_and_out_in_one_copy():
+    """Host rows (numpy and CPU tensors) go up in one copy; to_host=True returns numpy views of one read-back, equal to
+    the device results."""
+    states, vel, dx, nf, dtf, dtl = _ragged(7, 5)
+    dev_out, _ = D.run_batched(states, vel, dx, nf, dtf, dtl, scheme=5, model=MODEL5["sr_f32"], device=DEV)
+    mixed = [torch.as_tensor(s) if b % 2 else s for b, s in enumerate(states)]
+    host_out, _ = D.run_batched(mixed, vel, dx, nf, dtf, dtl, scheme=5, model=MODEL5["sr_f32"], device=DEV,
+                                to_host=True)
+    assert all(isinstance(h, np.ndarray) for h in host_out)
+    for d, h in zip(dev_out, host_out):
+        np.testing.assert_array_equal(d.cpu().numpy(), h)

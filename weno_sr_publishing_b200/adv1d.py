@@ -95,11 +95,12 @@ def _workspace(device):
 
 
 def run_batched(states, velocities, dx, n_full, dt_full, dt_last=None, *, scheme: int = 5, model="classical",
-                integrator: str = "ssprk3", device="cuda", opts: int = 0, count: bool = False):
-    """Advance ragged periodic trajectories; returns (list of final states as float64 tensors, info).
+                integrator: str = "ssprk3", device="cuda", opts: int = 0, count: bool = False, to_host: bool = False):
+    """Advance ragged periodic trajectories; returns (list of final states, info): float64 device tensors, or with
+    to_host=True float64 numpy arrays (one read-back of the whole batch, each array a view of it).
 
-    states: list of 1D arrays/tensors (n_b cells each); velocities, dx, dt_full, dt_last: per trajectory;
-    n_full: full steps per trajectory (then one step of dt_last[b] when it is > 0)."""
+    states: list of 1D arrays/tensors (n_b cells each; host arrays go up in one copy); velocities, dx, dt_full,
+    dt_last: per trajectory; n_full: full steps per trajectory (then one step of dt_last[b] when it is > 0)."""
     dev = torch.device(device)
     if dev.type != "cuda":
         raise ValueError("the 1D path runs on CUDA devices only")
@@ -117,7 +118,12 @@ def run_batched(states, velocities, dx, n_full, dt_full, dt_last=None, *, scheme
     width = 5 if scheme == 5 else 7
     if min(lens) < width or max(lens) > NMAX:
         raise ValueError(f"every trajectory needs {width} <= n <= {NMAX} cells")
-    flat = torch.cat([torch.as_tensor(s, dtype=torch.float64).reshape(-1).to(dev) for s in states]).contiguous()
+    if any(isinstance(s, torch.Tensor) and s.is_cuda for s in states):
+        flat = torch.cat([torch.as_tensor(s, dtype=torch.float64).reshape(-1).to(dev) for s in states]).contiguous()
+    else:  # host rows: concatenated on the host, one upload
+        host_rows = [s.detach().numpy() if isinstance(s, torch.Tensor) else s for s in states]
+        flat = torch.from_numpy(np.concatenate([np.asarray(s, dtype=np.float64).reshape(-1) for s in host_rows]))
+        flat = flat.to(dev)
     offsets = torch.tensor(np.concatenate([[0], np.cumsum(lens)]), dtype=torch.int64, device=dev)
     vel = torch.as_tensor(np.asarray(velocities, dtype=np.float64).reshape(B), device=dev)
     dxs = torch.as_tensor(np.broadcast_to(np.asarray(dx, dtype=np.float64), (B,)).copy(), device=dev)
@@ -142,7 +148,12 @@ def run_batched(states, velocities, dx, n_full, dt_full, dt_last=None, *, scheme
         P(dxs.data_ptr()), P(nf_t.data_ptr()), P(dtf_t.data_ptr()), P(dtl_t.data_ptr()), B, max(lens), scheme,
         N.METHOD[method], INTEG[integrator], int(opts) | (N.OPT_COUNT if count else 0), C.byref(fb), C.byref(err),
         cnt, P(wptr), wbytes, stream))
-    outs = list(torch.split(flat, lens))
+    if to_host:
+        host = flat.cpu().numpy()
+        edges = np.concatenate([[0], np.cumsum(lens)])
+        outs = [host[edges[k]:edges[k + 1]] for k in range(B)]
+    else:
+        outs = list(torch.split(flat, lens))
     return outs, {"fallbacks": fb.value, "mlp": int(cnt[0]), "plateau": int(cnt[1])}
 
 
