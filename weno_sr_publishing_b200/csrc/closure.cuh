@@ -201,7 +201,7 @@ __device__ __forceinline__ double swish<double>(double z) {
 // FP32-closure transcendentals: 1 = hardware approximations (ex2.approx via __expf, rcp.approx via
 // __fdividef), 0 = the accurate expf/tanhf and IEEE division, 2 = exp on the FMA pipe (exp_fma) with a
 // Newton-refined reciprocal. Mode 1 keeps the end-of-run density L1 of the 2D quadrant problem within
-// 2.2e-9 of the FP64 closure (the north-star bound is 1e-8), so it is the default.
+// 2.2e-9 of the FP64 closure (the FP32 closure's precision bound is 1e-8), so it is the default.
 #ifndef WSR_SWISH_MODE
 #define WSR_SWISH_MODE 1
 #endif
