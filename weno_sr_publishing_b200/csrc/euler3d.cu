@@ -21,9 +21,11 @@
 //              cell's low-face (lr 2) and high-face (lr 1) states, 10 scalar closures;
 //   k3_trans   one thread per cell: the first transverse Gauss pass for both Gauss points of both normal
 //              arrays (the reference recomputes the first pass for each of the four flags; two of them are
-//              the same, so four arrays hold all that the flags need), 20 scalar closures;
+//              the same, so four arrays hold all that the flags need): 10 stencils, each read once and
+//              reconstructed at both Gauss points (one SR closure evaluation serves both), 20 values;
 //   k3_flux    one thread per face: the second transverse pass of the four Gauss points of both adjacent
-//              cells and the four face fluxes, summed in the reference's flag order and scaled by dt/h.
+//              cells (20 stencils, each giving two of the 40 values) and the four face fluxes, summed in the
+//              reference's flag order and scaled by dt/h.
 // k3_update applies the four-point flux difference of all three directions and, at the third stage, takes
 // the maximum wave speed for the next step's dt, which k3_step_begin turns into dt on the device.
 #include <cuda_runtime.h>
@@ -355,6 +357,30 @@ __device__ __forceinline__ double recon(const double q[5], int head, const typen
   }
 }
 
+// Both Gauss-point values (heads 2 and 3) of one transverse stencil. The SR closure's weights are a function of the
+// five stencil values alone, so one closure evaluation serves both heads (the reference evaluates it once per head,
+// with the same result); WENO5-JS and WENO-Z evaluate each head as a separate call, as the reference does.
+template <int M>
+__device__ __forceinline__ void recon_pair(const double q[5], const typename ClosureParams<M>::type& P, int opts,
+                                           Tally& tally, double& v2, double& v3) {
+  if constexpr (M == M_JS || M == M_Z) {
+    v2 = recon<M>(q, 2, P, opts, tally);
+    v3 = recon<M>(q, 3, P, opts, tally);
+  } else {
+    if (plateau5(q)) {
+      ++tally.plateau;
+      v2 = linear_value(q, 2);
+      v3 = linear_value(q, 3);
+      return;
+    }
+    ++tally.mlp;
+    double a0, a1, a2;
+    sr_betas<M>(q, P, a0, a1, a2);
+    v2 = sr_value<M>(q, 2, a0, a1, a2, opts, tally);
+    v3 = sr_value<M>(q, 3, a0, a1, a2, opts, tally);
+  }
+}
+
 // --- control block -------------------------------------------------------------------------------
 struct Ctl3 {
   double t, t_end, dt, cfl, hmin;
@@ -519,16 +545,18 @@ __global__ void __launch_bounds__(kT3) k3_trans(const double* __restrict__ nl, c
   const int3 e = step_of<TA>();
   Tally tally;
   const size_t o = d.cell(k, j, i);
-  // items (side, Gauss point, component) in one loop, so the closure is inlined once
+  // items (side, component) in one loop, so the closure is inlined once; each stencil gives both Gauss points
 #pragma unroll 1
-  for (int item = 0; item < 20; ++item) {
-    const int side = item / 10, gp = (item / 5) & 1, c = item % 5;
+  for (int item = 0; item < 10; ++item) {
+    const int side = item / 5, c = item % 5;
     const double* src = side == 0 ? nl : nr;
     double st[5];
 #pragma unroll
     for (int p = 0; p < 5; ++p) st[p] = src[d.cell(k + (p + 1) * e.z, j + (p + 1) * e.y, i + (p + 1) * e.x) * 5 + c];
-    double* dst = side == 0 ? (gp == 0 ? a_l1 : a_l2) : (gp == 0 ? a_r1 : a_r2);
-    dst[o * 5 + c] = recon<M>(st, 2 + gp, P, opts, tally);
+    double v1, v2;
+    recon_pair<M>(st, P, opts, tally, v1, v2);
+    (side == 0 ? a_l1 : a_r1)[o * 5 + c] = v1;
+    (side == 0 ? a_l2 : a_r2)[o * 5 + c] = v2;
   }
   if (counters && (opts & OPT_COUNT)) {
     if (tally.mlp) atomicAdd(&counters[2], (unsigned long long)tally.mlp);
@@ -539,7 +567,7 @@ __global__ void __launch_bounds__(kT3) k3_trans(const double* __restrict__ nl, c
 
 // --- second transverse pass and face fluxes (kernels.py:1015-1076; solver.py:175-199) ------------------
 template <int M, int DIR, int TB, int FLUX>
-__global__ void __launch_bounds__(kT3) k3_flux(const double* __restrict__ a_l1, const double* __restrict__ a_l2,
+__global__ void __launch_bounds__(kT3, 4) k3_flux(const double* __restrict__ a_l1, const double* __restrict__ a_l2,
                                                const double* __restrict__ a_r1, const double* __restrict__ a_r2,
                                                double* __restrict__ flux, Dims3 d, int kf, int jf, int iff, double h,
                                                int opts, const Ctl3* ctl, unsigned long long* counters,
@@ -550,13 +578,16 @@ __global__ void __launch_bounds__(kT3) k3_flux(const double* __restrict__ a_l1, 
   const double dt_h = ctl->dt / h;
   const int3 e = step_of<DIR>(), eb = step_of<TB>();
   Tally tally;
-  V5 acc;
+  // The four Gauss-point pairs (first, second) of the face: the stencils depend on the first point only (a_?1 or
+  // a_?2 along TB), the head on the second, so each pass over the first point reconstructs both second points.
+  // The reference sums the four fluxes in the order (1,1), (2,1), (1,2), (2,2); s3 holds the first pass's scaled
+  // (1,2) flux until the sum reaches it, so that the sum keeps that order.
+  V5 acc, s3;
 #pragma unroll 1
-  for (int flag = 1; flag <= 4; ++flag) {
-    const int first = (flag == 1 || flag == 3) ? 1 : 2, second = (flag == 1 || flag == 2) ? 1 : 2;
+  for (int first = 1; first <= 2; ++first) {
     const double* srcl = first == 1 ? a_l1 : a_l2;
     const double* srcr = first == 1 ? a_r1 : a_r2;
-    V5 pl, pr;
+    V5 pl[2], pr[2];  // [second - 1]
     // items (side, component) in one loop, so the closure is inlined once
 #pragma unroll 1
     for (int item = 0; item < 10; ++item) {
@@ -567,21 +598,37 @@ __global__ void __launch_bounds__(kT3) k3_flux(const double* __restrict__ a_l1, 
         const int kk = k + (p + 1) * eb.z, jj = j + (p + 1) * eb.y, ii = i + (p + 1) * eb.x;
         st[p] = side == 0 ? srcl[d.cell(kk + e.z, jj + e.y, ii + e.x) * 5 + c] : srcr[d.cell(kk, jj, ii) * 5 + c];
       }
-      const double v = recon<M>(st, second == 1 ? 2 : 3, P, opts, tally);
-      if (side == 0)
-        pl.v[c] = v;
-      else
-        pr.v[c] = v;
+      double v1, v2;
+      recon_pair<M>(st, P, opts, tally, v1, v2);
+      if (side == 0) {
+        pl[0].v[c] = v1;
+        pl[1].v[c] = v2;
+      } else {
+        pr[0].v[c] = v1;
+        pr[1].v[c] = v2;
+      }
     }
-    V5 f;
-    if constexpr (FLUX == 1)
-      f = hllc<DIR>(pr, pl);
-    else
-      f = flux_pri<DIR>(con_to_pri(evilin<DIR>(pr, pl, dt_h)));
+#pragma unroll 1
+    for (int second = 0; second < 2; ++second) {
+      V5 f;
+      if constexpr (FLUX == 1)
+        f = hllc<DIR>(pr[second], pl[second]);
+      else
+        f = flux_pri<DIR>(con_to_pri(evilin<DIR>(pr[second], pl[second], dt_h)));
 #pragma unroll
-    for (int c = 0; c < 5; ++c) {
-      const double scaled = f.v[c] * dt_h;
-      acc.v[c] = flag == 1 ? scaled : acc.v[c] + scaled;
+      for (int c = 0; c < 5; ++c) {
+        const double scaled = f.v[c] * dt_h;
+        if (first == 1) {
+          if (second == 0)
+            acc.v[c] = scaled;
+          else
+            s3.v[c] = scaled;
+        } else if (second == 0) {
+          acc.v[c] = acc.v[c] + scaled;  // (1,1) + (2,1)
+        } else {
+          acc.v[c] = (acc.v[c] + s3.v[c]) + scaled;  // + (1,2) + (2,2)
+        }
+      }
     }
   }
   st5(flux, ((size_t)k * jf + j) * iff + i, acc);
