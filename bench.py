@@ -1024,6 +1024,12 @@ def bench_3d(args, world, rank, local):
            opts=4)
     line["closure_tally_per_step"] = {k: {"mlp": v[0] / K, "plateau": v[1] / K} for k, v in E3.counters(ws).items()
                                       if k != "fallbacks"}
+    # one more step from the state the tally run reached: ncu --profile-from-start off captures these launches only
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    E3.run(q, sb.nx, sb.ny, sb.nz, dx, dy, dz, 0.4, method, "hllc", params, inflow=sb.inflow(), steps=1, ws=ws)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     if method not in ("js", "z"):
         line["roofline"] = _closure_roofline(
             "k3_normal + k3_trans + k3_flux (closure work only)", method,

@@ -313,8 +313,12 @@ __device__ __forceinline__ double js3(const double q[5], int head) {
 // (weno_z_borges_p2_results/weno5_3d_kernels_z.py:527-562, 673-706): tau5 = |beta0 - beta2|,
 // alpha_k = d_k (1 + (tau5 / (beta_k + eps))^2), w_k = alpha_k / sum. Same betas, linear weights and
 // candidates as js3, so the two differ only in the alphas.
-__device__ __forceinline__ double z3(const double q[5], int head, double eps) {
-  const Lin3 d = linear_weights(head);
+// z3 in two parts: the head-independent ratios tau5 / (beta_k + eps) and one head's weights and candidates
+struct Z3Ratio {
+  double r0, r1, r2;
+};
+
+__device__ __forceinline__ Z3Ratio z3_ratio(const double q[5], double eps) {
   const double t0 = q[0] - 2.0 * q[1] + q[2], u0 = q[0] - 4.0 * q[1] + 3.0 * q[2];
   const double t1 = q[1] - 2.0 * q[2] + q[3], u1 = q[1] - q[3];
   const double t2 = q[2] - 2.0 * q[3] + q[4], u2 = 3.0 * q[2] - 4.0 * q[3] + q[4];
@@ -322,12 +326,20 @@ __device__ __forceinline__ double z3(const double q[5], int head, double eps) {
   const double b1 = (13.0 / 12.0) * t1 * t1 + 0.25 * u1 * u1;
   const double b2 = (13.0 / 12.0) * t2 * t2 + 0.25 * u2 * u2;
   const double tau = fabs(b0 - b2);
-  const double r0 = tau / (b0 + eps), r1 = tau / (b1 + eps), r2 = tau / (b2 + eps);
-  const double a0 = d.d0 * (1.0 + r0 * r0), a1 = d.d1 * (1.0 + r1 * r1), a2 = d.d2 * (1.0 + r2 * r2);
+  return Z3Ratio{tau / (b0 + eps), tau / (b1 + eps), tau / (b2 + eps)};
+}
+
+__device__ __forceinline__ double z3_head(const double q[5], const Z3Ratio& r, int head) {
+  const Lin3 d = linear_weights(head);
+  const double a0 = d.d0 * (1.0 + r.r0 * r.r0), a1 = d.d1 * (1.0 + r.r1 * r.r1), a2 = d.d2 * (1.0 + r.r2 * r.r2);
   const double s = a0 + a1 + a2;
   double c[3];
   candidates(q, head, c);
   return (a0 / s) * c[0] + (a1 / s) * c[1] + (a2 / s) * c[2];
+}
+
+__device__ __forceinline__ double z3(const double q[5], int head, double eps) {
+  return z3_head(q, z3_ratio(q, eps), head);
 }
 
 // rho > 0 and p > 0 of a conserved 3D state
@@ -359,13 +371,17 @@ __device__ __forceinline__ double recon(const double q[5], int head, const typen
 
 // Both Gauss-point values (heads 2 and 3) of one transverse stencil. The SR closure's weights are a function of the
 // five stencil values alone, so one closure evaluation serves both heads (the reference evaluates it once per head,
-// with the same result); WENO5-JS and WENO-Z evaluate each head as a separate call, as the reference does.
+// with the same result); WENO-Z shares its smoothness ratios between the heads the same way.
 template <int M>
 __device__ __forceinline__ void recon_pair(const double q[5], const typename ClosureParams<M>::type& P, int opts,
                                            Tally& tally, double& v2, double& v3) {
-  if constexpr (M == M_JS || M == M_Z) {
-    v2 = recon<M>(q, 2, P, opts, tally);
-    v3 = recon<M>(q, 3, P, opts, tally);
+  if constexpr (M == M_JS) {
+    v2 = js3(q, 2);  // two calls: measured faster here than sharing the smoothness factors (fewer live registers)
+    v3 = js3(q, 3);
+  } else if constexpr (M == M_Z) {
+    const Z3Ratio r = z3_ratio(q, P.ex);
+    v2 = z3_head(q, r, 2);
+    v3 = z3_head(q, r, 3);
   } else {
     if (plateau5(q)) {
       ++tally.plateau;
@@ -476,15 +492,29 @@ __device__ __forceinline__ int3 step_of() {
   return DIR == 1 ? make_int3(1, 0, 0) : (DIR == 2 ? make_int3(0, 1, 0) : make_int3(0, 0, 1));  // (i, j, k)
 }
 
+// Thread tiling of a 128-thread block for a kernel whose 5-point stencils run along axis AX (1 = i, 2 = j, 3 = k):
+// rows of 128 cells along i when the stencil runs along i (the stencils of a warp overlap in the same row), else
+// 32 (i) x 4 (along AX) tiles, so that the four warps of a block read 8 overlapping stencil rows through L1
+// instead of 20 rows that only neighbouring blocks share (through L2).
+template <int AX>
+struct Tile3 {
+  static constexpr int bi = AX == 1 ? kT3 : 32, bj = AX == 2 ? kT3 / 32 : 1, bk = AX == 3 ? kT3 / 32 : 1;
+  __device__ static int i() { return (int)blockIdx.x * bi + (AX == 1 ? (int)threadIdx.x : (int)(threadIdx.x & 31)); }
+  __device__ static int j() { return (int)blockIdx.y * bj + (AX == 2 ? (int)(threadIdx.x >> 5) : 0); }
+  __device__ static int k() { return (int)blockIdx.z * bk + (AX == 3 ? (int)(threadIdx.x >> 5) : 0); }
+  static dim3 grid(int ni, int nj, int nk) { return dim3((ni + bi - 1) / bi, (nj + bj - 1) / bj, (nk + bk - 1) / bk); }
+};
+
 // --- normal reconstruction (kernels.py:869-927; mlp_normal_scalar.py) ---------------------------------
 template <int M, int DIR>
-__global__ void __launch_bounds__(kT3) k3_normal(const double* __restrict__ q, double* __restrict__ nl,
-                                                 double* __restrict__ nr, Dims3 d, int ni, int opts,
+__global__ void __launch_bounds__(kT3, 4) k3_normal(const double* __restrict__ q, double* __restrict__ nl,
+                                                 double* __restrict__ nr, Dims3 d, int ni, int nj, int nk, int opts,
                                                  const Ctl3* ctl, unsigned long long* counters,
                                                  const __grid_constant__ typename ClosureParams<M>::type P) {
   if (ctl && ctl->done) return;
-  const int i = blockIdx.x * kT3 + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= ni) return;
+  using TL = Tile3<DIR>;
+  const int i = TL::i(), j = TL::j(), k = TL::k();
+  if (i >= ni || j >= nj || k >= nk) return;
   const int3 e = step_of<DIR>();
   Tally tally;
   V5 ch[5];
@@ -537,11 +567,13 @@ template <int M, int TA>
 __global__ void __launch_bounds__(kT3) k3_trans(const double* __restrict__ nl, const double* __restrict__ nr,
                                                 double* __restrict__ a_l1, double* __restrict__ a_l2,
                                                 double* __restrict__ a_r1, double* __restrict__ a_r2, Dims3 d, int ni,
-                                                int opts, const Ctl3* ctl, unsigned long long* counters,
+                                                int nj, int nk, int opts, const Ctl3* ctl,
+                                                unsigned long long* counters,
                                                 const __grid_constant__ typename ClosureParams<M>::type P) {
   if (ctl && ctl->done) return;
-  const int i = blockIdx.x * kT3 + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= ni) return;
+  using TL = Tile3<TA>;
+  const int i = TL::i(), j = TL::j(), k = TL::k();
+  if (i >= ni || j >= nj || k >= nk) return;
   const int3 e = step_of<TA>();
   Tally tally;
   const size_t o = d.cell(k, j, i);
@@ -573,8 +605,9 @@ __global__ void __launch_bounds__(kT3, 4) k3_flux(const double* __restrict__ a_l
                                                int opts, const Ctl3* ctl, unsigned long long* counters,
                                                const __grid_constant__ typename ClosureParams<M>::type P) {
   if (ctl->done) return;
-  const int i = blockIdx.x * kT3 + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-  if (i >= iff) return;
+  using TL = Tile3<TB>;
+  const int i = TL::i(), j = TL::j(), k = TL::k();
+  if (i >= iff || j >= jf || k >= kf) return;
   const double dt_h = ctl->dt / h;
   const int3 e = step_of<DIR>(), eb = step_of<TB>();
   Tally tally;
@@ -749,19 +782,19 @@ int sweep3(wsr_ctx* ctx, const Run3& r, const Ws3& w, double h, cudaStream_t st)
   constexpr int TA = DIR == 1 ? 2 : (DIR == 2 ? 1 : 2);
   constexpr int TB = DIR == 3 ? 1 : 3;
   const int kn = DIR == 3 ? nz + 2 : pz, jn = DIR == 2 ? ny + 2 : py, in = DIR == 1 ? nx + 2 : px;
-  k3_normal<M, DIR><<<grid3(in, jn, kn), kT3, 0, st>>>(r.q, w.nl, w.nr, d, in, r.opts, w.ctl, w.counters,
-                                                       kparams<M, DIR>(ctx, r));
+  k3_normal<M, DIR><<<Tile3<DIR>::grid(in, jn, kn), kT3, 0, st>>>(r.q, w.nl, w.nr, d, in, jn, kn, r.opts, w.ctl,
+                                                                   w.counters, kparams<M, DIR>(ctx, r));
   WSR_LAUNCHED(ctx, "k3_normal");
   const int ka = TA == 3 ? nz : (DIR == 3 ? nz + 2 : pz);
   const int ja = TA == 2 ? ny : (DIR == 2 ? ny + 2 : py);
   const int ia = TA == 1 ? nx : (DIR == 1 ? nx + 2 : px);
-  k3_trans<M, TA><<<grid3(ia, ja, ka), kT3, 0, st>>>(w.nl, w.nr, w.al1, w.al2, w.ar1, w.ar2, d, ia, r.opts, w.ctl,
-                                                      w.counters, kparams<M, TA>(ctx, r));
+  k3_trans<M, TA><<<Tile3<TA>::grid(ia, ja, ka), kT3, 0, st>>>(w.nl, w.nr, w.al1, w.al2, w.ar1, w.ar2, d, ia, ja, ka,
+                                                                 r.opts, w.ctl, w.counters, kparams<M, TA>(ctx, r));
   WSR_LAUNCHED(ctx, "k3_trans");
   const int kf = DIR == 3 ? nz + 1 : nz, jf = DIR == 2 ? ny + 1 : ny, iff = DIR == 1 ? nx + 1 : nx;
   double* out = DIR == 1 ? w.fx : (DIR == 2 ? w.fy : w.fz);
-  k3_flux<M, DIR, TB, FLUX><<<grid3(iff, jf, kf), kT3, 0, st>>>(w.al1, w.al2, w.ar1, w.ar2, out, d, kf, jf, iff, h,
-                                                                r.opts, w.ctl, w.counters, kparams<M, TB>(ctx, r));
+  k3_flux<M, DIR, TB, FLUX><<<Tile3<TB>::grid(iff, jf, kf), kT3, 0, st>>>(
+      w.al1, w.al2, w.ar1, w.ar2, out, d, kf, jf, iff, h, r.opts, w.ctl, w.counters, kparams<M, TB>(ctx, r));
   WSR_LAUNCHED(ctx, "k3_flux");
   return WSR_OK;
 }
