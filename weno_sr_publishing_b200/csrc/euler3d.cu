@@ -493,15 +493,17 @@ __device__ __forceinline__ int3 step_of() {
 }
 
 // Thread tiling of a 128-thread block for a kernel whose 5-point stencils run along axis AX (1 = i, 2 = j, 3 = k):
-// rows of 128 cells along i when the stencil runs along i (the stencils of a warp overlap in the same row), else
-// 32 (i) x 4 (along AX) tiles, so that the four warps of a block read 8 overlapping stencil rows through L1
-// instead of 20 rows that only neighbouring blocks share (through L2).
+// 32 (i) x 4 tiles. When the stencil runs along j or k the four warp rows lie along that axis, so that a block's
+// warps read 8 overlapping stencil rows through L1 instead of 20 rows that only neighbouring blocks share (through
+// L2); when it runs along i they lie along j. 32-wide rows also fill the launch when a row is not a multiple of 128
+// cells (224 faces: 7 full warps instead of two 128-thread blocks with 32 idle threads).
 template <int AX>
 struct Tile3 {
-  static constexpr int bi = AX == 1 ? kT3 : 32, bj = AX == 2 ? kT3 / 32 : 1, bk = AX == 3 ? kT3 / 32 : 1;
-  __device__ static int i() { return (int)blockIdx.x * bi + (AX == 1 ? (int)threadIdx.x : (int)(threadIdx.x & 31)); }
-  __device__ static int j() { return (int)blockIdx.y * bj + (AX == 2 ? (int)(threadIdx.x >> 5) : 0); }
-  __device__ static int k() { return (int)blockIdx.z * bk + (AX == 3 ? (int)(threadIdx.x >> 5) : 0); }
+  static constexpr int kRows = AX == 1 ? 2 : AX;  // the axis of the tile's four warp rows
+  static constexpr int bi = 32, bj = kRows == 2 ? kT3 / 32 : 1, bk = kRows == 3 ? kT3 / 32 : 1;
+  __device__ static int i() { return (int)blockIdx.x * bi + (int)(threadIdx.x & 31); }
+  __device__ static int j() { return (int)blockIdx.y * bj + (kRows == 2 ? (int)(threadIdx.x >> 5) : 0); }
+  __device__ static int k() { return (int)blockIdx.z * bk + (kRows == 3 ? (int)(threadIdx.x >> 5) : 0); }
   static dim3 grid(int ni, int nj, int nk) { return dim3((ni + bi - 1) / bi, (nj + bj - 1) / bj, (nk + bk - 1) / bk); }
 };
 
