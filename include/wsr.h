@@ -87,7 +87,8 @@ typedef struct wsr_ctx wsr_ctx;
 /* Create a context bound to CUDA device `device`. */
 int wsr_ctx_create(int device, wsr_ctx **out);
 void wsr_ctx_destroy(wsr_ctx *ctx);
-/* Message of the last failed call on this context (static storage inside the context). */
+/* Message of the last failed call on this context (static storage inside the context). With a null context: the
+ * message of the last wsr_ctx_create that failed on the calling thread (thread-local storage), e.g. no CUDA device. */
 const char *wsr_last_error(const wsr_ctx *ctx);
 
 /* Closure parameters: `packed` is a HOST array in the order w1 b1 w2 b2 w3 b3 w4 b4 ([in][out]

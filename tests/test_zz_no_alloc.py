@@ -30,11 +30,7 @@ TOL = 1e-13  # relative max-norm, the tightest stage tolerance of the GPU suite
 
 
 def _lib():
-    L = N.lib()
-    vp, i, d = C.c_void_p, C.c_int, C.c_double
-    L.wsr_euler2d_stage_noalloc.argtypes = [vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, C.POINTER(d), vp]
-    L.wsr_euler2d_stage_noalloc.restype = i
-    return L
+    return N.lib()  # the binding declares wsr_euler2d_stage_noalloc's argument types
 
 
 def _noalloc(u_stage, u0, u_out, p, dt, rk, method, packed, bc="transmissive", flux="hllc"):

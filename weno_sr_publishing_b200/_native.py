@@ -56,6 +56,7 @@ def lib() -> C.CDLL:
             L.wsr_euler2d_workspace_bytes.restype = sz
             L.wsr_euler2d_stage.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, vp, sz, vp]
             L.wsr_euler2d_stage_at.argtypes = [vp, vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, d, vp, sz, vp]
+            L.wsr_euler2d_stage_noalloc.argtypes = [vp, vp, vp, i, i, d, d, d, d, i, i, i, i, i, C.POINTER(d), vp]
             L.wsr_euler2d_w7_workspace_bytes.restype = sz
             L.wsr_euler2d_w7_workspace_bytes.argtypes = [i, i]
             L.wsr_euler2d_w7_rhs.argtypes = [vp, vp, vp, i, i, d, d, d, i, i, i, i, vp, sz, vp]
@@ -134,7 +135,8 @@ class Context:
         h = C.c_void_p()
         rc = lib().wsr_ctx_create(device, C.byref(h))
         if rc != WSR_OK:
-            raise RuntimeError(f"wsr_ctx_create failed with status {rc}")
+            msg = lib().wsr_last_error(None).decode(errors="replace")
+            raise RuntimeError(f"wsr_ctx_create failed with status {rc}: {msg}")
         self.handle = h
         self._closure_keys: dict[int, bytes] = {}
 

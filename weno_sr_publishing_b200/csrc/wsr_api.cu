@@ -490,16 +490,31 @@ inline int band_lo(int ny, int nb, int k) {
 
 extern "C" {
 
+// Message of the last wsr_ctx_create that failed on this thread (there is no context to hold it).
+thread_local char g_create_err[256] = "";
+
 int wsr_ctx_create(int device, wsr_ctx** out) {
-  if (!out) return WSR_ERR_ARG;
+  if (!out) {
+    std::snprintf(g_create_err, sizeof(g_create_err), "wsr_ctx_create: null output pointer");
+    return WSR_ERR_ARG;
+  }
   *out = nullptr;
   wsr_ctx* ctx = new (std::nothrow) wsr_ctx();
-  if (!ctx) return WSR_ERR_ARG;
+  if (!ctx) {
+    std::snprintf(g_create_err, sizeof(g_create_err), "wsr_ctx_create: out of host memory");
+    return WSR_ERR_ARG;
+  }
   std::memset(ctx, 0, sizeof(*ctx));
   ctx->device = device;
   cudaError_t e = cudaSetDevice(device);
-  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&ctx->host_pinned), 4096);
+  const char* what = "cudaSetDevice";
+  if (e == cudaSuccess) {
+    e = cudaMallocHost(reinterpret_cast<void**>(&ctx->host_pinned), 4096);
+    what = "cudaMallocHost";
+  }
   if (e != cudaSuccess) {
+    std::snprintf(g_create_err, sizeof(g_create_err), "wsr_ctx_create(device %d): %s: %s", device, what,
+                  cudaGetErrorString(e));
     delete ctx;
     return WSR_ERR_CUDA;
   }
@@ -524,7 +539,10 @@ void wsr_ctx_destroy(wsr_ctx* ctx) {
   delete ctx;
 }
 
-const char* wsr_last_error(const wsr_ctx* ctx) { return ctx ? ctx->err : "null context"; }
+const char* wsr_last_error(const wsr_ctx* ctx) {
+  if (ctx) return ctx->err;
+  return g_create_err[0] ? g_create_err : "null context";
+}
 
 int wsr_closure_upload(wsr_ctx* ctx, int kind, const double* packed, int n) {
   if (!ctx) return WSR_ERR_ARG;
