@@ -510,9 +510,9 @@ struct Tile3 {
 // --- normal reconstruction (kernels.py:869-927; mlp_normal_scalar.py) ---------------------------------
 template <int M, int DIR>
 __global__ void __launch_bounds__(kT3, 4) k3_normal(const double* __restrict__ q, double* __restrict__ nl,
-                                                 double* __restrict__ nr, Dims3 d, int ni, int nj, int nk, int opts,
-                                                 const Ctl3* ctl, unsigned long long* counters,
-                                                 const __grid_constant__ typename ClosureParams<M>::type P) {
+                                                    double* __restrict__ nr, Dims3 d, int ni, int nj, int nk, int opts,
+                                                    const Ctl3* ctl, unsigned long long* counters,
+                                                    const __grid_constant__ typename ClosureParams<M>::type P) {
   if (ctl && ctl->done) return;
   using TL = Tile3<DIR>;
   const int i = TL::i(), j = TL::j(), k = TL::k();
@@ -602,10 +602,10 @@ __global__ void __launch_bounds__(kT3) k3_trans(const double* __restrict__ nl, c
 // --- second transverse pass and face fluxes (kernels.py:1015-1076; solver.py:175-199) ------------------
 template <int M, int DIR, int TB, int FLUX>
 __global__ void __launch_bounds__(kT3, 4) k3_flux(const double* __restrict__ a_l1, const double* __restrict__ a_l2,
-                                               const double* __restrict__ a_r1, const double* __restrict__ a_r2,
-                                               double* __restrict__ flux, Dims3 d, int kf, int jf, int iff, double h,
-                                               int opts, const Ctl3* ctl, unsigned long long* counters,
-                                               const __grid_constant__ typename ClosureParams<M>::type P) {
+                                                  const double* __restrict__ a_r1, const double* __restrict__ a_r2,
+                                                  double* __restrict__ flux, Dims3 d, int kf, int jf, int iff, double h,
+                                                  int opts, const Ctl3* ctl, unsigned long long* counters,
+                                                  const __grid_constant__ typename ClosureParams<M>::type P) {
   if (ctl->done) return;
   using TL = Tile3<TB>;
   const int i = TL::i(), j = TL::j(), k = TL::k();
